@@ -1,0 +1,433 @@
+"""FP64 CPU oracle for the matvis per-(time, frequency) visibility path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference`` legs of
+``bench.py`` may import it.  The product (``matvis_b200``) never does; the product
+runs only on the CUDA library and fails loudly without it.
+
+It restates, in plain numpy at complex128 / float64 (the reference's precision=2),
+the reference CPU path ``matvis.cpu.simulate`` with ``CPUMatMul`` / ``CPUVectorDot``.
+Each function names the reference lines it follows (paths relative to the
+reference project root).
+
+Parity pinning: ``tests/golden/make_golden.py`` runs the reference's own functions
+(loaded with inert stand-ins for astropy / pyuvdata / cupy, which are absent) and
+freezes their outputs in ``tests/golden/*.npz``; ``tests/test_oracle_golden.py``
+checks every function below against those fixtures.  Two pieces of the reference
+cannot be executed here at all and are therefore restated, not pinned:
+
+* the astropy / ERFA sky rotation (``cpu/coords.py``): replaced by the rigid
+  LST rotation ``eci_to_enu_matrix(lst, lat) @ point_source_crd_eq(ra, dec)`` that
+  the reference's own coordinate tests use (``tests/test_coordinates.py:71-160``);
+* pyuvdata's ``UVBeam`` / analytic beams: replaced by the reference GPU bilinear
+  scheme (``gpu/beams.py:127-200``, pinned) on in-memory grids, plus an achromatic
+  Gaussian power beam defined in this file.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+from scipy import ndimage
+
+#: Speed of light in m/s (the SI-defined value astropy's ``constants.c`` carries).
+SPEED_OF_LIGHT = 299792458.0
+
+
+# ---------------------------------------------------------------------------
+# Coordinates (src/matvis/coordinates.py)
+# ---------------------------------------------------------------------------
+def point_source_crd_eq(ra, dec):
+    """ECI unit vectors of sources; ``coordinates.py:174-200``. Shape (3, N)."""
+    ra = np.asarray(ra, dtype=np.float64)
+    dec = np.asarray(dec, dtype=np.float64)
+    return np.asarray([np.cos(ra) * np.cos(dec), np.cos(dec) * np.sin(ra), np.sin(dec)])
+
+
+def eci_to_enu_matrix(ha, lat):
+    """3x3 ECI->ENU rotation; ``coordinates.py:91-125``."""
+    return np.array(
+        [
+            [-np.sin(ha), np.cos(ha), 0.0 * ha],
+            [-np.sin(lat) * np.cos(ha), -np.sin(lat) * np.sin(ha), np.cos(lat)],
+            [np.cos(lat) * np.cos(ha), np.cos(lat) * np.sin(ha), np.sin(lat)],
+        ],
+        dtype=np.float64,
+    )
+
+
+def rotate_fixed_order(rot, eci):
+    """Topocentric ENU coordinates ``rot @ eci`` in one fixed operation order.
+
+    Row r is ``(R[r,0]*x + R[r,1]*y) + R[r,2]*z`` with each multiply and add
+    rounded separately (numpy elementwise operations never fuse).  The CUDA
+    rotation kernel evaluates exactly this sequence with ``__dmul_rn`` /
+    ``__dadd_rn``, so the horizon test ``z > 0`` selects bit-identical sources.
+    """
+    rot = np.asarray(rot, dtype=np.float64)
+    x, y, z = (np.asarray(eci[i], dtype=np.float64) for i in range(3))
+    out = np.empty((3, x.size), dtype=np.float64)
+    for r in range(3):
+        out[r] = (rot[r, 0] * x + rot[r, 1] * y) + rot[r, 2] * z
+    return out
+
+
+def enu_to_az_za(enu_e, enu_n, orientation="astropy", periodic_azimuth=True):
+    """Azimuth / zenith angle from ENU direction cosines; ``coordinates.py:31-88``."""
+    enu_e = np.asarray(enu_e, dtype=np.float64)
+    enu_n = np.asarray(enu_n, dtype=np.float64)
+    lsqr = enu_n**2.0 + enu_e**2.0
+    mask = lsqr < 1
+    zeta = np.zeros_like(lsqr)
+    zeta[mask] = np.sqrt(1 - lsqr[mask])
+    az = np.arctan2(enu_e, enu_n)
+    za = 0.5 * np.pi - np.arcsin(zeta)
+    if orientation == "uvbeam":
+        az = 0.5 * np.pi - az
+    if periodic_azimuth:
+        az = np.mod(az, 2 * np.pi)
+    return az, za
+
+
+# ---------------------------------------------------------------------------
+# Horizon selection (src/matvis/core/coords.py:77-150)
+# ---------------------------------------------------------------------------
+def nsrc_alloc(chunk_size: int, source_buffer: float) -> int:
+    """Capacity of the above-horizon buffers; ``core/coords.py:77-82``."""
+    if chunk_size > 1000:
+        return int(chunk_size * source_buffer)
+    return chunk_size
+
+
+def select_chunk(topo, flux, chunk: int, chunk_size: int, alloc: int):
+    """Strict ``z > 0`` selection of one source chunk; ``core/coords.py:99-150``.
+
+    Returns (coords (3, alloc), flux (alloc,), n, kept_indices).  Slots past ``n``
+    hold zero coordinates here (the reference keeps stale values there, which only
+    ever meet zero flux).
+    """
+    slc = slice(chunk * chunk_size, (chunk + 1) * chunk_size)
+    t = topo[:, slc]
+    f = flux[slc]
+    kept = np.where(t[2] > 0)[0]
+    n = len(kept)
+    if n > alloc:
+        raise ValueError(
+            f"nsrc_alloc ({alloc}) is too small for the number of sources above "
+            f"horizon ({n}). Try increasing source_buffer."
+        )
+    coords = np.zeros((3, alloc), dtype=np.float64)
+    fl = np.zeros(alloc, dtype=f.dtype)
+    coords[:, :n] = t[:, kept]
+    fl[:n] = f[kept]
+    return coords, fl, n, kept + chunk * chunk_size
+
+
+# ---------------------------------------------------------------------------
+# Beams
+# ---------------------------------------------------------------------------
+@dataclass
+class GridBeam:
+    """A beam tabulated on a regular (za, az) grid.
+
+    ``data`` has shape (nax, nfeed, nza, naz): complex E-field components when
+    ``beam_type == "efield"``, a real power pattern (1, 1, nza, naz) when
+    ``beam_type == "power"``.  ``za[0]`` must be 0 (the reference maps
+    ``za / dza`` to the row coordinate, ``gpu/beams.py:184``).
+    """
+
+    data: np.ndarray
+    az: np.ndarray
+    za: np.ndarray
+    beam_type: str = "efield"
+
+    @property
+    def daz(self):
+        return float(np.diff(self.az)[0])
+
+    @property
+    def dza(self):
+        return float(np.diff(self.za)[0])
+
+    @property
+    def azmin(self):
+        return float(np.min(self.az))
+
+
+@dataclass
+class GaussianPowerBeam:
+    """Achromatic Gaussian beam in zenith angle, unpolarised.
+
+    E-field amplitude ``exp(-za^2 / (2 sigma^2))``; the power pattern is its
+    square, and the simulation takes ``sqrt`` of the power as ``cpu/beams.py:46``.
+    """
+
+    sigma: float
+    beam_type: str = "power"
+
+    def power(self, za):
+        return np.exp(-(za**2) / (self.sigma**2))
+
+
+def bilinear_beam(grids, daz, dza, azmin, az, za):
+    """Order-1 ``map_coordinates`` per (beam, feed, axis); ``gpu/beams.py:127-200``.
+
+    ``grids`` has shape (nbeam, nax, nfeed, nza, naz); the output is
+    (nbeam, nfeed, nax, nsrc) complex128, with ``sqrt`` applied for power grids.
+    Points outside ``[0, n-1]`` on either grid axis give 0 (scipy's
+    ``mode='constant'``, which cupyx mirrors).
+    """
+    grids = np.asarray(grids)
+    nbeam, nax, nfeed = grids.shape[:3]
+    out = np.zeros((nbeam, nfeed, nax, len(az)), dtype=np.complex128)
+    for bm in range(nbeam):
+        coords = np.asarray([za / dza[bm], (az - azmin[bm]) / daz[bm]])
+        for fd in range(nfeed):
+            for ax in range(nax):
+                g = grids[bm, ax, fd]
+                if np.iscomplexobj(g):
+                    v = ndimage.map_coordinates(g.real.astype(np.float64), coords, order=1) + 1j * ndimage.map_coordinates(
+                        g.imag.astype(np.float64), coords, order=1
+                    )
+                else:
+                    v = ndimage.map_coordinates(g.astype(np.float64), coords, order=1)
+                out[bm, fd, ax] = v
+    if not np.iscomplexobj(grids):
+        out = np.sqrt(out)
+    return out
+
+
+def beam_response(beams, polarized: bool, crd_e, crd_n):
+    """Interpolated beam (nbeam, nfeed, nax, nsrc) at ENU direction cosines.
+
+    Follows ``GPUBeamInterpolator._interp`` (``gpu/beams.py:103-124``): uvbeam
+    azimuth orientation, then :func:`bilinear_beam`; analytic Gaussian power beams
+    are evaluated directly (``sqrt`` of power, ``cpu/beams.py:43-46``).
+    """
+    az, za = enu_to_az_za(crd_e, crd_n, orientation="uvbeam")
+    nfeed = nax = 2 if polarized else 1
+    out = np.zeros((len(beams), nfeed, nax, len(az)), dtype=np.complex128)
+    for i, bm in enumerate(beams):
+        if isinstance(bm, GaussianPowerBeam):
+            if polarized:
+                raise ValueError("beam type must be efield if using polarized=True")
+            out[i, 0, 0] = np.sqrt(bm.power(za))
+        else:
+            if polarized and bm.beam_type != "efield":
+                raise ValueError("beam type must be efield if using polarized=True")
+            data = bm.data
+            if not polarized and bm.beam_type == "efield":
+                # Unpolarised use of an E-field grid: power of feed 0 summed over
+                # the vector axes (the single-feed power pattern), as prepared by
+                # prepare_beam_unpolarized (core/beams.py:15-32) for feed "x".
+                data = np.sum(np.abs(data[:, :1]) ** 2, axis=0, keepdims=True)
+            out[i] = bilinear_beam(data[None], [bm.daz], [bm.dza], [bm.azmin], az, za)[0]
+    return out
+
+
+# ---------------------------------------------------------------------------
+# tau, Z, products (src/matvis/core/tau.py, core/getz.py, cpu/matprod.py)
+# ---------------------------------------------------------------------------
+def exptau(antpos, freq, crd):
+    """``exp(+i 2 pi nu / c * D . X)``; ``core/tau.py:30-31, 65-66`` (code sign)."""
+    ap = np.asarray(antpos, dtype=np.float64) * (2.0 * np.pi * freq) * 1j / SPEED_OF_LIGHT
+    return np.exp(ap @ np.asarray(crd, dtype=np.float64))
+
+
+def zmatrix(sqrt_flux, beam, ext, beam_idx, nfeed, nax):
+    """Z (nant*nfeed, nax*nsrc); ``core/getz.py:80-100``."""
+    nant, nsrc = ext.shape
+    e = ext * sqrt_flux
+    z = np.empty((nant, nfeed, nax, nsrc), dtype=np.complex128)
+    for fd in range(nfeed):
+        for ax in range(nax):
+            z[:, fd, ax, :] = e
+    if beam_idx is None:
+        z *= beam
+    else:
+        for ant, bmidx in enumerate(beam_idx):
+            z[ant] *= beam[bmidx]
+    return z.reshape(nant * nfeed, nax * nsrc)
+
+
+def matmul_vis(z, nant, nfeed, antpairs=None):
+    """``CPUMatMul.compute``; ``cpu/matprod.py:11-32``. Returns (npairs, nfeed, nfeed)."""
+    v = z.conj().dot(z.T)
+    v = v.reshape(nant, nfeed, nant, nfeed).transpose((0, 2, 3, 1))
+    if antpairs is None:
+        return v.reshape(nant * nant, nfeed, nfeed)
+    ap = np.asarray(antpairs)
+    return v[ap[:, 0], ap[:, 1]]
+
+
+def vectordot_vis(z, nant, nfeed, antpairs):
+    """``CPUVectorDot.compute``; ``cpu/matprod.py:35-53``."""
+    z = z.reshape((nant, nfeed, -1))
+    ap = np.asarray(antpairs)
+    out = np.empty((len(ap), nfeed, nfeed), dtype=np.complex128)
+    for i, (ai, aj) in enumerate(ap):
+        out[i] = z[aj].dot(z[ai].conj().T)
+    return out
+
+
+def all_pairs(nant):
+    """Default pair list, ``i`` slow; ``core/matprod.py:37-40``."""
+    return np.array([(i, j) for i in range(nant) for j in range(nant)])
+
+
+# ---------------------------------------------------------------------------
+# Driver (src/matvis/cpu/cpu.py:163-277) and wrapper (src/matvis/wrapper.py)
+# ---------------------------------------------------------------------------
+def simulate(
+    *,
+    antpos,
+    freq,
+    lsts,
+    latitude,
+    ra,
+    dec,
+    I_sky,
+    beam_list,
+    polarized=False,
+    beam_idx=None,
+    antpairs=None,
+    nchunks=1,
+    source_buffer=1.0,
+    matprod="MatMul",
+    eci=None,
+):
+    """One frequency, all times; ``cpu/cpu.py:163-277`` at precision=2.
+
+    Returns (ntimes, npairs, nfeed, nfeed) complex128 when polarized, else
+    (ntimes, npairs).
+    """
+    antpos = np.asarray(antpos, dtype=np.float64)
+    nant = antpos.shape[0]
+    nfeed = nax = 2 if polarized else 1
+    nsrc = len(I_sky)
+    nbeam = len(beam_list)
+    if beam_idx is None and nbeam not in (1, nant):
+        raise ValueError("If number of beams provided is not 1 or nant, beam_idx must be provided.")
+    if beam_idx is None and nbeam == nant:
+        beam_idx = np.arange(nant)
+    if beam_idx is None:
+        beam_idx = np.zeros(nant, dtype=int)
+    flux = np.sqrt(0.5 * np.asarray(I_sky, dtype=np.float64))  # cpu/cpu.py:188
+    if eci is None:
+        eci = point_source_crd_eq(ra, dec)
+    chunk_size = int(np.ceil(nsrc / nchunks))
+    alloc = nsrc_alloc(chunk_size, source_buffer)
+    pairs = all_pairs(nant) if antpairs is None else np.asarray(antpairs)
+    vis = np.zeros((len(lsts), len(pairs), nfeed, nfeed), dtype=np.complex128)
+    for t, lst in enumerate(lsts):
+        topo = rotate_fixed_order(eci_to_enu_matrix(lst, latitude), eci)
+        for c in range(nchunks):
+            crd, fl, n, _ = select_chunk(topo, flux, c, chunk_size, alloc)
+            if n == 0:
+                continue  # contributes exact zeros (CPU-driver semantics)
+            crd = crd[:, :n]
+            fl = fl[:n]
+            beam = beam_response(beam_list, polarized, crd[0], crd[1])
+            ext = exptau(antpos, freq, crd)
+            z = zmatrix(fl, beam, ext, beam_idx, nfeed, nax)
+            if matprod in ("MatMul", "CPUMatMul"):
+                vis[t] += matmul_vis(z, nant, nfeed, antpairs)
+            else:
+                vis[t] += vectordot_vis(z, nant, nfeed, pairs)
+    return vis if polarized else vis[:, :, 0, 0]
+
+
+def simulate_vis(
+    *,
+    ants,
+    fluxes,
+    ra,
+    dec,
+    freqs,
+    lsts,
+    latitude,
+    beams,
+    polarized=False,
+    beam_idx=None,
+    antpairs=None,
+    matprod="MatMul",
+    nchunks=1,
+    source_buffer=1.0,
+):
+    """Frequency loop of ``wrapper.simulate_vis``; ``wrapper.py:150-199``."""
+    antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
+    fluxes = np.asarray(fluxes)
+    assert fluxes.shape == (len(ra), len(freqs)), "The `fluxes` array must have shape (NSRCS, NFREQS)."
+    eci = point_source_crd_eq(ra, dec)
+    out = []
+    for i, freq in enumerate(freqs):
+        out.append(
+            simulate(
+                antpos=antpos,
+                freq=freq,
+                lsts=lsts,
+                latitude=latitude,
+                ra=ra,
+                dec=dec,
+                I_sky=fluxes[:, i],
+                beam_list=beams,
+                polarized=polarized,
+                beam_idx=beam_idx,
+                antpairs=antpairs,
+                nchunks=nchunks,
+                source_buffer=source_buffer,
+                matprod=matprod,
+                eci=eci,
+            )
+        )
+    return np.asarray(out)
+
+
+# ---------------------------------------------------------------------------
+# Chunk planning (src/matvis/_utils.py:124-319)
+# ---------------------------------------------------------------------------
+def get_required_chunks(freemem, nax, nfeed, nant, nsrc, nbeam, nbeampix, precision, source_buffer=1.0, memory_buffer=0.9):
+    """Byte-model chunk count; ``_utils.py:124-209``."""
+    if not (0 < memory_buffer <= 1.0):
+        raise ValueError("memory_buffer must be in the range (0, 1]")
+    rsize = 4 * precision
+    csize = 2 * rsize
+    total = freemem
+    ch = 0
+    while total >= freemem * memory_buffer and ch < 100:
+        ch += 1
+        nchunk = int(nsrc // ch * source_buffer)
+        total = (
+            nant * 3 * rsize
+            + nsrc * rsize
+            + nbeampix * nfeed * nax * csize
+            + 3 * nsrc * rsize
+            + 3 * 3 * rsize
+            + 3 * nsrc * rsize
+            + 3 * nchunk * rsize
+            + nchunk * rsize
+            + nant * nchunk * csize
+            + nbeam * nfeed * nax * nchunk * csize
+            + nchunk * nfeed * nant * nax * csize
+            + ch * nfeed * nant * nfeed * nant * csize
+        )
+    return max(ch, 1)
+
+
+def cosine_error_metric(v, ref, nfeed):
+    """Max over outputs of ``|V - V_ref| / sqrt(|V_ii^pp| |V_jj^qq|)`` (all-pairs layout).
+
+    ``v`` / ``ref``: (..., nant*nant, nfeed, nfeed).  The denominator uses the
+    oracle's autocorrelations, bounding each cross term by Cauchy-Schwarz.
+    """
+    ref = np.asarray(ref)
+    v = np.asarray(v)
+    nant = int(round(np.sqrt(ref.shape[-3])))
+    r = ref.reshape(ref.shape[:-3] + (nant, nant, nfeed, nfeed))
+    d = (v - ref).reshape(r.shape)
+    auto = np.abs(np.einsum("...iipp->...ip", r))  # (..., nant, nfeed)
+    # out[i, j, p, q] pairs feed q of antenna i with feed p of antenna j.
+    den = np.sqrt(auto[..., :, None, None, :] * auto[..., None, :, :, None])
+    den = np.where(den > 0, den, np.inf)
+    return float(np.max(np.abs(d) / den)) if d.size else 0.0
