@@ -1,0 +1,421 @@
+#!/usr/bin/env python
+"""Headline benchmark: antenna-pair x source terms/s on the HERA-350-like workload.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+
+Workload (one "step"): the whole config-2 job -- 350 antennas (320 on a 14.6 m
+hexagon + 30 outriggers), 196,608 sources (nside = 128 equal-area centres,
+lognormal flux), 64 frequencies x 16 LSTs, polarised (2 feeds x 2 axes), 4
+gridded beams with per-antenna beam_idx.  Seeded synthetic inputs.
+
+Terms per job = sum over (f, t) of Nant^2 * n_t, n_t the sources above the
+horizon at time t (the reference's all-pairs output, wrapper.py:168-174).
+
+`value` times graph replays of the job with inputs resident in HBM; `e2e` times
+``simulate_vis`` with host numpy inputs and outputs (H2D and D2H inside the
+timed region).  `roofline` is the Hermitian-product kernel (mvb_herk), timed
+live with CUDA events on its own launch stream.  `cpu_baseline` is the FP64
+oracle on a bounded sample of the same workload on this host's cores, and
+`plain_gpu` a complex64 torch restatement of the reference GPU driver (per-slice
+stages, full cgemm, per-time device->host copy) on a sample of slices.
+
+With --impl reference, rank 0 times the reference's CPU algorithm (the FP64
+oracle restatement; the reference package itself cannot be imported here:
+astropy / pyuvdata are absent) on one slice of the workload per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "antenna-pair×source terms/s vs plain GPU path at rel.err≤1e-6; p50/p99 latency"
+UNIT = "antenna-pair×source terms/s"
+SPEED_OF_LIGHT = 299792458.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--gemm-mode", default="bf16x6")
+    ap.add_argument("--k-chunk", type=int, default=None)
+    ap.add_argument("--nfreq", type=int, default=64)
+    ap.add_argument("--ntimes", type=int, default=16)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.path is None or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def terms_per_job(cfg) -> tuple[float, np.ndarray]:
+    """Nant^2 * sum_t n_t * Nf, with n_t from the same FP64 fixed-order rotation as the kernels."""
+    from matvis_b200.coordinates import eci_to_enu_matrix, point_source_crd_eq
+
+    eci = point_source_crd_eq(cfg["ra"], cfg["dec"])
+    counts = []
+    for lst in cfg["lsts"]:
+        R = eci_to_enu_matrix(lst, cfg["latitude"])
+        z = (R[2, 0] * eci[0] + R[2, 1] * eci[1]) + R[2, 2] * eci[2]
+        counts.append(int((z > 0).sum()))
+    nant = len(cfg["antpos"])
+    return float(nant * nant * sum(counts) * len(cfg["freqs"])), np.array(counts)
+
+
+# ----------------------------------------------------------------------------- plain GPU path
+def plain_gpu_sample(cfg, nslices: int = 6):
+    """Complex64 torch restatement of the reference GPU driver (gpu/gpu.py:197-254) on
+    `nslices` (f, t) slices: FP32 rotation, horizon gather with a host count,
+    bilinear beam via grid_sample, FP32 phase, per-antenna Z loop, full complex64
+    matmul (TF32 off), device->host copy of the full matrix per slice."""
+    import torch
+    import torch.nn.functional as Fnn
+
+    from matvis_b200.coordinates import eci_to_enu_matrix, point_source_crd_eq
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    dev = torch.device("cuda")
+    eci = torch.as_tensor(point_source_crd_eq(cfg["ra"], cfg["dec"]), dtype=torch.float32, device=dev)
+    antpos = torch.as_tensor(cfg["antpos"], dtype=torch.float32, device=dev)
+    beams = cfg["beams"]
+    grids = torch.as_tensor(np.stack([b.data for b in beams]), dtype=torch.complex64, device=dev)  # B,X,F,za,az
+    bidx = np.asarray(cfg["beam_idx"])
+    nant = len(cfg["antpos"])
+    nb, X, F, nza, naz = grids.shape
+    flux = torch.as_tensor(np.sqrt(0.5 * cfg["fluxes"]), dtype=torch.float32, device=dev)
+    terms = 0.0
+    times = []
+    for k in range(nslices + 1):
+        f = k % len(cfg["freqs"])
+        t = k % len(cfg["lsts"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        R = torch.as_tensor(eci_to_enu_matrix(cfg["lsts"][t], cfg["latitude"]), dtype=torch.float32, device=dev)
+        top = R @ eci
+        idx = torch.nonzero(top[2] > 0).squeeze(1)
+        n = int(idx.numel())  # host sync, as len(where) in the reference
+        crd = top[:, idx]
+        e, nn = crd[0], crd[1]
+        az = torch.remainder(0.5 * np.pi - torch.atan2(e, nn), 2 * np.pi)
+        za = 0.5 * np.pi - torch.asin(torch.sqrt(torch.clamp(1 - e * e - nn * nn, min=0)))
+        gx = az / (2 * np.pi) * 2 - 1  # grid_sample coords in [-1, 1], align_corners=True
+        gy = za / (0.5 * np.pi) * 2 - 1
+        grid = torch.stack([gx, gy], -1).view(1, 1, n, 2)
+        planes = torch.view_as_real(grids).permute(0, 1, 2, 5, 3, 4).reshape(1, nb * X * F * 2, nza, naz)
+        bv = Fnn.grid_sample(planes, grid, mode="bilinear", align_corners=True).view(nb, X, F, 2, n)
+        beam = torch.complex(bv[:, :, :, 0], bv[:, :, :, 1]).permute(0, 2, 1, 3)  # B,F,X,n
+        phase = (2 * np.pi * float(cfg["freqs"][f]) / SPEED_OF_LIGHT) * (antpos @ crd)
+        ext = torch.polar(torch.ones_like(phase), phase) * flux[idx, f][None, :]
+        z = ext[:, None, None, :].expand(nant, F, X, n).clone()
+        for a in range(nant):  # per-antenna loop of core/getz.py:95-96
+            z[a] *= beam[int(bidx[a])]
+        z = z.reshape(nant * F, X * n)
+        v = z.conj() @ z.T
+        _ = v.cpu()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if k > 0:  # first slice is warm-up
+            times.append(dt)
+            terms += nant * nant * n
+    return {"value": terms / sum(times), "unit": UNIT, "slices": nslices,
+            "sample": f"{nslices} (f, t) slices of the workload, complex64, TF32 off"}
+
+
+# ----------------------------------------------------------------------------- CPU oracle
+def cpu_oracle_sample(cfg, nsrc_sample: int, nslices: int = 1):
+    """FP64 oracle (reference CPU algorithm) on `nslices` slices with a source subset."""
+    from oracle import oracle as orc
+
+    from matvis_b200 import workloads as wl
+
+    sub = wl.subset(cfg, nsrc=nsrc_sample, nfreq=1, ntimes=1, seed=11)
+    beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in sub["beams"]]
+    antpos = np.asarray(sub["antpos"])
+    terms = 0.0
+    t0 = time.perf_counter()
+    for _ in range(nslices):
+        vis = orc.simulate(antpos=antpos, freq=float(sub["freqs"][0]), lsts=sub["lsts"], latitude=sub["latitude"],
+                           ra=sub["ra"], dec=sub["dec"], I_sky=sub["fluxes"][:, 0], beam_list=beams, polarized=True,
+                           beam_idx=sub["beam_idx"])
+        n = terms_per_job(sub)[1].sum()
+        terms += len(antpos) ** 2 * n
+    dt = time.perf_counter() - t0
+    del vis
+    return terms / dt, dt, f"{nslices} (f, t) slice(s), all {len(antpos)} antennas, {nsrc_sample} of " \
+                           f"{len(cfg['ra'])} sources (seeded subset), FP64 numpy/scipy"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from matvis_b200 import workloads as wl
+
+    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes)
+    nsrc_sample = 49152
+    for _ in range(max(args.warmup, 0)):
+        cpu_oracle_sample(cfg, nsrc_sample)
+    vals, dts = [], []
+    for _ in range(args.steps):
+        v, dt, sample = cpu_oracle_sample(cfg, nsrc_sample)
+        vals.append(v)
+        dts.append(dt)
+    value = float(np.median(vals))
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.median(dts)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "config2 HERA-350-like (350 ant, 196608 src, 64 f x 16 LST, polarised, 4 beams)",
+                   "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference package not importable here (astropy, pyuvdata absent); its CPU algorithm is timed "
+                "through the FP64 oracle restatement (oracle/oracle.py), pinned to fixtures from the reference code",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- B200 arm
+def run_b200(args, rank, world, local_rank):
+    import torch
+
+    import matvis_b200 as mv
+    from matvis_b200 import _lib
+    from matvis_b200 import workloads as wl
+    from matvis_b200.engine import VisEngine, job_from_arrays
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes)
+    terms, counts = terms_per_job(cfg)
+    spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
+                           lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
+                           polarized=True, precision=1, gemm_mode=args.gemm_mode, k_chunk=args.k_chunk)
+    eng = VisEngine(spec, device=dev)
+    eng.upload()
+    eng.run()  # uncaptured run: checks status, warms caches
+    eng.capture()
+    stream = torch.cuda.current_stream()
+
+    for _ in range(max(args.warmup, 0)):
+        eng.run(check=False)
+    torch.cuda.synchronize()
+    _lib.check_status_word(eng.status, "warm-up")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            eng.run(check=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    clocks = clk.summary()
+    _lib.check_status_word(eng.status, "timed run")
+    ms = ev0.elapsed_time(ev1) / max(args.steps, 1)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * terms / (ms_max / 1000.0)
+
+    # ---- roofline of the dominant kernel: mvb_herk on the last slice's panel
+    panel = eng.zcalc.z
+    M = eng.nant * eng.nfeed
+    nlast = int(eng.n_above.item())
+    kvalid = nlast * eng.nax
+    kc = eng.k_chunk
+    reps = 10
+    hs = torch.cuda.Stream(device=dev)
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ws = eng.matprod.workspace(panel, kc)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(hs):
+        for r in range(reps + 2):
+            if r == 2:
+                h0.record(hs)
+            _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), eng.matprod.mode, panel.Mpad, panel.Kcap,
+                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, _lib.ptr(ws), ws.numel(),
+                                         _lib.ptr(eng.status), _lib.stream_handle(hs)))
+        h1.record(hs)
+    torch.cuda.synchronize()
+    herk_ms = h0.elapsed_time(h1) / reps
+    algo_flops = 4.0 * M * (M + 1) * kvalid
+    T = panel.Mpad // 128
+    nprod = {"bf16x3": 3, "bf16x6": 6, "tf32x3": 3}[args.gemm_mode]
+    exec_flops = 8.0 * (T * (T + 1) // 2) * 128 * 128 * kvalid * nprod
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
+    achieved = algo_flops / (herk_ms / 1000.0) / 1e12
+    tensor_peak = bf16_peak if args.gemm_mode.startswith("bf16") else bf16_peak / 2
+    roofline = {
+        "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
+        "traffic": None, "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
+        "kernel": f"mvb_herk {args.gemm_mode}: M={M}, K={kvalid}, k_chunk={kc}",
+        "herk_ms": herk_ms,
+        "algorithmic_flops_per_launch": algo_flops,
+        "executed_tensor_tflops": exec_flops / (herk_ms / 1000.0) / 1e12,
+        "executed_tensor_frac": exec_flops / (herk_ms / 1000.0) / 1e12 / tensor_peak,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16" if args.gemm_mode.startswith("bf16") else "tf32",
+        "data": "synthetic (seeded; HEALPix nside=128 centres, HERA-350-like array, dipole-like beams)",
+        "config": {
+            "workload": f"config2 HERA-350-like: 350 ant x 196608 src x {len(cfg['freqs'])} freq x "
+                        f"{len(cfg['lsts'])} LST, polarised 2x2, 4 gridded beams + beam_idx; one job per step",
+            "gemm_mode": args.gemm_mode, "k_chunk": kc, "terms_per_job": terms,
+            "above_horizon_per_time": [int(c) for c in counts],
+            "l2": "inputs larger than L2 (Z panel ~%.1f GB per slice)" % (panel.data.numel() *
+                                                                          panel.data.element_size() / 1e9 * kvalid /
+                                                                          panel.Kcap),
+            "parallelism": "replicas (one job per GPU)" if world > 1 else "1 GPU",
+            "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, split-bf16 6-product "
+                         "tcgen05 Hermitian product with FP32 TMEM accumulation per k-slice, FP64 slice sums"
+                         if args.gemm_mode == "bf16x6" else args.gemm_mode,
+        },
+        "roofline": roofline,
+        "gpu_launches": eng.launches_per_run() * args.steps,
+        "clocks": clocks,
+    }
+
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        v, dt, sample = cpu_oracle_sample(cfg, 49152)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample,
+                                "seconds": dt}
+    if rank == 0 and not args.skip_plain:
+        try:
+            line["plain_gpu"] = plain_gpu_sample(cfg)
+            line["vs_plain_gpu"] = value / world / line["plain_gpu"]["value"]
+        except Exception as exc:  # the denominator is informative only
+            line["plain_gpu"] = {"error": repr(exc)[:200]}
+
+    if not args.skip_e2e:
+        ants = {i: tuple(p) for i, p in enumerate(cfg["antpos"])}
+        kw = dict(polarized=True, precision=1, beam_idx=cfg["beam_idx"], gemm_mode=args.gemm_mode,
+                  k_chunk=args.k_chunk, device=dev)
+        mv.simulate_vis(ants, cfg["fluxes"], cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
+                        cfg["latitude"], **kw)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nb_out = 0
+        for _ in range(args.e2e_steps):
+            out = mv.simulate_vis(ants, cfg["fluxes"], cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
+                                  cfg["latitude"], **kw)
+            nb_out = out.nbytes
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        e_t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
+        h2d = eng.h2d_bytes() + sum(b.data.nbytes for b in cfg["beams"]) + eng.antpos_host.nbytes
+        line["e2e"] = {"value": world * terms / float(e_t.item()), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(nb_out), "seconds_per_step": float(e_t.item()),
+                       "api": "matvis_b200.simulate_vis (host numpy in/out)", "steps": args.e2e_steps}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * matvis_b200.h -- C ABI of the B200 (sm_100a) visibility-path library
+ * (libmatvis_b200.so).
+ *
+ * Every entry point takes caller-owned DEVICE pointers (the 3x3 rotation of
+ * mvb_rotate is the one host array), plain sizes and a CUDA
+ * stream (cudaStream_t passed as void*), enqueues its kernels on that stream
+ * and returns an int status (MVB_OK = 0).  No entry point allocates device
+ * memory: scratch space is a caller-provided workspace whose size a *_ws_bytes
+ * query returns.  Device-side failures (buffer overflow, a bounded wait that
+ * ran out) are written to a caller-provided int32 status word on the device,
+ * never raised with a trap; the host reads it after the stream synchronises.
+ *
+ * Paths in the comments below are relative to the matvis project root; each
+ * entry point names the reference interface it replaces.
+ *
+ * Array conventions
+ *   - "SoA (3, ld)" coordinates: x at [0, ld), y at [ld, 2 ld), z at [2 ld, 3 ld).
+ *   - complex64 = interleaved float2, complex128 = interleaved double2.
+ *   - Z panel (the operand of the Hermitian product): real planes
+ *       plane[q][m][k],  q in [0, 2P),  m in [0, Mpad),  k in [0, Kcap)
+ *     with plane q = 2 p + c holding split term p (p = 0 most significant)
+ *     of component c (0 = real, 1 = imaginary).  Row m = ant * nfeed + feed,
+ *     column k = src * nax + ax.  Rows >= M and columns >= K_valid are zero.
+ *     Element type: bfloat16 for MVB_GEMM_BF16_*, float32 for MVB_GEMM_TF32_3.
+ */
+#ifndef MATVIS_B200_H
+#define MATVIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------- */
+#define MVB_OK 0
+#define MVB_ERR_ARG 1         /* bad argument (shape, alignment, enum)      */
+#define MVB_ERR_CUDA 2        /* a CUDA runtime call failed                 */
+#define MVB_ERR_OVERFLOW 3    /* above-horizon count exceeds the capacity   */
+#define MVB_ERR_NONFINITE 4   /* non-finite value in an interpolated beam   */
+#define MVB_ERR_TIMEOUT 5     /* a bounded device-side wait ran out         */
+#define MVB_ERR_UNSUPPORTED 6 /* device or configuration not supported      */
+
+/* device status word bits (OR-ed by kernels into *status) */
+#define MVB_DEV_OVERFLOW 0x1
+#define MVB_DEV_TIMEOUT 0x2
+#define MVB_DEV_NONFINITE 0x4
+
+/* ---- Hermitian-product precision modes ---------------------------------- */
+#define MVB_GEMM_BF16_3 0 /* 2-term bf16 split, 3 products (hh+hl+lh)        */
+#define MVB_GEMM_BF16_6 1 /* 3-term bf16 split, 6 products (order <= 2)      */
+#define MVB_GEMM_TF32_3 2 /* 2-term tf32 split, 3 products (3xTF32)          */
+#define MVB_Z_C64 3       /* plain complex64 Z (M, Kcap), for the pair loop */
+
+/* ---- library ----------------------------------------------------------- */
+int mvb_version(void);
+/* Message for the last non-OK status returned on the calling host thread. */
+const char *mvb_last_error(void);
+/* Number of SMs and compute capability of the current device. */
+int mvb_device_info(int *sm_count, int *cc_major, int *cc_minor);
+
+/* ---- A3: rotation ------------------------------------------------------- */
+/* topo(3, N) = R(3x3, row-major, host) @ eci(3, N), FP64, each row evaluated as
+ * (R[r,0]*x + R[r,1]*y) + R[r,2]*z with separately rounded operations.
+ * Replaces CoordinateRotation.rotate (core/coords.py:177-179; the LST form of
+ * coordinates.eci_to_enu_matrix @ point_source_crd_eq, coordinates.py:91-125,
+ * 174-200).  eci and topo are SoA with leading dimension N. */
+int mvb_rotate(const double *eci, int64_t N, const double *R, double *topo, void *stream);
+
+/* ---- A4: horizon selection ---------------------------------------------- */
+/* Bytes of workspace mvb_horizon_compact needs for a chunk of `count` sources. */
+size_t mvb_horizon_ws_bytes(int64_t count);
+/* Strict z > 0 selection over sources [c0, c1) of topo (SoA, leading dim ld):
+ * kept sources in ascending index order -> crd_out (SoA, leading dim cap),
+ * idx_out (global source index), n_out (device int32).  If flux != NULL,
+ * flux_out[i] = flux[idx_out[i]] for i < n and 0 for n <= i < cap.  If n > cap
+ * the first cap entries are written, *n_out = n and MVB_DEV_OVERFLOW is set.
+ * Replaces CoordinateRotation.select_chunk (core/coords.py:99-150). */
+int mvb_horizon_compact(const double *topo, int64_t ld, int64_t c0, int64_t c1, const double *flux, double *crd_out,
+                        int32_t *idx_out, double *flux_out, int32_t *n_out, int64_t cap, int32_t *status, void *ws,
+                        size_t ws_bytes, void *stream);
+
+/* ---- A5: beam interpolation ---------------------------------------------- */
+/* Bilinear interpolation (order-1 map_coordinates, 0 outside [0, n-1] on either
+ * axis) of grids (nbeam, nax, nfeed, nza, naz) at the sources of crd (SoA,
+ * leading dim ld): az/za from enu_to_az_za(orientation="uvbeam").  grid_kind:
+ * 0 complex64 E-field, 1 float32 power (sqrt applied after interpolation).
+ * params: nbeam x 3 doubles (daz, dza, azmin).  Output (nbeam, nfeed, nax, nout)
+ * complex64 (out_c128 = 0) or complex128 (1); sources i >= n (n = *n_dev if
+ * n_dev != NULL, else nsrc) are written as 0.  Grids of up to 200 KB per real
+ * plane are staged in shared memory.  If status != NULL, a non-finite result
+ * sets MVB_DEV_NONFINITE.  Replaces BeamInterpolator.__call__ /
+ * GPUBeamInterpolator._interp (core/beams.py:184-208, gpu/beams.py:103-200). */
+int mvb_beam_interp(const void *grids, int grid_kind, int nbeam, int nax, int nfeed, int nza, int naz,
+                    const double *params, const double *crd, int64_t ld, const int32_t *n_dev, int64_t nsrc,
+                    void *out, int out_c128, int64_t nout, int32_t *status, void *stream);
+/* Same interpolation at given (azimuth, zenith angle) rows azza (SoA, leading
+ * dim ld): the reference's gpu_beam_interpolation(beam, daz, dza, azmin, az, za)
+ * (gpu/beams.py:127-200).  Output (nbeam, nfeed, nax, nsrc). */
+int mvb_beam_interp_azza(const void *grids, int grid_kind, int nbeam, int nax, int nfeed, int nza, int naz,
+                         const double *params, const double *azza, int64_t ld, int64_t nsrc, void *out, int out_c128,
+                         void *stream);
+/* Achromatic Gaussian power beam, amplitude exp(-za^2 / (2 sigma^2)), one beam
+ * per sigma (nbeam entries), nfeed = nax = 1.  Replaces the analytic-beam path
+ * of GPUBeamInterpolator.interp (gpu/beams.py:100-101), on the device. */
+int mvb_beam_gaussian(const double *sigmas, int nbeam, const double *crd, int64_t ld, const int32_t *n_dev,
+                      int64_t nsrc, void *out, int out_c128, int64_t nout, void *stream);
+
+/* ---- A6: tau and Z --------------------------------------------------------- */
+/* exptau(A, nsrc) = exp(+2 pi i (freq/c) antpos . crd) with the phase in cycles
+ * reduced mod 1 in FP64 before an FP32 (out_c128 = 0) or FP64 sincospi.
+ * Replaces TauCalculator.__call__ (core/tau.py:48-71). */
+int mvb_exptau(const double *antpos, int A, double freq, const double *crd, int64_t ld, int64_t nsrc,
+               void *exptau, int out_c128, void *stream);
+/* Bytes of a Z panel for the given mode (2P planes of Mpad x Kcap). */
+size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap);
+/* Fused tau + Z: Z[a*F+f, s*X+x] = exptau(a, s) * sflux[j] * beam[bidx[a], f, x, s]
+ * with j = sidx[s] (sidx != NULL: sflux is the full per-source sqrt(0.5 I) at
+ * this frequency, float32) or j = s (sidx == NULL: sflux already compacted),
+ * written straight into a Z panel (mode MVB_GEMM_*) or a plain complex64 Z
+ * (mode MVB_Z_C64, row pitch Kcap).  n = *n_dev (or nsrc); sources in
+ * [n, roundup(n*X, 64)/X) are written as zeros.  beam: complex64 (nbeam, F, X,
+ * beam_ld) (device); beam_idx: int32 per antenna (NULL = beam 0 for all).
+ * Replaces TauCalculator.__call__ + ZMatrixCalc.__call__ (core/tau.py:48-71,
+ * core/getz.py:52-105) with no exptau round trip through HBM. */
+int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
+              int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld, int nbeam,
+              const int32_t *beam_idx, int F, int X, int mode, void *z, int64_t Mpad, int64_t Kcap, void *stream);
+/* Z panel (or plain complex64 Z) from a caller exptau (A, e_ld), complex64
+ * (e_c128 = 0) or complex128: Z[a*F+f, s*X+x] = exptau[a, s] * sflux[s] *
+ * beam[bidx[a], f, x, s] for s < nsrc, zeros up to roundup(nsrc*X, 64)/X.
+ * Replaces ZMatrixCalc.__call__ (core/getz.py:52-105); the caller's exptau is
+ * not modified (the reference scales it in place). */
+int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, int A, int64_t nsrc, const float *sflux,
+                      const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X, int mode,
+                      void *z, int64_t Mpad, int64_t Kcap, void *stream);
+/* Z panel (or plain complex64 Z) from a caller complex matrix z (M, K) with row
+ * pitch ldz elements, complex64 (z_c128 = 0) or complex128.  Columns in
+ * [K, roundup(K, 64)) are zero-filled.  Serves MatProd.__call__(z, chunk)
+ * on an externally built Z (core/matprod.py:83-101). */
+int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, void *z, int64_t Mpad,
+               int64_t Kcap, void *stream);
+
+/* ---- A7: Hermitian product on the tensor cores ------------------------------ */
+/* In the entry points below the valid K extent of the panel is
+ *   K_valid = min(n * kmul, Kcap),  n = *n_dev if n_dev != NULL else n_host,
+ * i.e. a source count times the columns per source (nax); the device count
+ * comes straight from mvb_horizon_compact, with no host round trip. */
+/* Workspace bytes: one FP32 partial tile (256 x 128 floats) per (k-slice, tile). */
+size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
+/* Upper-triangle 128 x 128 complex tiles of V = conj(Z) Z^T over K_valid
+ * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05
+ * tensor cores with TMEM accumulators, fed by TMA (cp.async.bulk.tensor,
+ * 32-byte swizzle); mode MVB_GEMM_* selects the split precision.
+ * Replaces GPUMatMul.compute -> zdotz -> cublas.c/zgemm (gpu/matprod.py:31-36,
+ * gpu/_cublas.py:7-65) and CPUMatMul.compute's z.conj().dot(z.T)
+ * (cpu/matprod.py:11-32); computes only the upper-triangle tiles. */
+int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
+             int k_chunk, void *ws, size_t ws_bytes, int32_t *status, void *stream);
+/* Reduces the FP32 partial tiles in FP64 and writes the visibilities in the
+ * reference layout out[pair, p, q] = V[ant_i*F + q, ant_j*F + p]
+ * (cpu/matprod.py:21-30): all nant^2 pairs (pairs = NULL, i slow) or the
+ * npairs listed in pairs (int32 [npairs][2]).  out: complex64 (out_c128 = 0)
+ * or complex128; accumulate != 0 adds to out (the sum over source chunks).
+ * Replaces MatProd.sum_chunks and the host transpose/gather of
+ * GPUMatMul.sum_chunks (core/matprod.py:103-115, gpu/matprod.py:38-63). */
+int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
+                    int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs, void *out, int out_c128,
+                    int accumulate, void *stream);
+
+/* ---- A8: per-pair source sums ----------------------------------------------- */
+size_t mvb_vecdot_ws_bytes(int64_t npairs, int nfeed, int64_t Kcap, int k_chunk);
+/* out[i, p, q] = sum_k Z[aj*F+p, k] conj(Z[ai*F+q, k]) for (ai, aj) = pairs[i]
+ * over K_valid columns (as for mvb_herk), Z a plain complex64 panel (row pitch
+ * Kcap), one warp per (k-slice, pair), FP64 slice sums in a fixed order.
+ * Replaces GPUVectorDot.compute (one cuBLAS call per pair, gpu/matprod.py:66-98)
+ * and CPUVectorDot.compute (cpu/matprod.py:35-53). */
+int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul, int nfeed,
+               const int32_t *pairs, int64_t npairs, int k_chunk, void *ws, size_t ws_bytes, void *out, int out_c128,
+               int accumulate, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MATVIS_B200_H */

@@ -1,0 +1,103 @@
+"""Host-side coordinate helpers (input preparation, FP64 numpy).
+
+Same functions and conventions as the reference's ``coordinates.py``; they build
+the per-job inputs (source unit vectors, the per-time 3x3 rotation) that the CUDA
+kernels consume.  Per-source work per time step runs on the GPU.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def point_source_crd_eq(ra, dec):
+    """ECI unit vectors, shape (3, N); coordinates.py:174-200."""
+    ra = np.asarray(ra, dtype=np.float64)
+    dec = np.asarray(dec, dtype=np.float64)
+    return np.asarray([np.cos(ra) * np.cos(dec), np.cos(dec) * np.sin(ra), np.sin(dec)])
+
+
+def eci_to_enu_matrix(ha, lat):
+    """3x3 ECI -> ENU rotation for hour angle (here: LST) and latitude; coordinates.py:91-125."""
+    return np.array(
+        [
+            [-np.sin(ha), np.cos(ha), 0.0 * ha],
+            [-np.sin(lat) * np.cos(ha), -np.sin(lat) * np.sin(ha), np.cos(lat)],
+            [np.cos(lat) * np.cos(ha), np.cos(lat) * np.sin(ha), np.sin(lat)],
+        ],
+        dtype=np.float64,
+    )
+
+
+def enu_to_eci_matrix(ha, lat):
+    """Inverse of :func:`eci_to_enu_matrix`; coordinates.py:128-160."""
+    return np.array(
+        [
+            [-np.sin(ha), -np.cos(ha) * np.sin(lat), np.cos(ha) * np.cos(lat)],
+            [np.cos(ha), -np.sin(ha) * np.sin(lat), np.sin(ha) * np.cos(lat)],
+            [0.0 * ha, np.cos(lat), np.sin(lat)],
+        ],
+        dtype=np.float64,
+    )
+
+
+def enu_to_az_za(enu_e, enu_n, orientation="astropy", periodic_azimuth=True):
+    """Azimuth / zenith angle of ENU direction cosines; coordinates.py:31-88."""
+    assert orientation in ("astropy", "uvbeam"), "orientation must be either 'astropy' or 'uvbeam'"
+    enu_e = np.asarray(enu_e, dtype=np.float64)
+    enu_n = np.asarray(enu_n, dtype=np.float64)
+    lsqr = enu_n**2.0 + enu_e**2.0
+    mask = lsqr < 1
+    zeta = np.zeros_like(lsqr)
+    zeta[mask] = np.sqrt(1 - lsqr[mask])
+    az = np.arctan2(enu_e, enu_n)
+    za = 0.5 * np.pi - np.arcsin(zeta)
+    if orientation == "uvbeam":
+        az = 0.5 * np.pi - az
+    if periodic_azimuth:
+        az = np.mod(az, 2 * np.pi)
+    return az, za
+
+
+def latitude_of(telescope_loc) -> float:
+    """Latitude in radians from a float or an object with a ``lat`` attribute."""
+    lat = getattr(telescope_loc, "lat", telescope_loc)
+    lat = getattr(lat, "rad", lat)
+    return float(lat)
+
+
+def lsts_of(times) -> np.ndarray:
+    """Local sidereal times (radians) for the time axis.
+
+    The rotation here is the rigid LST rotation, so ``times`` are LSTs in
+    radians (a 1-D array); an object with ``.rad`` is unwrapped.
+    """
+    t = getattr(times, "rad", times)
+    t = np.atleast_1d(np.asarray(t, dtype=np.float64))
+    if t.ndim != 1:
+        raise ValueError("times must be a 1-D array of LSTs (radians)")
+    return t
+
+
+def radec_of(skycoords) -> tuple[np.ndarray, np.ndarray]:
+    """(ra, dec) in radians from a (ra, dec) pair or an object with ra / dec."""
+    if hasattr(skycoords, "ra") and hasattr(skycoords, "dec"):
+        ra, dec = skycoords.ra, skycoords.dec
+        ra = getattr(ra, "rad", ra)
+        dec = getattr(dec, "rad", dec)
+    else:
+        ra, dec = skycoords
+    return np.asarray(ra, dtype=np.float64), np.asarray(dec, dtype=np.float64)
+
+
+class SkyCoords:
+    """Minimal (ra, dec) container in radians, the sky input of the plugins."""
+
+    def __init__(self, ra, dec):
+        self.ra = np.asarray(ra, dtype=np.float64)
+        self.dec = np.asarray(dec, dtype=np.float64)
+        if self.ra.shape != self.dec.shape:
+            raise ValueError("ra and dec must have the same shape")
+
+    def __len__(self):
+        return len(self.ra)

@@ -1,0 +1,505 @@
+// A7: V = conj(Z) Z^T on the 5th-generation tensor cores (tcgen05 + TMEM),
+// upper-triangle tiles only, in split precision.
+//
+// Reference: gpu/matprod.py:31-36 / gpu/_cublas.py:7-65 (one full c/zgemm with
+// OP_C, OP_N per time and chunk), cpu/matprod.py:11-32 (z.conj().dot(z.T)),
+// core/matprod.py:103-115 (sum over source chunks).
+//
+// Formulation.  For rows m, n of Z (row = ant * nfeed + feed):
+//   Re V[m, n] = sum_k Zr[m,k] Zr[n,k] + Zi[m,k] Zi[n,k]
+//   Im V[m, n] = sum_k Zr[m,k] Zi[n,k] - Zi[m,k] Zr[n,k]
+// A 128 x 128 complex tile (I, J), I <= J, accumulates in one 128 x 256 FP32
+// TMEM block D (columns 0..127 real, 128..255 imaginary) from three UMMAs per
+// k-step and split-term product (pa, pb):
+//   D[:,   0:256] += Zr_I^pa . [Zr_J^pb ; Zi_J^pb]^T     (N = 256)
+//   D[:,   0:128] += Zi_I^pa . Zi_J^pb^T                  (N = 128)
+//   D[:, 128:256] += Zi_I^pa . (-Zr_J^pb)^T               (N = 128, negate-B bit)
+// Split products: BF16_3 {00, 01, 10}; BF16_6 {00, 01, 10, 02, 11, 20};
+// TF32_3 {00, 01, 10}.
+//
+// Schedule.  Work unit u = (k-slice s, tile t), t fastest so the CTAs that run
+// together read the same Z columns (L2 reuse).  Persistent CTAs (one per SM,
+// 192 KB of shared memory) loop over units.  Warp roles:
+//   warp 0 lane 0 : TMA producer, one 3-D box per operand per stage (all 2P
+//                   split/component planes of 128 rows x 32 bytes, SWIZZLE_32B);
+//   warp 1        : TMEM owner (512 columns = two accumulators); lane 0 issues
+//                   the UMMAs and tcgen05.commit's stage / accumulator barriers;
+//   warps 2..5    : epilogue, tcgen05.ld of TMEM lane quadrant (warp % 4) and
+//                   coalesced FP32 stores of the tile to the workspace
+//                   [u][256 columns][128 rows]; double-buffered accumulators let
+//                   unit u drain while unit u + 1 accumulates.
+// Every mbarrier wait is bounded by wall time; on expiry the CTA records
+// MVB_DEV_TIMEOUT in the status word, stops issuing work, drains the copies and
+// MMAs it issued, frees TMEM and returns.
+//
+// The FP32 partial tiles of the k-slices are summed in FP64 by herk_reduce_*.
+#include <algorithm>
+#include <mutex>
+
+#include <cudaTypedefs.h>
+
+#include "common.cuh"
+
+namespace mvb {
+
+constexpr int kHerkThreads = 192;
+constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s
+constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
+constexpr int kPlaneBytes = 128 * 32;              // one 128-row x 32-byte plane tile
+constexpr int kSmemBudget = 192 * 1024;
+
+template <int MODE>
+struct HerkCfg {
+  static constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
+  static constexpr int ES = MODE == MVB_GEMM_TF32_3 ? 4 : 2;
+  static constexpr int KSTEP = 32 / ES;  // elements per 32-byte k-step (= UMMA K)
+  static constexpr int OPER_BYTES = 2 * P * kPlaneBytes;
+  static constexpr int STAGE_BYTES = 2 * OPER_BYTES;
+  static constexpr int STAGES = kSmemBudget / STAGE_BYTES;
+  static constexpr int NPROD = P == 3 ? 6 : 3;
+  static constexpr uint32_t FMT = MODE == MVB_GEMM_TF32_3 ? 2u : 1u;
+  static constexpr uint32_t ID256 = umma_idesc(FMT, 256, 0);
+  static constexpr uint32_t ID128 = umma_idesc(FMT, 128, 0);
+  static constexpr uint32_t ID128N = umma_idesc(FMT, 128, 1);
+};
+
+// Valid K columns: (source count) x (columns per source), clamped to the panel.
+__device__ __forceinline__ int64_t valid_k(const int32_t *n_dev, int64_t n_host, int kmul, int64_t Kcap) {
+  int64_t n = n_dev ? (int64_t)*n_dev : n_host;
+  n = n < 0 ? 0 : n;
+  return min(n * kmul, Kcap);
+}
+
+__device__ __forceinline__ void decode_tile(int t, int T, int &I, int &J) {
+  int i = 0;
+  while (t >= T - i) {
+    t -= T - i;
+    ++i;
+  }
+  I = i;
+  J = i + t;
+}
+
+template <int MODE>
+__device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  if constexpr (MODE == MVB_GEMM_TF32_3)
+    umma_tf32(d, a, b, idesc, acc);
+  else
+    umma_bf16(d, a, b, idesc, acc);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kHerkThreads, 1)
+    herk_kernel(const __grid_constant__ CUtensorMap zmap, int T, int n_tiles, const int32_t *__restrict__ n_dev,
+                int64_t n_host, int kmul, int64_t Kcap, int k_chunk, float *__restrict__ partials,
+                int32_t *__restrict__ status) {
+  using C = HerkCfg<MODE>;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[C::STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[C::STAGES];
+  __shared__ __align__(8) uint64_t tfull_bar[2];
+  __shared__ __align__(8) uint64_t tempty_bar[2];
+  __shared__ __align__(8) uint64_t drain_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
+  const int nsplit = (int)((kvalid + k_chunk - 1) / k_chunk);
+  const int n_units = n_tiles * nsplit;
+  if ((int)blockIdx.x >= n_units) return;  // uniform over the CTA
+
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 4);
+    }
+    mbar_init(&drain_bar, 1);
+    abort_flag = 0;
+    fence_mbar_init();
+    tma_prefetch_desc(&zmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(&tmem_base_sh, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tmem_base_sh;
+
+  uint64_t issued = 0;  // producer: stages issued
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    uint32_t st = 0, ph = 0;
+    for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
+      const int s = u / n_tiles, t = u % n_tiles;
+      int I, J;
+      decode_tile(t, T, I, J);
+      const int64_t k0 = (int64_t)s * k_chunk;
+      const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
+      const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
+      const bool diag = I == J;
+      const uint32_t bytes = diag ? C::OPER_BYTES : 2 * C::OPER_BYTES;
+      for (int ks = 0; ks < nks; ++ks) {
+        if (!mbar_wait(&empty_bar[st], ph ^ 1, kWaitLimitNs)) {
+          atomicOr(status, MVB_DEV_TIMEOUT);
+          abort_flag = 1;
+          break;
+        }
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        uint8_t *a = smem + (size_t)st * C::STAGE_BYTES;
+        const int kc = (int)(k0 + (int64_t)ks * C::KSTEP);
+        tma_load_3d(a, &zmap, &full_bar[st], kc, I * 128, 0);
+        if (!diag) tma_load_3d(a + C::OPER_BYTES, &zmap, &full_bar[st], kc, J * 128, 0);
+        ++issued;
+        if (++st == C::STAGES) {
+          st = 0;
+          ph ^= 1;
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- UMMA issuer ----------------
+    constexpr int pa_tab[6] = {0, 0, 1, 0, 1, 2};
+    constexpr int pb_tab[6] = {0, 1, 0, 2, 1, 0};
+    uint32_t st = 0, ph = 0, buf = 0;
+    uint32_t tph = 0;  // bit b: phase of accumulator b
+    for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
+      const int s = u / n_tiles, t = u % n_tiles;
+      int I, J;
+      decode_tile(t, T, I, J);
+      const int64_t k0 = (int64_t)s * k_chunk;
+      const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
+      const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
+      const bool diag = I == J;
+      if (!mbar_wait(&tempty_bar[buf], ((tph >> buf) & 1u) ^ 1u, kWaitLimitNs)) {
+        atomicOr(status, MVB_DEV_TIMEOUT);
+        abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d = tbase + buf * 256;
+      bool ok = true;
+      for (int ks = 0; ks < nks; ++ks) {
+        if (!mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
+          atomicOr(status, MVB_DEV_TIMEOUT);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a_base = smem_u32(smem + (size_t)st * C::STAGE_BYTES);
+        const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
+#pragma unroll
+        for (int q = 0; q < C::NPROD; ++q) {
+          const uint32_t pa = pa_tab[q], pb = pb_tab[q];
+          const uint64_t a_re = umma_desc_sw32(a_base + (2 * pa) * kPlaneBytes);
+          const uint64_t a_im = umma_desc_sw32(a_base + (2 * pa + 1) * kPlaneBytes);
+          const uint64_t b_re = umma_desc_sw32(b_base + (2 * pb) * kPlaneBytes);
+          const uint64_t b_im = umma_desc_sw32(b_base + (2 * pb + 1) * kPlaneBytes);
+          umma<MODE>(d, a_re, b_re, C::ID256, (ks > 0 || q > 0) ? 1u : 0u);
+          umma<MODE>(d, a_im, b_im, C::ID128, 1u);
+          umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+        }
+        tc_commit(&empty_bar[st]);
+        if (++st == C::STAGES) {
+          st = 0;
+          ph ^= 1;
+        }
+      }
+      if (!ok) break;
+      tc_commit(&tfull_bar[buf]);
+      tph ^= 1u << buf;
+      buf ^= 1;
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue ----------------
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    uint32_t buf = 0;
+    uint32_t tph = 0;  // bit b: phase of accumulator b
+    for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
+      // every lane waits; the vote keeps the warp converged for tcgen05.ld
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull_bar[buf], (tph >> buf) & 1u, kWaitLimitNs));
+      if (!ok) {
+        if (lane == 0) atomicOr(status, MVB_DEV_TIMEOUT);
+        abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      float *dst = partials + (size_t)u * (256 * 128);
+      const uint32_t taddr = tbase + ((uint32_t)(quad * 32) << 16) + buf * 256;
+#pragma unroll 1
+      for (int c = 0; c < 8; ++c) {
+        uint32_t v[32];
+        tmem_ld32(taddr + c * 32, v);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) dst[(c * 32 + j) * 128 + row] = __uint_as_float(v[j]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
+      tph ^= 1u << buf;
+      buf ^= 1;
+    }
+  }
+
+  __syncthreads();
+  if (abort_flag) {
+    if (warp == 0 && lane == 0) {
+      // wait for the copies still in flight (the last STAGES issued)
+      const uint64_t first = issued > (uint64_t)C::STAGES ? issued - C::STAGES : 0;
+      for (uint64_t i = first; i < issued; ++i)
+        mbar_wait(&full_bar[i % C::STAGES], (uint32_t)((i / C::STAGES) & 1), kDrainLimitNs);
+    }
+    if (warp == 1 && lane == 0) {
+      tc_commit(&drain_bar);
+      mbar_wait(&drain_bar, 0, kDrainLimitNs);
+    }
+    __syncthreads();
+  }
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tbase, 512);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 reduction of the partial tiles into the reference output layout
+// out[pair, p, q] = V[ant_i * F + q, ant_j * F + p].
+// ---------------------------------------------------------------------------
+constexpr int kRedRows = 32, kRedCols = 32;
+
+__device__ __forceinline__ int tile_index(int I, int J, int T) { return I * T - (I * (I - 1)) / 2 + (J - I); }
+
+template <typename OT>
+__device__ __forceinline__ void store_out(void *out, int64_t idx, double re, double im, int accumulate) {
+  OT *o = static_cast<OT *>(out) + idx;
+  if (accumulate) {
+    o->x += re;
+    o->y += im;
+  } else {
+    o->x = re;
+    o->y = im;
+  }
+}
+
+// One CTA (256 threads) per 32 x 32 sub-block of an upper tile.
+template <typename OT>
+__global__ void __launch_bounds__(256)
+    herk_reduce_all_kernel(const float *__restrict__ part, int T, int n_tiles, const int32_t *__restrict__ n_dev,
+                           int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int A, int F, void *__restrict__ out,
+                           int accumulate) {
+  __shared__ double sre[kRedRows][kRedCols + 1], sim[kRedRows][kRedCols + 1];
+  const int t = blockIdx.x / 16, sub = blockIdx.x % 16;
+  int I, J;
+  decode_tile(t, T, I, J);
+  const int r0 = (sub / 4) * kRedRows, c0 = (sub % 4) * kRedCols;
+  const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
+  const int nsplit = (int)((kvalid + k_chunk - 1) / k_chunk);
+  const int M = A * F;
+  const int mbase = I * 128 + r0, nbase = J * 128 + c0;
+  if (mbase >= M || nbase >= M) return;
+
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double are[4] = {0, 0, 0, 0}, aim[4] = {0, 0, 0, 0};
+  for (int s = 0; s < nsplit; ++s) {
+    const float *p = part + ((size_t)s * n_tiles + t) * (256 * 128);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + w * 4 + j;
+      are[j] += (double)p[c * 128 + r0 + lane];
+      aim[j] += (double)p[(128 + c) * 128 + r0 + lane];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    sre[lane][w * 4 + j] = are[j];
+    sim[lane][w * 4 + j] = aim[j];
+  }
+  __syncthreads();
+
+  const int64_t AF2 = (int64_t)A * F * F;
+  // direct: rows m -> (i, q), columns n -> (j, p); out[(i*A + j)*F*F + p*F + q]
+  for (int e = threadIdx.x; e < kRedRows * kRedCols; e += 256) {
+    const int rl = e % kRedRows, cl = e / kRedRows;  // consecutive threads: consecutive rows
+    const int m = mbase + rl, n = nbase + cl;
+    if (m >= M || n >= M) continue;
+    const int i = m / F, q = m % F, j = n / F, p = n % F;
+    store_out<OT>(out, i * AF2 + (int64_t)j * F * F + p * F + q, sre[rl][cl], sim[rl][cl], accumulate);
+  }
+  if (I == J) return;
+  // mirror: V[n, m] = conj(V[m, n]); rows n -> (i2, q2), columns m -> (j2, p2)
+  for (int e = threadIdx.x; e < kRedRows * kRedCols; e += 256) {
+    const int cl = e % kRedCols, rl = e / kRedCols;  // consecutive threads: consecutive m
+    const int m = mbase + rl, n = nbase + cl;
+    if (m >= M || n >= M) continue;
+    const int i2 = n / F, q2 = n % F, j2 = m / F, p2 = m % F;
+    store_out<OT>(out, i2 * AF2 + (int64_t)j2 * F * F + p2 * F + q2, sre[rl][cl], -sim[rl][cl], accumulate);
+  }
+}
+
+// Explicit pair list: one thread per (pair, p, q).
+template <typename OT>
+__global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, int n_tiles,
+                                         const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap,
+                                         int k_chunk, int F, const int32_t *__restrict__ pairs, int64_t npairs,
+                                         void *__restrict__ out, int accumulate) {
+  const int64_t total = npairs * F * F;
+  const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
+  const int nsplit = (int)((kvalid + k_chunk - 1) / k_chunk);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pr = e / (F * F);
+    const int p = (int)((e / F) % F), q = (int)(e % F);
+    int m = pairs[2 * pr] * F + q, n = pairs[2 * pr + 1] * F + p;
+    bool conj = false;
+    if (m / 128 > n / 128) {
+      const int tmp = m;
+      m = n;
+      n = tmp;
+      conj = true;
+    }
+    const int t = tile_index(m / 128, n / 128, T);
+    const int r = m % 128, c = n % 128;
+    double re = 0, im = 0;
+    for (int s = 0; s < nsplit; ++s) {
+      const float *p0 = part + ((size_t)s * n_tiles + t) * (256 * 128);
+      re += (double)p0[c * 128 + r];
+      im += (double)p0[(128 + c) * 128 + r];
+    }
+    store_out<OT>(out, e, re, conj ? -im : im, accumulate);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+// Raises a kernel's dynamic shared-memory limit once per (device, slot); the
+// attribute is not touched again, in particular not during graph capture.
+int set_smem_once(const void *fn, int bytes, int slot) {
+  static bool done[64][8] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 8)
+    return fail(MVB_ERR_CUDA, "set_smem_once: bad device");
+  if (done[dev][slot]) return MVB_OK;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return fail(MVB_ERR_CUDA, "smem attribute: %s", cudaGetErrorString(e));
+  done[dev][slot] = true;
+  return MVB_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+template <int MODE>
+static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
+                       int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
+  using C = HerkCfg<MODE>;
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(MVB_ERR_UNSUPPORTED, "mvb_herk: cuTensorMapEncodeTiled unavailable");
+  CUtensorMap map;
+  cuuint64_t dims[3] = {(cuuint64_t)Kcap, (cuuint64_t)Mpad, (cuuint64_t)(2 * C::P)};
+  cuuint64_t strides[2] = {(cuuint64_t)Kcap * C::ES, (cuuint64_t)Mpad * Kcap * C::ES};
+  cuuint32_t box[3] = {(cuuint32_t)C::KSTEP, 128u, (cuuint32_t)(2 * C::P)};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(&map, MODE == MVB_GEMM_TF32_3 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+                   const_cast<void *>(z), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MVB_ERR_CUDA, "mvb_herk: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  const int T = (int)(Mpad / 128);
+  const int n_tiles = T * (T + 1) / 2;
+  const int64_t max_units = (int64_t)n_tiles * ceil_div(Kcap, k_chunk);
+  const int grid = (int)std::min<int64_t>(max_units, num_sms());
+  const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
+  int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE>), (int)smem, MODE);
+  if (rc) return rc;
+  if (grid <= 0) return MVB_OK;
+  herk_kernel<MODE><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, partials,
+                                                     status);
+  return check_launch("herk_kernel");
+}
+
+}  // namespace mvb
+
+using namespace mvb;
+
+extern "C" size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk) {
+  if (Mpad <= 0 || Kcap <= 0 || k_chunk <= 0) return 0;
+  const int64_t T = Mpad / 128;
+  return (size_t)(T * (T + 1) / 2) * (size_t)ceil_div(Kcap, k_chunk) * 256 * 128 * sizeof(float);
+}
+
+extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
+                        int kmul, int k_chunk, void *ws, size_t ws_bytes, int32_t *status, void *stream) {
+  if (!z || !ws || !status || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || Kcap % kKAlign || k_chunk <= 0 ||
+      k_chunk % kKAlign || n_host < 0 || kmul <= 0)
+    return fail(MVB_ERR_ARG, "mvb_herk: bad arguments");
+  if (!n_dev && n_host * kmul > Kcap) return fail(MVB_ERR_ARG, "mvb_herk: n * kmul exceeds Kcap");
+  if (reinterpret_cast<uintptr_t>(z) % 16) return fail(MVB_ERR_ARG, "mvb_herk: panel not 16-byte aligned");
+  if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk)) return fail(MVB_ERR_ARG, "mvb_herk: workspace too small");
+  if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk: panel too large");
+  cudaStream_t s = as_stream(stream);
+  float *part = static_cast<float *>(ws);
+  switch (mode) {
+    case MVB_GEMM_BF16_3:
+      return launch_herk<MVB_GEMM_BF16_3>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s);
+    case MVB_GEMM_BF16_6:
+      return launch_herk<MVB_GEMM_BF16_6>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s);
+    case MVB_GEMM_TF32_3:
+      return launch_herk<MVB_GEMM_TF32_3>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s);
+    default: return fail(MVB_ERR_ARG, "mvb_herk: unknown mode %d", mode);
+  }
+}
+
+extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
+                               int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs,
+                               void *out, int out_c128, int accumulate, void *stream) {
+  if (!ws || !out || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || nant <= 0 || (nfeed != 1 && nfeed != 2) ||
+      k_chunk <= 0 || kmul <= 0 || (int64_t)nant * nfeed > Mpad || (pairs && npairs < 0))
+    return fail(MVB_ERR_ARG, "mvb_herk_reduce: bad arguments");
+  const int T = (int)(Mpad / 128);
+  const int n_tiles = T * (T + 1) / 2;
+  const float *part = static_cast<const float *>(ws);
+  cudaStream_t s = as_stream(stream);
+  if (!pairs) {
+    const int grid = n_tiles * 16;
+    if (out_c128)
+      herk_reduce_all_kernel<double2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nant,
+                                                           nfeed, out, accumulate);
+    else
+      herk_reduce_all_kernel<float2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nant,
+                                                          nfeed, out, accumulate);
+  } else {
+    if (npairs == 0) return MVB_OK;
+    const int64_t total = npairs * nfeed * nfeed;
+    const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), (int64_t)num_sms() * 8);
+    if (out_c128)
+      herk_reduce_pairs_kernel<double2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
+                                                                         k_chunk, nfeed, pairs, npairs, out,
+                                                                         accumulate);
+    else
+      herk_reduce_pairs_kernel<float2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
+                                                                        k_chunk, nfeed, pairs, npairs, out,
+                                                                        accumulate);
+  }
+  return check_launch("herk_reduce");
+}

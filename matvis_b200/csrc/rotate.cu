@@ -1,0 +1,180 @@
+// A3 / A4: FP64 rotation of source unit vectors to topocentric ENU and the
+// strict z > 0 horizon selection with ascending kept indices.
+//
+// Reference: coordinates.py:91-125 (eci_to_enu_matrix), :174-200
+// (point_source_crd_eq), core/coords.py:99-150 (select_chunk).
+//
+// The rotation evaluates (R[r,0]*x + R[r,1]*y) + R[r,2]*z with every multiply and
+// add rounded on its own (__dmul_rn / __dadd_rn forbid FMA contraction), the
+// same operation sequence as the FP64 oracle, so the kept set is bit-identical.
+//
+// Compaction is two wait-free launches over blocks of 1024 sources: a count pass
+// (ballot + popc) and a scatter pass in which each block sums the counts of the
+// blocks before it, then ranks its own sources with warp ballots.  No block
+// waits on another, so there is no inter-block spin.
+#include "common.cuh"
+
+namespace mvb {
+
+struct Rot3 {
+  double r[9];
+};
+
+__global__ void rotate_kernel(const double *__restrict__ eci, int64_t n, Rot3 R, double *__restrict__ topo) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = eci[i], y = eci[n + i], z = eci[2 * n + i];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const double a = __dmul_rn(R.r[3 * r + 0], x);
+      const double b = __dmul_rn(R.r[3 * r + 1], y);
+      const double c = __dmul_rn(R.r[3 * r + 2], z);
+      topo[r * n + i] = __dadd_rn(__dadd_rn(a, b), c);
+    }
+  }
+}
+
+constexpr int kCompactThreads = 256;
+constexpr int kCompactPerThread = 4;
+constexpr int kCompactBlock = kCompactThreads * kCompactPerThread;  // sources per block
+
+__global__ void __launch_bounds__(kCompactThreads) horizon_count_kernel(const double *__restrict__ zrow, int64_t count,
+                                                                         int32_t *__restrict__ block_counts) {
+  __shared__ int warp_tot[kCompactThreads / 32];
+  const int64_t base = (int64_t)blockIdx.x * kCompactBlock;
+  int mine = 0;
+#pragma unroll
+  for (int j = 0; j < kCompactPerThread; ++j) {
+    const int64_t i = base + j * kCompactThreads + threadIdx.x;
+    mine += (i < count && zrow[i] > 0.0) ? 1 : 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = mine;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < kCompactThreads / 32; ++w) s += warp_tot[w];
+    block_counts[blockIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(kCompactThreads)
+    horizon_scatter_kernel(const double *__restrict__ topo, int64_t ld, int64_t c0, int64_t count,
+                           const int32_t *__restrict__ block_counts, int nblocks, const double *__restrict__ flux,
+                           double *__restrict__ crd_out, int32_t *__restrict__ idx_out, double *__restrict__ flux_out,
+                           int32_t *__restrict__ n_out, int64_t cap, int32_t *__restrict__ status) {
+  __shared__ long long red_before[kCompactThreads / 32];
+  __shared__ long long red_total[kCompactThreads / 32];
+  __shared__ int warp_cnt[kCompactThreads / 32];
+  __shared__ int warp_off[kCompactThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  // counts of earlier blocks, and the grand total
+  long long before = 0, total = 0;
+  for (int b = threadIdx.x; b < nblocks; b += kCompactThreads) {
+    const long long c = block_counts[b];
+    total += c;
+    if (b < (int)blockIdx.x) before += c;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    before += __shfl_xor_sync(0xffffffffu, before, o);
+    total += __shfl_xor_sync(0xffffffffu, total, o);
+  }
+  if (lane == 0) {
+    red_before[warp] = before;
+    red_total[warp] = total;
+  }
+  __syncthreads();
+  before = 0;
+  total = 0;
+  for (int w = 0; w < kCompactThreads / 32; ++w) {
+    before += red_before[w];
+    total += red_total[w];
+  }
+
+  const double *xr = topo + c0;
+  const double *yr = topo + ld + c0;
+  const double *zr = topo + 2 * ld + c0;
+  const int64_t base = (int64_t)blockIdx.x * kCompactBlock;
+  long long run = before;
+  if ((int)blockIdx.x < nblocks) {
+    for (int j = 0; j < kCompactPerThread; ++j) {
+      const int64_t i = base + j * kCompactThreads + threadIdx.x;
+      const bool keep = i < count && zr[i] > 0.0;
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) warp_cnt[warp] = __popc(m);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int s = 0;
+        for (int w = 0; w < kCompactThreads / 32; ++w) {
+          warp_off[w] = s;
+          s += warp_cnt[w];
+        }
+      }
+      __syncthreads();
+      if (keep) {
+        const long long pos = run + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
+        if (pos < cap) {
+          crd_out[pos] = xr[i];
+          crd_out[cap + pos] = yr[i];
+          crd_out[2 * cap + pos] = zr[i];
+          idx_out[pos] = (int32_t)(c0 + i);
+          if (flux != nullptr) flux_out[pos] = flux[c0 + i];
+        }
+      }
+      run += warp_off[kCompactThreads / 32 - 1] + warp_cnt[kCompactThreads / 32 - 1];
+      __syncthreads();
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *n_out = (int32_t)total;
+    if (total > cap && status != nullptr) atomicOr(status, MVB_DEV_OVERFLOW);
+  }
+  // zero the flux tail [total, cap)
+  if (flux != nullptr) {
+    for (long long i = total + (long long)blockIdx.x * kCompactThreads + threadIdx.x; i < cap;
+         i += (long long)gridDim.x * kCompactThreads)
+      flux_out[i] = 0.0;
+  }
+}
+
+}  // namespace mvb
+
+using namespace mvb;
+
+extern "C" int mvb_rotate(const double *eci, int64_t N, const double *R, double *topo, void *stream) {
+  if (N < 0 || (N > 0 && (!eci || !topo)) || !R) return fail(MVB_ERR_ARG, "mvb_rotate: bad arguments");
+  if (N == 0) return MVB_OK;
+  Rot3 r;
+  for (int i = 0; i < 9; ++i) r.r[i] = R[i];
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>(ceil_div(N, threads), (int64_t)num_sms() * 16);
+  rotate_kernel<<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(eci, N, r, topo);
+  return check_launch("rotate_kernel");
+}
+
+extern "C" size_t mvb_horizon_ws_bytes(int64_t count) {
+  return (size_t)std::max<int64_t>(1, ceil_div(std::max<int64_t>(count, 0), kCompactBlock)) * sizeof(int32_t);
+}
+
+extern "C" int mvb_horizon_compact(const double *topo, int64_t ld, int64_t c0, int64_t c1, const double *flux,
+                                   double *crd_out, int32_t *idx_out, double *flux_out, int32_t *n_out, int64_t cap,
+                                   int32_t *status, void *ws, size_t ws_bytes, void *stream) {
+  const int64_t count = c1 - c0;
+  if (count < 0 || c0 < 0 || c1 > ld || cap < 0 || !n_out || !ws || (count > 0 && !topo) ||
+      (cap > 0 && (!crd_out || !idx_out)) || (flux && cap > 0 && !flux_out))
+    return fail(MVB_ERR_ARG, "mvb_horizon_compact: bad arguments");
+  if (count > INT32_MAX) return fail(MVB_ERR_ARG, "mvb_horizon_compact: chunk too large");
+  if (ws_bytes < mvb_horizon_ws_bytes(count)) return fail(MVB_ERR_ARG, "mvb_horizon_compact: workspace too small");
+  const int nblocks = (int)ceil_div(count, kCompactBlock);
+  int32_t *counts = static_cast<int32_t *>(ws);
+  cudaStream_t s = as_stream(stream);
+  if (nblocks > 0) {
+    horizon_count_kernel<<<nblocks, kCompactThreads, 0, s>>>(topo + 2 * ld + c0, count, counts);
+    int rc = check_launch("horizon_count_kernel");
+    if (rc) return rc;
+  }
+  const int grid = std::max(nblocks, 1);
+  horizon_scatter_kernel<<<grid, kCompactThreads, 0, s>>>(topo, ld, c0, count, counts, nblocks, flux, crd_out, idx_out,
+                                                         flux_out, n_out, cap, status);
+  return check_launch("horizon_scatter_kernel");
+}

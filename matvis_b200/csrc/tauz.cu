@@ -1,0 +1,333 @@
+// A6: phase term and Z matrix.
+//
+// Reference: core/tau.py:30-31, 48-71 (exptau = exp(+i 2 pi nu / c * D . X), the
+// sign the code uses), core/getz.py:52-105 (Z[a, f, x, s] = exptau[a, s] *
+// sqrt_flux[s] * beam[beam_idx[a], f, x, s], rows a * nfeed + f, columns
+// x * nsrc + s).
+//
+// Phase: t = (nu / c) (D . X) in cycles, evaluated in FP64 and reduced to
+// r = t - rint(t) in [-1/2, 1/2] before an FP32 sincospi(2 r); at 1 km and
+// 200 MHz |t| reaches 670 cycles, where an FP32 phase would carry 2.4e-4 rad of
+// error.  Z columns are ordered k = s * nax + x (the source sum is the same).
+//
+// Split formats (the operand of the tensor-core Hermitian product):
+//   bf16, P terms: t0 = bf16_rn(v), t1 = bf16_rn(v - t0), t2 = bf16_rn(v - t0 - t1)
+//   tf32, 2 terms: t0 = tf32_rna(v), t1 = tf32_rna(v - t0)
+// each residual being exact in FP32.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace mvb {
+
+constexpr double kInvC = 1.0 / 299792458.0;
+
+__device__ __forceinline__ float tf32_rna(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return __uint_as_float(r);
+}
+
+// Writes X consecutive values (one per axis) of the P split terms of one real
+// component into planes [2p + comp] of a panel row.
+template <int MODE>
+struct PanelWriter {
+  static constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
+  static __device__ __forceinline__ void put(void *z, int64_t plane_stride, int64_t off, int comp, const float *v,
+                                             int X) {
+    if constexpr (MODE == MVB_GEMM_TF32_3) {
+      float *zp = static_cast<float *>(z) + off;
+      float hi[2], lo[2];
+      for (int x = 0; x < X; ++x) {
+        hi[x] = tf32_rna(v[x]);
+        lo[x] = tf32_rna(v[x] - hi[x]);
+      }
+      float *p0 = zp + (2 * 0 + comp) * plane_stride;
+      float *p1 = zp + (2 * 1 + comp) * plane_stride;
+      if (X == 2) {
+        *reinterpret_cast<float2 *>(p0) = make_float2(hi[0], hi[1]);
+        *reinterpret_cast<float2 *>(p1) = make_float2(lo[0], lo[1]);
+      } else {
+        *p0 = hi[0];
+        *p1 = lo[0];
+      }
+    } else {
+      __nv_bfloat16 *zp = static_cast<__nv_bfloat16 *>(z) + off;
+      __nv_bfloat16 t[3][2];
+      for (int x = 0; x < X; ++x) {
+        float r = v[x];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          t[p][x] = __float2bfloat16_rn(r);
+          r = r - __bfloat162float(t[p][x]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        __nv_bfloat16 *pp = zp + (2 * p + comp) * plane_stride;
+        if (X == 2) {
+          __nv_bfloat162 two;
+          two.x = t[p][0];
+          two.y = t[p][1];
+          *reinterpret_cast<__nv_bfloat162 *>(pp) = two;
+        } else {
+          *pp = t[p][0];
+        }
+      }
+    }
+  }
+};
+
+constexpr int kTauZThreads = 128;
+constexpr int kTauZAnts = 8;     // antennas per CTA
+constexpr int kTauZMaxBFX = 16;  // nbeam * F * X staged per source
+
+// grid.x: source blocks of kTauZThreads, grid.y: antenna blocks.
+// EXT = 0: phase from antpos . crd (fused tau); EXT = 1 / 2: phase factor read
+// from a caller exptau (A, e_ld) in complex64 / complex128, multiplied by sflux.
+template <int MODE, int EXT = 0>
+__global__ void __launch_bounds__(kTauZThreads)
+    tau_z_kernel(const double *__restrict__ antpos, int A, double f_over_c, const double *__restrict__ crd, int64_t ld,
+                 const int32_t *__restrict__ n_dev, int64_t nsrc, const float *__restrict__ sflux,
+                 const int32_t *__restrict__ sidx, const float2 *__restrict__ beam, int64_t beam_ld, int nbeam,
+                 const int32_t *__restrict__ beam_idx, int F, int X, void *__restrict__ z, int64_t Mpad,
+                 int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
+  __shared__ float2 bsm[kTauZMaxBFX][kTauZThreads];
+  const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
+  const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
+  const int64_t s = (int64_t)blockIdx.x * kTauZThreads + threadIdx.x;
+  if ((int64_t)blockIdx.x * kTauZThreads >= s_end) return;  // uniform per CTA
+  const bool live = s < n;
+  const bool write = s < s_end;
+
+  double cx = 0, cy = 0, cz = 0;
+  float sf = 0.f;
+  if (live) {
+    if (EXT == 0) {
+      cx = crd[s];
+      cy = crd[ld + s];
+      cz = crd[2 * ld + s];
+    }
+    sf = sflux[sidx ? sidx[s] : s];
+  }
+  const int nbfx = nbeam * F * X;
+  for (int q = 0; q < nbfx; ++q) bsm[q][threadIdx.x] = live ? beam[(int64_t)q * beam_ld + s] : make_float2(0.f, 0.f);
+  // (each thread reads only its own column of bsm: no barrier needed)
+
+  const int a0 = blockIdx.y * kTauZAnts;
+  const int a1 = min(a0 + kTauZAnts, A);
+  const int64_t plane = Mpad * Kcap;
+  for (int a = a0; a < a1; ++a) {
+    float er = 0.f, ei = 0.f;
+    if (live && EXT == 1) {
+      const float2 e = static_cast<const float2 *>(ext)[(int64_t)a * e_ld + s];
+      er = e.x * sf;
+      ei = e.y * sf;
+    } else if (live && EXT == 2) {
+      const double2 e = static_cast<const double2 *>(ext)[(int64_t)a * e_ld + s];
+      er = (float)(e.x * (double)sf);
+      ei = (float)(e.y * (double)sf);
+    } else if (live) {
+      const double dx = antpos[3 * a], dy = antpos[3 * a + 1], dz = antpos[3 * a + 2];
+      const double t = (dx * cx + dy * cy + dz * cz) * f_over_c;
+      const double r = t - rint(t);
+      float sn, cs;
+      sincospif((float)(2.0 * r), &sn, &cs);
+      er = cs * sf;
+      ei = sn * sf;
+    }
+    const int b = beam_idx ? beam_idx[a] : 0;
+    for (int f = 0; f < F; ++f) {
+      float vr[2], vi[2];
+      for (int x = 0; x < X; ++x) {
+        const float2 bv = bsm[(b * F + f) * X + x][threadIdx.x];
+        vr[x] = er * bv.x - ei * bv.y;
+        vi[x] = er * bv.y + ei * bv.x;
+      }
+      if (!write) continue;
+      const int64_t m = (int64_t)a * F + f;
+      const int64_t off = m * Kcap + s * X;
+      if constexpr (MODE == MVB_Z_C64) {
+        float2 *zp = static_cast<float2 *>(z) + off;
+        if (X == 2)
+          *reinterpret_cast<float4 *>(zp) = make_float4(vr[0], vi[0], vr[1], vi[1]);
+        else
+          *zp = make_float2(vr[0], vi[0]);
+      } else {
+        PanelWriter<MODE>::put(z, plane, off, 0, vr, X);
+        PanelWriter<MODE>::put(z, plane, off, 1, vi, X);
+      }
+    }
+  }
+}
+
+__global__ void exptau_kernel(const double *__restrict__ antpos, int A, double f_over_c, const double *__restrict__ crd,
+                              int64_t ld, int64_t nsrc, void *__restrict__ out, int out_c128) {
+  const int64_t total = (int64_t)A * nsrc;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = i / nsrc, s = i % nsrc;
+    const double t = (antpos[3 * a] * crd[s] + antpos[3 * a + 1] * crd[ld + s] + antpos[3 * a + 2] * crd[2 * ld + s]) *
+                     f_over_c;
+    const double r = t - rint(t);
+    if (out_c128) {
+      double sn, cs;
+      sincospi(2.0 * r, &sn, &cs);
+      static_cast<double2 *>(out)[i] = make_double2(cs, sn);
+    } else {
+      float sn, cs;
+      sincospif((float)(2.0 * r), &sn, &cs);
+      static_cast<float2 *>(out)[i] = make_float2(cs, sn);
+    }
+  }
+}
+
+// Packs a caller complex matrix (M, K) into a panel; one thread per (m, k-pair).
+template <int MODE, typename CT>
+__global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, int64_t ldz, void *__restrict__ z,
+                              int64_t Mpad, int64_t Kcap) {
+  const int64_t kend = round_up(K, kKAlign);
+  const int64_t half = kend / 2;
+  const int64_t total = M * half;
+  const int64_t plane = Mpad * Kcap;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = i / half, k = (i % half) * 2;
+    float vr[2], vi[2];
+    for (int x = 0; x < 2; ++x) {
+      if (k + x < K) {
+        const CT v = zs[m * ldz + k + x];
+        vr[x] = (float)v.x;
+        vi[x] = (float)v.y;
+      } else {
+        vr[x] = vi[x] = 0.f;
+      }
+    }
+    const int64_t off = m * Kcap + k;
+    if constexpr (MODE == MVB_Z_C64) {
+      *reinterpret_cast<float4 *>(static_cast<float2 *>(z) + off) = make_float4(vr[0], vi[0], vr[1], vi[1]);
+    } else {
+      PanelWriter<MODE>::put(z, plane, off, 0, vr, 2);
+      PanelWriter<MODE>::put(z, plane, off, 1, vi, 2);
+    }
+  }
+}
+
+}  // namespace mvb
+
+using namespace mvb;
+
+extern "C" size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap) {
+  if (mode == MVB_Z_C64) return (size_t)Mpad * Kcap * 8;
+  return (size_t)2 * mode_terms(mode) * Mpad * Kcap * mode_elem_bytes(mode);
+}
+
+static int check_panel(int mode, int64_t M, int64_t Mpad, int64_t Kcap, const char *who) {
+  if (mode < MVB_GEMM_BF16_3 || mode > MVB_Z_C64) return fail(MVB_ERR_ARG, "%s: unknown mode %d", who, mode);
+  if (Kcap % kKAlign) return fail(MVB_ERR_ARG, "%s: Kcap must be a multiple of %d", who, kKAlign);
+  if (Mpad < M) return fail(MVB_ERR_ARG, "%s: Mpad < M", who);
+  if (mode != MVB_Z_C64 && Mpad % kTile) return fail(MVB_ERR_ARG, "%s: Mpad must be a multiple of %d", who, kTile);
+  return MVB_OK;
+}
+
+extern "C" int mvb_exptau(const double *antpos, int A, double freq, const double *crd, int64_t ld, int64_t nsrc,
+                          void *exptau, int out_c128, void *stream) {
+  if (A < 0 || nsrc < 0 || ((int64_t)A * nsrc > 0 && (!antpos || !crd || !exptau)))
+    return fail(MVB_ERR_ARG, "mvb_exptau: bad arguments");
+  const int64_t total = (int64_t)A * nsrc;
+  if (total == 0) return MVB_OK;
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>(ceil_div(total, threads), (int64_t)num_sms() * 16);
+  exptau_kernel<<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(antpos, A, freq * kInvC, crd, ld, nsrc, exptau,
+                                                                     out_c128);
+  return check_launch("exptau_kernel");
+}
+
+extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
+                         int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld,
+                         int nbeam, const int32_t *beam_idx, int F, int X, int mode, void *z, int64_t Mpad,
+                         int64_t Kcap, void *stream) {
+  if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !sflux || (nsrc > 0 && !crd) || (F != 1 && F != 2) ||
+      (X != 1 && X != 2) || nbeam <= 0 || nbeam * F * X > kTauZMaxBFX || beam_ld < nsrc)
+    return fail(MVB_ERR_ARG, "mvb_tau_z: bad arguments");
+  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z");
+  if (rc) return rc;
+  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z: Kcap too small for nsrc * nax");
+  const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
+  if (s_max == 0) return MVB_OK;
+  dim3 grid((unsigned)ceil_div(s_max, kTauZThreads), (unsigned)ceil_div(A, kTauZAnts));
+  const double foc = freq * kInvC;
+  const float2 *bm = static_cast<const float2 *>(beam);
+  cudaStream_t s = as_stream(stream);
+#define MVB_TAUZ(M)                                                                                                  \
+  tau_z_kernel<M><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, \
+                                                beam_idx, F, X, z, Mpad, Kcap)
+  switch (mode) {
+    case MVB_GEMM_BF16_3: MVB_TAUZ(MVB_GEMM_BF16_3); break;
+    case MVB_GEMM_BF16_6: MVB_TAUZ(MVB_GEMM_BF16_6); break;
+    case MVB_GEMM_TF32_3: MVB_TAUZ(MVB_GEMM_TF32_3); break;
+    default: MVB_TAUZ(MVB_Z_C64); break;
+  }
+#undef MVB_TAUZ
+  return check_launch("tau_z_kernel");
+}
+
+extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, void *z,
+                          int64_t Mpad, int64_t Kcap, void *stream) {
+  if (M < 0 || K < 0 || ldz < K || !z || (M * K > 0 && !zsrc)) return fail(MVB_ERR_ARG, "mvb_z_pack: bad arguments");
+  int rc = check_panel(mode, M, Mpad, Kcap, "mvb_z_pack");
+  if (rc) return rc;
+  if (round_up(K, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_z_pack: Kcap too small");
+  const int64_t total = M * (round_up(K, kKAlign) / 2);
+  if (total == 0) return MVB_OK;
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>(ceil_div(total, threads), (int64_t)num_sms() * 16);
+  cudaStream_t s = as_stream(stream);
+#define MVB_PACK(M_, CT)                                                                                             \
+  z_pack_kernel<M_, CT><<<(unsigned)blocks, threads, 0, s>>>(static_cast<const CT *>(zsrc), M, K, ldz, z, Mpad, Kcap)
+#define MVB_PACK2(M_) \
+  if (z_c128)         \
+    MVB_PACK(M_, double2); \
+  else                \
+    MVB_PACK(M_, float2)
+  switch (mode) {
+    case MVB_GEMM_BF16_3: MVB_PACK2(MVB_GEMM_BF16_3); break;
+    case MVB_GEMM_BF16_6: MVB_PACK2(MVB_GEMM_BF16_6); break;
+    case MVB_GEMM_TF32_3: MVB_PACK2(MVB_GEMM_TF32_3); break;
+    default: MVB_PACK2(MVB_Z_C64); break;
+  }
+#undef MVB_PACK2
+#undef MVB_PACK
+  return check_launch("z_pack_kernel");
+}
+
+extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, int A, int64_t nsrc, const float *sflux,
+                                 const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X,
+                                 int mode, void *z, int64_t Mpad, int64_t Kcap, void *stream) {
+  if (A <= 0 || nsrc < 0 || !exptau || !z || !beam || !sflux || (F != 1 && F != 2) || (X != 1 && X != 2) ||
+      nbeam <= 0 || nbeam * F * X > kTauZMaxBFX || beam_ld < nsrc || e_ld < nsrc)
+    return fail(MVB_ERR_ARG, "mvb_z_from_exptau: bad arguments");
+  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_z_from_exptau");
+  if (rc) return rc;
+  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_z_from_exptau: Kcap too small");
+  const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
+  if (s_max == 0) return MVB_OK;
+  dim3 grid((unsigned)ceil_div(s_max, kTauZThreads), (unsigned)ceil_div(A, kTauZAnts));
+  const float2 *bm = static_cast<const float2 *>(beam);
+  cudaStream_t s = as_stream(stream);
+#define MVB_ZX(M, E)                                                                                                  \
+  tau_z_kernel<M, E><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, nullptr, bm,     \
+                                                   beam_ld, nbeam, beam_idx, F, X, z, Mpad, Kcap, exptau, e_ld)
+#define MVB_ZX2(M) \
+  if (e_c128)      \
+    MVB_ZX(M, 2);  \
+  else             \
+    MVB_ZX(M, 1)
+  switch (mode) {
+    case MVB_GEMM_BF16_3: MVB_ZX2(MVB_GEMM_BF16_3); break;
+    case MVB_GEMM_BF16_6: MVB_ZX2(MVB_GEMM_BF16_6); break;
+    case MVB_GEMM_TF32_3: MVB_ZX2(MVB_GEMM_TF32_3); break;
+    default: MVB_ZX2(MVB_Z_C64); break;
+  }
+#undef MVB_ZX2
+#undef MVB_ZX
+  return check_launch("tau_z_kernel(exptau)");
+}

@@ -1,0 +1,229 @@
+"""Batched visibility engine: every (frequency, time) slice of a job on one GPU.
+
+The reference runs ``simulate`` once per frequency (wrapper.py:180-199) and,
+inside it, rotation -> horizon selection -> beam -> tau -> Z -> product per time
+and chunk with a device synchronisation after each stage (cpu/cpu.py:247-272,
+gpu/gpu.py:197-254).  Here one job is one stream of launches:
+
+    for t:      mvb_rotate -> (per chunk) mvb_horizon_compact -> mvb_beam_*
+      for f:    mvb_tau_z -> mvb_herk + mvb_herk_reduce   (or mvb_vecdot)
+
+Rotation, selection and beam interpolation depend on time only and are done once
+per time for all frequencies.  The above-horizon count never leaves the device:
+every later kernel reads it from ``n_above`` and sizes its work from it, so the
+whole job can be captured once as a CUDA graph and replayed.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .beams import B200BeamInterpolator, GaussianBeam, GridBeam
+from .coordinates import eci_to_enu_matrix, point_source_crd_eq
+from .getz import ZMatrixCalc
+from .matprod import B200MatMul, B200VectorDot, choose_k_chunk
+
+
+@dataclass
+class JobSpec:
+    antpos: np.ndarray  # (A, 3) metres
+    eci: np.ndarray  # (3, N) unit vectors
+    fluxes: np.ndarray  # (N, Nf) Stokes I
+    freqs: np.ndarray  # (Nf,) Hz
+    lsts: np.ndarray  # (Nt,) radians
+    latitude: float  # radians
+    beams: list
+    beam_idx: np.ndarray | None = None
+    polarized: bool = False
+    antpairs: np.ndarray | None = None
+    precision: int = 1
+    gemm_mode: str = "bf16x6"
+    matprod: str = "MatMul"  # or "VectorDot"
+    k_chunk: int | None = None
+    source_buffer: float = 1.0
+    nchunks: int = 1
+
+
+def _norm_matprod(name: str) -> str:
+    n = str(name)
+    for p in ("B200", "GPU", "CPU"):
+        if n.startswith(p):
+            n = n[len(p):]
+    if n in ("MatMul",):
+        return "MatMul"
+    if n in ("VectorDot", "VectorLoop"):
+        return "VectorDot"
+    raise ValueError(f"unknown matprod_method {name!r}")
+
+
+class VisEngine:
+    """Device-resident state and launch sequence of one job."""
+
+    def __init__(self, spec: JobSpec, device=None):
+        self.spec = spec
+        self.device = _lib.require_cuda(device)
+        s = spec
+        self.antpos_host = np.ascontiguousarray(np.asarray(s.antpos, dtype=np.float64))
+        self.nant = self.antpos_host.shape[0]
+        self.nfeed = self.nax = 2 if s.polarized else 1
+        self.eci_host = np.ascontiguousarray(np.asarray(s.eci, dtype=np.float64))
+        self.nsrc = self.eci_host.shape[1]
+        self.freqs = np.asarray(s.freqs, dtype=np.float64)
+        self.lsts = np.asarray(s.lsts, dtype=np.float64)
+        fl = np.asarray(s.fluxes, dtype=np.float64)
+        if fl.shape != (self.nsrc, len(self.freqs)):
+            raise ValueError("The `fluxes` array must have shape (NSRCS, NFREQS).")
+        # sqrt(0.5 I) per frequency (cpu/cpu.py:188), frequency-major, float32
+        self.sflux_host = np.ascontiguousarray(np.sqrt(0.5 * fl).T.astype(np.float32))
+        self.method = _norm_matprod(s.matprod)
+        self.nchunks = max(1, int(s.nchunks))
+        self.chunk_size = int(np.ceil(self.nsrc / self.nchunks)) if self.nsrc else 1
+        if not 0 < s.source_buffer <= 1:
+            raise ValueError("source_buffer must satisfy 0 < source_buffer <= 1")
+        self.cap = int(self.chunk_size * s.source_buffer) if self.chunk_size > 1000 else self.chunk_size
+        self.cap = max(self.cap, 1)
+        self.ctype = torch.complex64 if s.precision == 1 else torch.complex128
+        self.rot = np.stack([eci_to_enu_matrix(l, s.latitude) for l in self.lsts]) if len(self.lsts) else np.zeros((0, 3, 3))
+        self._graph = None
+        self._allocated = False
+
+    # ------------------------------------------------------------------ setup
+    def allocate(self):
+        dev = self.device
+        s = self.spec
+        A, N = self.nant, self.nsrc
+        self.eci = torch.empty((3, N), dtype=torch.float64, device=dev)
+        self.antpos = torch.empty((A, 3), dtype=torch.float64, device=dev)
+        self.sflux = torch.empty((len(self.freqs), N), dtype=torch.float32, device=dev)
+        self.topo = torch.zeros((3, N), dtype=torch.float64, device=dev)
+        self.crd = torch.zeros((3, self.cap), dtype=torch.float64, device=dev)
+        self.kept = torch.zeros((self.cap,), dtype=torch.int32, device=dev)
+        self.n_above = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ws_compact = torch.empty(_lib.lib.mvb_horizon_ws_bytes(self.chunk_size), dtype=torch.uint8, device=dev)
+        self.bmfunc = B200BeamInterpolator(
+            beam_list=s.beams, beam_idx=s.beam_idx, polarized=s.polarized, nant=A, freq=float(self.freqs[0]) if len(self.freqs) else 0.0,
+            nsrc=self.cap, precision=1, device=dev,
+        )
+        self.bmfunc.setup()
+        if self.method == "MatMul":
+            self.matprod = B200MatMul(1, self.nfeed, A, s.antpairs, precision=s.precision, gemm_mode=s.gemm_mode,
+                                      k_chunk=s.k_chunk, device=dev)
+            zmode = self.matprod.mode
+        else:
+            pairs = s.antpairs if s.antpairs is not None else np.array([(i, j) for i in range(A) for j in range(A)])
+            self.matprod = B200VectorDot(1, self.nfeed, A, pairs, precision=s.precision,
+                                         k_chunk=s.k_chunk or 4096, device=dev)
+            zmode = _lib.Z_C64
+        self.matprod.setup()
+        self.matprod.status = self.status
+        self.zcalc = ZMatrixCalc(A, self.nfeed, self.nax, self.cap, mode=zmode, device=dev)
+        self.zcalc.setup()
+        self.npairs = self.matprod.npairs
+        self.vis = torch.zeros((len(self.freqs), len(self.lsts), self.npairs, self.nfeed, self.nfeed), dtype=self.ctype,
+                               device=dev)
+        if self.method == "MatMul":
+            panel = self.zcalc.z
+            self.k_chunk = self.matprod.resolve_k_chunk(panel)
+            self.matprod.workspace(panel, self.k_chunk)
+        self._allocated = True
+
+    def upload(self, stream=None):
+        """Host -> device copies of the job inputs (pinned staging when possible)."""
+        if not self._allocated:
+            self.allocate()
+        self.eci.copy_(torch.from_numpy(self.eci_host), non_blocking=False)
+        self.antpos.copy_(torch.from_numpy(self.antpos_host))
+        self.sflux.copy_(torch.from_numpy(self.sflux_host))
+
+    def h2d_bytes(self) -> int:
+        return self.eci_host.nbytes + self.antpos_host.nbytes + self.sflux_host.nbytes
+
+    # ----------------------------------------------------------------- launch
+    def enqueue(self, stream=None):
+        """Enqueue every kernel of the job on ``stream`` (no host synchronisation)."""
+        L = _lib.lib
+        sh = _lib.stream_handle(stream)
+        chk = _lib.check
+        A = self.nant
+        F, X = self.nfeed, self.nax
+        panel = self.zcalc.z
+        for t in range(len(self.lsts)):
+            R = np.ascontiguousarray(self.rot[t])
+            chk(L.mvb_rotate(_lib.ptr(self.eci), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
+            for c in range(self.nchunks):
+                c0 = min(c * self.chunk_size, self.nsrc)
+                c1 = min((c + 1) * self.chunk_size, self.nsrc)
+                chk(L.mvb_horizon_compact(
+                    _lib.ptr(self.topo), self.nsrc, c0, c1, None, _lib.ptr(self.crd), _lib.ptr(self.kept), None,
+                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.status), _lib.ptr(self.ws_compact),
+                    self.ws_compact.numel(), sh))
+                self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, self.bmfunc.interpolated_beam,
+                                   stream=stream, status=self.status)
+                beam = self.bmfunc.interpolated_beam
+                for f in range(len(self.freqs)):
+                    chk(L.mvb_tau_z(
+                        _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
+                        _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f]), _lib.ptr(self.kept), _lib.ptr(beam),
+                        beam.shape[-1], beam.shape[0], _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode,
+                        _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
+                    panel.n_dev = self.n_above
+                    panel.n_host = self.cap
+                    out = self.vis[f, t]
+                    if self.method == "MatMul":
+                        self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream, k_chunk=self.k_chunk)
+                    else:
+                        self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream)
+
+    def launches_per_run(self) -> int:
+        per_f = 3 if self.method == "MatMul" else 2
+        per_chunk = 3 + per_f * len(self.freqs)  # count + scatter + beam, then per frequency
+        return len(self.lsts) * (1 + self.nchunks * per_chunk)
+
+    def run(self, check: bool = True) -> torch.Tensor:
+        """Run the job on the current stream; returns the device visibilities."""
+        if not self._allocated:
+            self.upload()
+        self.status.zero_()
+        if self._graph is not None:
+            self._graph.replay()
+        else:
+            self.enqueue()
+        if check:
+            torch.cuda.current_stream().synchronize()
+            _lib.check_status_word(self.status, "VisEngine")
+        return self.vis
+
+    def capture(self):
+        """Capture the launch sequence as one CUDA graph (run once uncaptured first)."""
+        if not self._allocated:
+            self.upload()
+        self.enqueue()  # warm-up: function attributes, lazy module loading
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.enqueue(stream=s)
+        torch.cuda.current_stream().wait_stream(s)
+        self._graph = g
+        return g
+
+    def result(self, polarized: bool | None = None) -> torch.Tensor:
+        pol = self.spec.polarized if polarized is None else polarized
+        return self.vis if pol else self.vis[..., 0, 0]
+
+
+def job_from_arrays(*, ants, fluxes, ra, dec, freqs, lsts, latitude, beams, **kw) -> JobSpec:
+    """JobSpec from the simulate_vis-style inputs (ants dict, ra/dec in radians)."""
+    if isinstance(ants, dict):
+        antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
+    else:
+        antpos = np.asarray(ants, dtype=np.float64)
+    return JobSpec(antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=np.asarray(fluxes), freqs=np.asarray(freqs),
+                   lsts=np.asarray(lsts), latitude=float(latitude), beams=list(beams), **kw)

@@ -1,0 +1,200 @@
+"""Source-summing plugins (mirror ``matvis.core.matprod.MatProd`` and its backends).
+
+* :class:`B200MatMul` -- upper-triangle Hermitian product on the tcgen05 tensor
+  cores (``mvb_herk`` + ``mvb_herk_reduce``); replaces CPUMatMul / GPUMatMul
+  (cpu/matprod.py:8-32, gpu/matprod.py:10-63).
+* :class:`B200VectorDot` -- per-pair warp reduction (``mvb_vecdot``); replaces
+  CPUVectorDot / GPUVectorDot (cpu/matprod.py:35-53, gpu/matprod.py:66-98).
+
+Output layout (npairs, nfeed, nfeed) with out[i, p, q] pairing feed q of ant1 with
+feed p of ant2, the reference's transposed feed convention (tests/test_matprod.py:57-65).
+"""
+
+from __future__ import annotations
+
+from abc import ABC, abstractmethod
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr, stream_handle
+from .getz import ZPanel
+
+
+def choose_k_chunk(n_tiles: int, kvalid: int, num_sms: int = 148, lo: int = 1024, hi: int = 8192) -> int:
+    """k-slice length of the Hermitian product.
+
+    Enough slices that every SM gets about two work units, no shorter than
+    ``lo`` columns (partial-tile traffic) and no longer than ``hi`` (FP32
+    accumulation length in TMEM before the FP64 reduction).
+    """
+    want_units = 2 * num_sms
+    slices = max(1, -(-want_units // max(n_tiles, 1)))
+    kc = -(-max(kvalid, 1) // slices)
+    kc = -(-kc // _lib.K_ALIGN) * _lib.K_ALIGN
+    return int(min(max(kc, lo), hi))
+
+
+def _pairs_tensor(antpairs, device):
+    if antpairs is None:
+        return None
+    a = np.ascontiguousarray(np.asarray(antpairs, dtype=np.int32).reshape(-1, 2))
+    return torch.as_tensor(a, device=device)
+
+
+class MatProd(ABC):
+    """Abstract source-summing operation; core/matprod.py:11-115."""
+
+    def __init__(self, nchunks: int, nfeed: int, nant: int, antpairs, precision=1, device=None):
+        self.device = _lib.require_cuda(device)
+        if antpairs is None:
+            self.all_pairs = True
+            self.antpairs = np.array([(i, j) for i in range(nant) for j in range(nant)])
+        else:
+            self.all_pairs = False
+            self.antpairs = np.asarray(antpairs)
+        self.nchunks = nchunks
+        self.nfeed = nfeed
+        self.nant = nant
+        self.npairs = len(self.antpairs)
+        self.precision = precision
+        self.ctype = torch.complex64 if precision == 1 else torch.complex128
+        self.ant1_idx = self.antpairs[:, 0] if self.npairs else np.zeros(0, int)
+        self.ant2_idx = self.antpairs[:, 1] if self.npairs else np.zeros(0, int)
+        self.status = None
+
+    def allocate_vis(self):
+        self.vis = torch.zeros((self.nchunks, self.npairs, self.nfeed, self.nfeed), dtype=self.ctype, device=self.device)
+
+    def setup(self):
+        self.allocate_vis()
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._pairs_dev = torch.as_tensor(
+            np.ascontiguousarray(self.antpairs.astype(np.int32).reshape(-1, 2)), device=self.device
+        )
+
+    @abstractmethod
+    def compute(self, z, out):
+        """Sum over sources of one (time, chunk) into ``out`` (npairs, nfeed, nfeed)."""
+
+    def __call__(self, z, chunk: int):
+        self.compute(z, out=self.vis[chunk])
+        return self.vis[chunk]
+
+    def sum_chunks(self, out):
+        """Sum the chunks into ``out`` (host array or device tensor)."""
+        tot = self.vis[0] if self.nchunks == 1 else self.vis.sum(dim=0)
+        if self.status is not None:
+            _lib.check_status_word(self.status, type(self).__name__)
+        if isinstance(out, torch.Tensor):
+            out.copy_(tot)
+        else:
+            out[:] = tot.cpu().numpy()
+
+    # -- helpers -------------------------------------------------------------
+    def _as_panel(self, z, mode: int) -> ZPanel:
+        if isinstance(z, ZPanel):
+            if z.mode != mode:
+                raise ValueError(f"Z panel mode {z.mode} does not match this product's mode {mode}")
+            return z
+        zt = torch.as_tensor(z, device=self.device)
+        if not torch.is_complex(zt) or zt.ndim != 2:
+            raise TypeError(f"invalid Z: expected a complex (nant*nfeed, K) matrix, got {zt.dtype} {tuple(zt.shape)}")
+        if zt.shape[0] != self.nant * self.nfeed:
+            raise ValueError("Z must have nant * nfeed rows")
+        if zt.dtype not in (torch.complex64, torch.complex128):
+            zt = zt.to(torch.complex128)
+        zt = zt.contiguous()
+        M, K = zt.shape
+        key = (mode, K)
+        panel = getattr(self, "_packed", {}).get(key)
+        if panel is None:
+            panel = ZPanel(mode, self.nant, self.nfeed, 1, K, self.device)
+            self._packed = {key: panel}
+        check(
+            _lib.lib.mvb_z_pack(
+                ptr(zt), 1 if zt.dtype == torch.complex128 else 0, M, K, K, mode, ptr(panel.data), panel.Mpad,
+                panel.Kcap, stream_handle(),
+            )
+        )
+        panel.n_dev = None
+        panel.n_host = K
+        return panel
+
+
+class B200MatMul(MatProd):
+    """Hermitian product V = conj(Z) Z^T, upper-triangle tiles on the tensor cores."""
+
+    def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, gemm_mode: str | int = "bf16x6",
+                 k_chunk: int | None = None, device=None):
+        super().__init__(nchunks, nfeed, nant, antpairs, precision=precision, device=device)
+        self.mode = _lib.GEMM_MODES[gemm_mode] if isinstance(gemm_mode, str) else int(gemm_mode)
+        if self.mode not in (_lib.GEMM_BF16_3, _lib.GEMM_BF16_6, _lib.GEMM_TF32_3):
+            raise ValueError(f"unknown gemm_mode {gemm_mode!r}")
+        self.k_chunk = k_chunk
+        self._ws = None
+
+    def workspace(self, panel: ZPanel, k_chunk: int) -> torch.Tensor:
+        nbytes = _lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, k_chunk)
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def resolve_k_chunk(self, panel: ZPanel) -> int:
+        if self.k_chunk is not None:
+            return int(self.k_chunk)
+        T = panel.Mpad // _lib.TILE
+        sm = torch.cuda.get_device_properties(self.device).multi_processor_count
+        return choose_k_chunk(T * (T + 1) // 2, panel.Kcap, sm)
+
+    def enqueue(self, panel: ZPanel, out: torch.Tensor, accumulate: bool = False, stream=None, k_chunk=None):
+        kc = k_chunk or self.resolve_k_chunk(panel)
+        ws = self.workspace(panel, kc)
+        sh = stream_handle(stream)
+        kmul = panel.nax
+        check(
+            _lib.lib.mvb_herk(
+                ptr(panel.data), self.mode, panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc, ptr(ws),
+                ws.numel(), ptr(self.status), sh,
+            )
+        )
+        pairs = None if self.all_pairs else self._pairs_dev
+        check(
+            _lib.lib.mvb_herk_reduce(
+                ptr(ws), panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc, self.nant, self.nfeed,
+                ptr(pairs), self.npairs, ptr(out), 1 if out.dtype == torch.complex128 else 0, int(accumulate), sh,
+            )
+        )
+
+    def compute(self, z, out):
+        panel = self._as_panel(z, self.mode)
+        self.enqueue(panel, out)
+        return out
+
+
+class B200VectorDot(MatProd):
+    """Per-pair source sums (warp reduction) for explicit pair lists."""
+
+    def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, k_chunk: int = 4096, device=None):
+        super().__init__(nchunks, nfeed, nant, antpairs, precision=precision, device=device)
+        self.mode = _lib.Z_C64
+        self.k_chunk = int(k_chunk)
+        self._ws = None
+
+    def enqueue(self, panel: ZPanel, out: torch.Tensor, accumulate: bool = False, stream=None):
+        nbytes = _lib.lib.mvb_vecdot_ws_bytes(self.npairs, self.nfeed, panel.Kcap, self.k_chunk)
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        check(
+            _lib.lib.mvb_vecdot(
+                ptr(panel.data), panel.Kcap, ptr(panel.n_dev), panel.n_host, panel.nax, self.nfeed,
+                ptr(self._pairs_dev), self.npairs, self.k_chunk, ptr(self._ws), self._ws.numel(), ptr(out),
+                1 if out.dtype == torch.complex128 else 0, int(accumulate), stream_handle(stream),
+            )
+        )
+
+    def compute(self, z, out):
+        panel = self._as_panel(z, self.mode)
+        self.enqueue(panel, out)
+        return out

@@ -1,0 +1,159 @@
+"""``simulate`` (one frequency) and ``simulate_vis`` (all frequencies).
+
+Keyword-compatible with ``matvis.cpu.simulate`` / ``matvis.gpu.simulate``
+(cpu/cpu.py:35-277, gpu/gpu.py:57-256) and ``matvis.simulate_vis``
+(wrapper.py:25-200), with these input conventions (astropy and pyuvdata are not
+dependencies):
+
+* ``times`` are local sidereal times in radians and ``telescope_loc`` is the
+  latitude in radians (or an object with ``.lat``); the rotation is the rigid
+  LST rotation (``coord_method="CoordinateRotationLST"``);
+* beams are :class:`~matvis_b200.beams.GridBeam` / :class:`~matvis_b200.beams.GaussianBeam`;
+* ``skycoords`` is an (ra, dec) pair in radians or an object with ``.ra``/``.dec``.
+
+Both run the batched engine (``engine.VisEngine``): every time and frequency of
+the call is one launch sequence on the GPU, with device-side source counts.
+"""
+
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._utils import get_desired_chunks
+from .coordinates import latitude_of, lsts_of, point_source_crd_eq, radec_of
+from .engine import JobSpec, VisEngine, _norm_matprod
+
+logger = logging.getLogger(__name__)
+
+_UNAVAILABLE_COORD = ("CoordinateRotationAstropy", "CoordinateRotationERFA", "GPUCoordinateRotationERFA")
+
+
+def _validate_inputs(precision, polarized, antpos, times, I_sky):
+    """core/__init__.py:11-32."""
+    assert precision in {1, 2}
+    nax = nfeed = 2 if polarized else 1
+    nant, ncrd = antpos.shape
+    assert ncrd == 3, "antpos must have shape (NANTS, 3)."
+    ntimes = len(times)
+    assert I_sky.ndim == 1, "I_sky must have shape (NSRCS,)."
+    return nax, nfeed, nant, ntimes
+
+
+def _check_coord_method(coord_method):
+    if coord_method in _UNAVAILABLE_COORD:
+        raise NotImplementedError(
+            f"{coord_method} needs astropy/ERFA time-dependent astrometry, which this build does not ship; "
+            "use coord_method='CoordinateRotationLST' with times given as LSTs (radians)"
+        )
+    if coord_method != "CoordinateRotationLST":
+        raise ValueError(f"unknown coord_method {coord_method!r}")
+
+
+def simulate(
+    *,
+    antpos,
+    freq: float,
+    times,
+    skycoords,
+    telescope_loc,
+    I_sky,
+    beam_list,
+    antpairs=None,
+    precision: int = 1,
+    polarized: bool = False,
+    beam_idx=None,
+    beam_spline_opts=None,
+    max_progress_reports: int = 100,
+    matprod_method: str = "B200MatMul",
+    coord_method: str = "CoordinateRotationLST",
+    max_memory=np.inf,
+    min_chunks: int = 1,
+    source_buffer: float = 1.0,
+    memory_buffer: float = 0.9,
+    coord_method_params=None,
+    gemm_mode: str = "bf16x6",
+    k_chunk: int | None = None,
+    device=None,
+):
+    """Visibilities at one frequency for all times; returns (Nt, Npairs, F, F) or (Nt, Npairs)."""
+    if not 0 < source_buffer <= 1:
+        raise ValueError("source_buffer must satisfy 0 < source_buffer <= 1")
+    if not 0 < memory_buffer <= 1:
+        raise ValueError("memory_buffer must satisfy 0 < memory_buffer <= 1")
+    _check_coord_method(coord_method)
+    dev = _lib.require_cuda(device)
+    antpos = np.asarray(antpos, dtype=np.float64)
+    I_sky = np.asarray(I_sky)
+    lsts = lsts_of(times)
+    nax, nfeed, nant, ntimes = _validate_inputs(precision, polarized, antpos, lsts, I_sky)
+    ra, dec = radec_of(skycoords)
+    free = torch.cuda.mem_get_info(dev)[0]
+    nchunks, _ = get_desired_chunks(min(max_memory, free), min_chunks, beam_list, nax, nfeed, nant, len(I_sky),
+                                    precision, source_buffer=source_buffer, memory_buffer=memory_buffer)
+    spec = JobSpec(
+        antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=I_sky[:, None], freqs=np.array([float(freq)]),
+        lsts=lsts, latitude=latitude_of(telescope_loc), beams=list(beam_list), beam_idx=beam_idx, polarized=polarized,
+        antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
+        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks,
+    )
+    eng = VisEngine(spec, device=dev)
+    vis = eng.run()[0]
+    out = vis.cpu().numpy()
+    return out if polarized else out[:, :, 0, 0]
+
+
+def simulate_vis(
+    ants,
+    fluxes,
+    ra,
+    dec,
+    freqs,
+    times,
+    beams,
+    telescope_loc,
+    polarized: bool = False,
+    precision: int = 1,
+    use_feed: str = "x",
+    use_gpu: bool = True,
+    beam_spline_opts=None,
+    beam_idx=None,
+    antpairs=None,
+    source_buffer: float = 1.0,
+    coord_method: str = "CoordinateRotationLST",
+    coord_method_params=None,
+    matprod_method: str = "MatMul",
+    gemm_mode: str = "bf16x6",
+    k_chunk: int | None = None,
+    min_chunks: int = 1,
+    device=None,
+    **backend_kwargs,
+):
+    """All frequencies and times; returns (Nf, Nt, Npairs, F, F) or (Nf, Nt, Npairs).
+
+    ``ants``: {index: (x, y, z)} in metres; ``fluxes``: (NSRCS, NFREQS);
+    ``ra``/``dec`` radians; ``freqs`` Hz; ``times`` LSTs (radians).
+    """
+    if not use_gpu:
+        raise ValueError("matvis_b200 runs on the GPU only (use_gpu=False has no CPU path here)")
+    _check_coord_method(coord_method)
+    fluxes = np.asarray(fluxes)
+    ra = np.asarray(ra, dtype=np.float64)
+    dec = np.asarray(dec, dtype=np.float64)
+    freqs = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
+    assert fluxes.shape == (ra.size, freqs.size), "The `fluxes` array must have shape (NSRCS, NFREQS)."
+    antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
+    if not 0 < source_buffer <= 1:
+        raise ValueError("source_buffer must satisfy 0 < source_buffer <= 1")
+    spec = JobSpec(
+        antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=fluxes, freqs=freqs, lsts=lsts_of(times),
+        latitude=latitude_of(telescope_loc), beams=list(beams), beam_idx=beam_idx, polarized=polarized,
+        antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
+        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=max(1, int(min_chunks)),
+    )
+    eng = VisEngine(spec, device=device)
+    vis = eng.run().cpu().numpy()
+    return vis if polarized else vis[..., 0, 0]

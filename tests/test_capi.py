@@ -1,0 +1,61 @@
+"""The C-ABI library loads and exports every symbol declared in include/*.h
+(no compute calls: these run without a GPU)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "matvis_b200.h"
+LIB = ROOT / "matvis_b200" / "libmatvis_b200.so"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mvb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("mvb_rotate", "mvb_horizon_compact", "mvb_beam_interp", "mvb_tau_z", "mvb_herk", "mvb_herk_reduce",
+              "mvb_vecdot"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    if not LIB.exists():
+        pytest.fail(f"{LIB} not built (python matvis_b200/build.py)")
+    lib = ctypes.CDLL(str(LIB))
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    from matvis_b200 import _lib
+
+    missing = [s for s in declared_symbols() if s not in _lib._SIGNATURES]
+    assert not missing, missing
+
+
+def test_workspace_queries_without_gpu():
+    from matvis_b200 import _lib
+
+    assert _lib.lib.mvb_version() == 1
+    assert _lib.lib.mvb_herk_ws_bytes(768, 393216, 2048) == 21 * 192 * 256 * 128 * 4
+    assert _lib.lib.mvb_zpanel_bytes(_lib.GEMM_BF16_6, 768, 393216) == 6 * 768 * 393216 * 2
+    assert _lib.lib.mvb_horizon_ws_bytes(196608) == 192 * 4
+    assert _lib.lib.mvb_vecdot_ws_bytes(10, 2, 4096, 1024) == 4 * 10 * 4 * 2 * 8
+
+
+def test_argument_errors_are_reported_without_gpu():
+    """Argument validation happens on the host, before any CUDA call."""
+    from matvis_b200 import _lib
+
+    rc = _lib.lib.mvb_herk(None, 0, 768, 100, None, 0, 1, 64, None, 0, None, None)
+    assert rc == _lib.MVB_ERR_ARG
+    assert b"mvb_herk" in _lib.lib.mvb_last_error()
+    with pytest.raises(ValueError):
+        _lib.check(rc)

@@ -1,0 +1,253 @@
+"""Kernel-level parity of the CUDA library against the FP64 oracle and the
+reference-generated fixtures (run on a B200: ``pytest -m gpu``).
+
+Tolerances (stated per test):
+* rotation and horizon selection: bit-exact (coordinates and kept indices);
+* beam interpolation: 1e-6 absolute against the FP64 result (grids are stored
+  in float32 on the device, the weights and blend are FP64);
+* exptau: 5e-7 absolute (complex64: FP64-reduced phase, FP32 sincospi),
+  1e-12 (complex128);
+* Hermitian product: max |dV| / sqrt(|V_ii| |V_jj|) <= 1e-6 for bf16x6 and
+  tf32x3, <= 3e-5 for bf16x3; integer-valued Z is exact in every mode.
+"""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import matvis_b200 as mv  # noqa: E402
+from matvis_b200 import _lib  # noqa: E402
+from oracle import oracle as orc  # noqa: E402
+
+from .conftest import golden  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def _cos_err(v, ref, nant, nfeed):
+    return orc.cosine_error_metric(np.asarray(v).reshape(-1, nfeed, nfeed), np.asarray(ref).reshape(-1, nfeed, nfeed), nfeed)
+
+
+# ---------------------------------------------------------------- rotation
+@pytest.mark.parametrize("nsrc", [1, 1000, 4097, 196608])
+def test_rotate_and_compact_bitexact(device, nsrc):
+    rng = np.random.default_rng(nsrc)
+    ra, dec = rng.uniform(0, 2 * np.pi, nsrc), np.arcsin(rng.uniform(-1, 1, nsrc))
+    eci = orc.point_source_crd_eq(ra, dec)
+    flux = np.sqrt(0.5 * rng.uniform(0.1, 10, nsrc))
+    lat = np.deg2rad(-30.72)
+    rot = mv.CoordinateRotationLST(flux=flux, times=np.array([0.3, 2.5]), telescope_loc=lat, skycoords=(ra, dec),
+                                   source_buffer=1.0)
+    rot.setup()
+    for t, lst in enumerate(rot.times):
+        rot.rotate(t)
+        ref_top = orc.rotate_fixed_order(orc.eci_to_enu_matrix(lst, lat), eci)
+        np.testing.assert_array_equal(rot.all_coords_topo.cpu().numpy(), ref_top)
+        crd, fl, n = rot.select_chunk(0, t)
+        rc, rf, rn, kept = orc.select_chunk(ref_top, flux, 0, nsrc, rot.nsrc_alloc)
+        assert n == rn
+        np.testing.assert_array_equal(rot.kept_index[:n].cpu().numpy(), kept)
+        np.testing.assert_array_equal(crd[:, :n].cpu().numpy(), rc[:, :n])
+        np.testing.assert_array_equal(fl.cpu().numpy(), rf)
+
+
+def test_select_chunk_matches_reference_fixture(device):
+    g = golden("coords")
+    eci, flux = g["sel_eci"], g["sel_flux"]
+    ra = np.arctan2(eci[1], eci[0])
+    dec = np.arcsin(eci[2])
+    rot = mv.CoordinateRotationLST(flux=flux, times=g["sel_lsts"], telescope_loc=float(g["sel_lat"]),
+                                   skycoords=(ra, dec), chunk_size=int(g["sel_chunk_size"]), source_buffer=0.7)
+    rot.setup()
+    rot.eci.copy_(torch.as_tensor(eci))  # the fixture's exact unit vectors
+    assert rot.nsrc_alloc == int(g["sel_alloc"])
+    for t in range(len(g["sel_lsts"])):
+        rot.rotate(t)
+        for ch in range(2):
+            crd, fl, n = rot.select_chunk(ch, t)
+            assert n == int(g[f"sel_n_t{t}_c{ch}"])
+            np.testing.assert_allclose(crd[:, :n].cpu().numpy(), g[f"sel_crd_t{t}_c{ch}"], rtol=0, atol=1e-15)
+            np.testing.assert_array_equal(fl.cpu().numpy(), g[f"sel_flux_t{t}_c{ch}"])
+
+
+def test_select_chunk_overflow_raises(device):
+    n = 3000
+    ra = np.zeros(n)
+    dec = np.full(n, np.deg2rad(-30.72))  # all near zenith at lst 0
+    rot = mv.CoordinateRotationLST(flux=np.ones(n), times=np.array([0.0]), telescope_loc=np.deg2rad(-30.72),
+                                   skycoords=(ra, dec), source_buffer=0.5)
+    rot.setup()
+    rot.rotate(0)
+    with pytest.raises(ValueError, match="nsrc_alloc"):
+        rot.select_chunk(0, 0)
+
+
+# ---------------------------------------------------------------- beams
+@pytest.mark.parametrize("case", ["ident", "lin", "cplx", "pow"])
+def test_bilinear_matches_reference(device, case):
+    g = golden("bilinear")
+    p = g[f"{case}_params"]
+    beam = g[f"{case}_beam"]
+    out = mv.beams.gpu_beam_interpolation(beam, p[:, 0], p[:, 1], p[:, 2], g[f"{case}_az"], g[f"{case}_za"])
+    ref = g[f"{case}_out"]
+    # grids are float32 on the device
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=0, atol=2e-6 * max(1.0, np.abs(ref).max()))
+
+
+def test_bilinear_wrong_dtype(device):
+    with pytest.raises(ValueError, match="as the dtype for beam, which is unrecognized"):
+        mv.beams.gpu_beam_interpolation(np.ones((1, 1, 1, 3, 3), dtype=int), 1.0, 1.0, 0.0, [0.0], [0.0])
+
+
+def test_beam_interpolator_enu_matches_oracle(device):
+    rng = np.random.default_rng(3)
+    beams = mv.workloads.dipole_beams(rng, 2, dgrid_deg=2.0)
+    n = 5000
+    e = rng.uniform(-0.7, 0.7, n)
+    nn = rng.uniform(-0.7, 0.7, n)
+    bi = mv.B200BeamInterpolator(beam_list=beams, beam_idx=np.array([0, 1, 1]), polarized=True, nant=3, freq=1e8,
+                                 nsrc=n, precision=2)
+    bi.setup()
+    out = bi(torch.as_tensor(e, device=DEV), torch.as_tensor(nn, device=DEV)).cpu().numpy()
+    ob = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in beams]
+    ref = orc.beam_response(ob, True, e, nn)
+    np.testing.assert_allclose(out, ref, rtol=0, atol=1e-6)
+
+
+def test_gaussian_beam(device):
+    rng = np.random.default_rng(4)
+    e, nn = rng.uniform(-0.6, 0.6, 1000), rng.uniform(-0.6, 0.6, 1000)
+    bi = mv.B200BeamInterpolator(beam_list=[mv.GaussianBeam(0.2), mv.GaussianBeam(0.35)], beam_idx=np.array([0, 1]),
+                                 polarized=False, nant=2, freq=1e8, nsrc=1000, precision=2)
+    bi.setup()
+    out = bi(torch.as_tensor(e, device=DEV), torch.as_tensor(nn, device=DEV)).cpu().numpy()
+    ref = orc.beam_response([orc.GaussianPowerBeam(0.2), orc.GaussianPowerBeam(0.35)], False, e, nn)
+    np.testing.assert_allclose(out, ref, rtol=1e-13, atol=1e-15)
+
+
+# ---------------------------------------------------------------- tau / Z
+@pytest.mark.parametrize("precision,tol", [(1, 5e-7), (2, 1e-12)])
+def test_exptau_matches_reference(device, precision, tol):
+    g = golden("tauz")
+    tc = mv.TauCalculator(antpos=g["antpos"], freq=float(g["freq"]), nsrc=g["crd"].shape[1], precision=precision)
+    tc.setup()
+    out = tc(torch.as_tensor(g["crd"], device=DEV)).cpu().numpy()
+    np.testing.assert_allclose(out, g["exptau"], rtol=0, atol=tol)
+
+
+def test_exptau_long_baseline_phase():
+    """1 km, 200 MHz: |phase| ~ 4e3 rad; the FP64 reduction keeps complex64 exact to ~1e-7."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    rng = np.random.default_rng(9)
+    antpos = rng.uniform(-1000, 1000, (50, 3))
+    crd = rng.normal(size=(3, 3000))
+    crd /= np.linalg.norm(crd, axis=0)
+    tc = mv.TauCalculator(antpos=antpos, freq=200e6, nsrc=3000, precision=1)
+    tc.setup()
+    out = tc(torch.as_tensor(crd, device=DEV)).cpu().numpy()
+    np.testing.assert_allclose(out, orc.exptau(antpos, 200e6, crd), rtol=0, atol=5e-7)
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32x3"])
+def test_z_from_exptau_matches_reference(device, mode):
+    g = golden("tauz")
+    zc = mv.ZMatrixCalc(nant=6, nfeed=2, nax=2, nsrc=g["exptau"].shape[1], mode=_lib.GEMM_MODES[mode])
+    zc.setup()
+    z = zc(g["sqrt_flux"], g["beam"], g["exptau"], g["beam_idx"])
+    zz = z.to_complex().cpu().numpy()
+    # panel column order is (src, ax); reference order is (ax, src)
+    ref = g["z"].reshape(12, 2, -1).transpose(0, 2, 1).reshape(12, -1)
+    tol = {"bf16x3": 2e-5, "bf16x6": 5e-7, "tf32x3": 5e-7}[mode]
+    np.testing.assert_allclose(zz, ref, rtol=0, atol=tol * np.abs(ref).max())
+
+
+# ---------------------------------------------------------------- Hermitian product
+@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32x3"])
+@pytest.mark.parametrize("nfeed", [1, 2])
+@pytest.mark.parametrize("explicit", [False, True])
+def test_matmul_arange_known_answer(device, mode, nfeed, explicit):
+    """tests/test_matprod.py:45-65: integer-valued Z is reproduced exactly."""
+    g = golden("matprod")
+    nant, nsrc = 5, 15
+    pairs = np.array([(i, j) for i in range(nant) for j in range(nant)]) if explicit else None
+    for precision in (1, 2):
+        mp = mv.B200MatMul(nchunks=1, nfeed=nfeed, nant=nant, antpairs=pairs, precision=precision, gemm_mode=mode)
+        mp.setup()
+        z = np.arange(nfeed * nant * nsrc, dtype=complex).reshape(nfeed * nant, nsrc) + 1j
+        out = np.zeros((mp.npairs, nfeed, nfeed), dtype=np.complex64 if precision == 1 else np.complex128)
+        mp(z, chunk=0)
+        mp.sum_chunks(out)
+        ref = g[f"arange_CPUMatMul_f{nfeed}_p{precision}_e{int(explicit)}_c1"]
+        np.testing.assert_array_equal(out, ref)
+
+
+def test_vectordot_arange_known_answer(device):
+    g = golden("matprod")
+    for nfeed in (1, 2):
+        mp = mv.B200VectorDot(nchunks=1, nfeed=nfeed, nant=5, antpairs=None, precision=2)
+        mp.setup()
+        z = np.arange(nfeed * 5 * 15, dtype=complex).reshape(nfeed * 5, 15) + 1j
+        out = np.zeros((25, nfeed, nfeed), dtype=complex)
+        mp(z, 0)
+        mp.sum_chunks(out)
+        np.testing.assert_allclose(out, g[f"arange_CPUVectorDot_f{nfeed}_p2_e0_c1"], rtol=1e-7)
+
+
+@pytest.mark.parametrize("mode,tol", [("bf16x6", 1e-6), ("tf32x3", 1e-6), ("bf16x3", 3e-5)])
+@pytest.mark.parametrize("nant,nfeed,K,k_chunk", [(350, 2, 20000, 2048), (64, 1, 777, 64), (129, 2, 4096, 1024)])
+def test_matmul_random_vs_oracle(device, mode, tol, nant, nfeed, K, k_chunk):
+    rng = np.random.default_rng(nant + K)
+    M = nant * nfeed
+    z = (rng.normal(size=(M, K)) + 1j * rng.normal(size=(M, K))) * rng.lognormal(0, 1, K)[None, :]
+    mp = mv.B200MatMul(nchunks=1, nfeed=nfeed, nant=nant, antpairs=None, precision=2, gemm_mode=mode, k_chunk=k_chunk)
+    mp.setup()
+    out = torch.zeros((mp.npairs, nfeed, nfeed), dtype=torch.complex128, device=DEV)
+    mp(z, 0)
+    mp.sum_chunks(out)
+    ref = orc.matmul_vis(z.astype(np.complex64).astype(np.complex128), nant, nfeed)
+    err = _cos_err(out.cpu().numpy(), ref, nant, nfeed)
+    assert err <= tol, f"{mode}: cosine error {err:.3e} > {tol}"
+
+
+def test_matmul_sparse_pairs_vs_reference(device):
+    g = golden("matprod")
+    z, pairs = g["random_z"], g["random_pairs"]
+    for mode in ("bf16x6", "tf32x3"):
+        mp = mv.B200MatMul(nchunks=1, nfeed=2, nant=7, antpairs=pairs, precision=2, gemm_mode=mode)
+        mp.setup()
+        out = np.zeros((len(pairs), 2, 2), dtype=complex)
+        mp(z, 0)
+        mp.sum_chunks(out)
+        np.testing.assert_allclose(out, g["random_CPUMatMul_sparse"], rtol=0, atol=1e-5)
+
+
+def test_vectordot_random_vs_reference(device):
+    g = golden("matprod")
+    z, pairs = g["random_z"], g["random_pairs"]
+    mp = mv.B200VectorDot(nchunks=1, nfeed=2, nant=7, antpairs=pairs, precision=2, k_chunk=64)
+    mp.setup()
+    out = np.zeros((len(pairs), 2, 2), dtype=complex)
+    mp(z, 0)
+    mp.sum_chunks(out)
+    np.testing.assert_allclose(out, g["random_CPUVectorDot_sparse"], rtol=0, atol=1e-5)
+
+
+@pytest.mark.parametrize("k_chunk", [512, 2048, 8192])
+def test_herk_accumulation_positive_sums(device, k_chunk):
+    """All-positive terms (autocorrelation-like) over a long K: FP32 TMEM
+    accumulation per k-slice, FP64 across slices."""
+    rng = np.random.default_rng(1)
+    M, K = 128, 65536
+    z = rng.uniform(0.5, 1.5, size=(M, K)) * np.exp(1j * 0.01 * rng.normal(size=(M, K)))
+    mp = mv.B200MatMul(nchunks=1, nfeed=1, nant=M, antpairs=None, precision=2, gemm_mode="bf16x6", k_chunk=k_chunk)
+    mp.setup()
+    out = torch.zeros((M * M, 1, 1), dtype=torch.complex128, device=DEV)
+    mp(z, 0)
+    mp.sum_chunks(out)
+    ref = orc.matmul_vis(z.astype(np.complex64).astype(np.complex128), M, 1)
+    rel = np.abs(out.cpu().numpy() - ref) / np.abs(ref)
+    print(f"k_chunk={k_chunk}: max rel {rel.max():.3e}, mean rel {rel.mean():.3e}")
+    assert rel.max() < 2e-6
