@@ -8,31 +8,37 @@
 // Formulation.  For rows m, n of Z (row = ant * nfeed + feed):
 //   Re V[m, n] = sum_k Zr[m,k] Zr[n,k] + Zi[m,k] Zi[n,k]
 //   Im V[m, n] = sum_k Zr[m,k] Zi[n,k] - Zi[m,k] Zr[n,k]
-// A 128 x 128 complex tile (I, J), I <= J, accumulates in one 128 x 256 FP32
-// TMEM block D (columns 0..127 real, 128..255 imaginary) from three UMMAs per
+// A 128 x 128 complex tile (I, J), I <= J, lives in one 128 x 256 FP32 TMEM
+// block D (columns 0..127 real, 128..255 imaginary) filled by three UMMAs per
 // k-step and split-term product (pa, pb):
 //   D[:,   0:256] += Zr_I^pa . [Zr_J^pb ; Zi_J^pb]^T     (N = 256)
 //   D[:,   0:128] += Zi_I^pa . Zi_J^pb^T                  (N = 128)
 //   D[:, 128:256] += Zi_I^pa . (-Zr_J^pb)^T               (N = 128, negate-B bit)
-// Split products: BF16_3 {00, 01, 10}; BF16_6 {00, 01, 10, 02, 11, 20};
-// TF32_3 {00, 01, 10}.
+//
+// Accuracy.  The tensor core rounds its FP32 accumulator toward zero at every
+// UMMA, so a long in-TMEM sum drifts by about one ulp per instruction (3e-5
+// relative after 2,048 columns).  Each k-step (one 32-byte column block) is
+// therefore accumulated into a FRESH TMEM block, products in ascending order of
+// magnitude -- BF16_6 {11, 02, 20, 01, 10, 00}, BF16_3 / TF32_3 {01, 10, 00} -- so
+// only the final hi x hi UMMAs round at full magnitude, and the block is drained
+// by the epilogue warps into FP32 registers with round-to-nearest adds.  One
+// k-slice (k_chunk columns) of register sums is one partial tile; slices are
+// summed in FP64 by herk_reduce_*.
 //
 // Schedule.  Work unit u = (k-slice s, tile t), t fastest so the CTAs that run
 // together read the same Z columns (L2 reuse).  Persistent CTAs (one per SM,
-// 192 KB of shared memory) loop over units.  Warp roles:
+// 192 KB of shared memory) loop over units.  Warp roles (320 threads):
 //   warp 0 lane 0 : TMA producer, one 3-D box per operand per stage (all 2P
 //                   split/component planes of 128 rows x 32 bytes, SWIZZLE_32B);
-//   warp 1        : TMEM owner (512 columns = two accumulators); lane 0 issues
-//                   the UMMAs and tcgen05.commit's stage / accumulator barriers;
-//   warps 2..5    : epilogue, tcgen05.ld of TMEM lane quadrant (warp % 4) and
-//                   coalesced FP32 stores of the tile to the workspace
-//                   [u][256 columns][128 rows]; double-buffered accumulators let
-//                   unit u drain while unit u + 1 accumulates.
+//   warp 1        : TMEM owner (512 columns = two k-step blocks); lane 0 issues
+//                   the UMMAs and tcgen05.commit's the stage / block barriers;
+//   warps 2..9    : epilogue; warp w drains TMEM lane quadrant (w % 4), column
+//                   half (w - 2) / 4 (real / imaginary), 128 FP32 register
+//                   sums per thread, and at the end of a unit stores them
+//                   coalesced to the workspace [u][256 columns][128 rows].
 // Every mbarrier wait is bounded by wall time; on expiry the CTA records
 // MVB_DEV_TIMEOUT in the status word, stops issuing work, drains the copies and
 // MMAs it issued, frees TMEM and returns.
-//
-// The FP32 partial tiles of the k-slices are summed in FP64 by herk_reduce_*.
 #include <algorithm>
 #include <mutex>
 
@@ -42,7 +48,8 @@
 
 namespace mvb {
 
-constexpr int kHerkThreads = 192;
+constexpr int kEpiWarps = 8;
+constexpr int kHerkThreads = 64 + 32 * kEpiWarps;
 constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s
 constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
 constexpr int kPlaneBytes = 128 * 32;              // one 128-row x 32-byte plane tile
@@ -62,6 +69,16 @@ struct HerkCfg {
   static constexpr uint32_t ID128 = umma_idesc(FMT, 128, 0);
   static constexpr uint32_t ID128N = umma_idesc(FMT, 128, 1);
 };
+
+// Split-term products (pa, pb), ascending magnitude 2^-8(pa + pb).
+// Tables packed one nibble per product: 6 products pa = 1,0,2,0,1,0 and
+// pb = 1,2,0,1,0,0; 3 products pa = 0,1,0 and pb = 1,0,0.
+__device__ __forceinline__ void product_terms(int nprod, int q, uint32_t &pa, uint32_t &pb) {
+  const uint32_t ta = nprod == 6 ? 0x010201u : 0x010u;
+  const uint32_t tb = nprod == 6 ? 0x001021u : 0x001u;
+  pa = (ta >> (4 * q)) & 0xFu;
+  pb = (tb >> (4 * q)) & 0xFu;
+}
 
 // Valid K columns: (source count) x (columns per source), clamped to the panel.
 __device__ __forceinline__ int64_t valid_k(const int32_t *n_dev, int64_t n_host, int kmul, int64_t Kcap) {
@@ -97,8 +114,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[C::STAGES];
   __shared__ __align__(8) uint64_t empty_bar[C::STAGES];
-  __shared__ __align__(8) uint64_t tfull_bar[2];
-  __shared__ __align__(8) uint64_t tempty_bar[2];
+  __shared__ __align__(8) uint64_t dfull_bar[2];
+  __shared__ __align__(8) uint64_t dempty_bar[2];
   __shared__ __align__(8) uint64_t drain_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
@@ -117,8 +134,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&tfull_bar[b], 1);
-      mbar_init(&tempty_bar[b], 4);
+      mbar_init(&dfull_bar[b], 1);
+      mbar_init(&dempty_bar[b], kEpiWarps);
     }
     mbar_init(&drain_bar, 1);
     abort_flag = 0;
@@ -166,11 +183,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       }
     }
   } else if (warp == 1 && lane == 0) {
-    // ---------------- UMMA issuer ----------------
-    constexpr int pa_tab[6] = {0, 0, 1, 0, 1, 2};
-    constexpr int pb_tab[6] = {0, 1, 0, 2, 1, 0};
-    uint32_t st = 0, ph = 0, buf = 0;
-    uint32_t tph = 0;  // bit b: phase of accumulator b
+    // ---------------- UMMA issuer: one fresh TMEM block per k-step ----------------
+    uint32_t st = 0, ph = 0, buf = 0, dph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
       const int s = u / n_tiles, t = u % n_tiles;
       int I, J;
@@ -179,76 +193,88 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
-      if (!mbar_wait(&tempty_bar[buf], ((tph >> buf) & 1u) ^ 1u, kWaitLimitNs)) {
-        atomicOr(status, MVB_DEV_TIMEOUT);
-        abort_flag = 1;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t d = tbase + buf * 256;
       bool ok = true;
       for (int ks = 0; ks < nks; ++ks) {
-        if (!mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
+        if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, kWaitLimitNs) ||
+            !mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
           atomicOr(status, MVB_DEV_TIMEOUT);
           abort_flag = 1;
           ok = false;
           break;
         }
         tc_fence_after();
+        const uint32_t d = tbase + buf * 256;
         const uint32_t a_base = smem_u32(smem + (size_t)st * C::STAGE_BYTES);
         const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
 #pragma unroll
         for (int q = 0; q < C::NPROD; ++q) {
-          const uint32_t pa = pa_tab[q], pb = pb_tab[q];
+          uint32_t pa, pb;
+          product_terms(C::NPROD, q, pa, pb);
           const uint64_t a_re = umma_desc_sw32(a_base + (2 * pa) * kPlaneBytes);
           const uint64_t a_im = umma_desc_sw32(a_base + (2 * pa + 1) * kPlaneBytes);
           const uint64_t b_re = umma_desc_sw32(b_base + (2 * pb) * kPlaneBytes);
           const uint64_t b_im = umma_desc_sw32(b_base + (2 * pb + 1) * kPlaneBytes);
-          umma<MODE>(d, a_re, b_re, C::ID256, (ks > 0 || q > 0) ? 1u : 0u);
+          umma<MODE>(d, a_re, b_re, C::ID256, q > 0 ? 1u : 0u);
           umma<MODE>(d, a_im, b_im, C::ID128, 1u);
           umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
         }
         tc_commit(&empty_bar[st]);
+        tc_commit(&dfull_bar[buf]);
+        dph ^= 1u << buf;
+        buf ^= 1u;
         if (++st == C::STAGES) {
           st = 0;
           ph ^= 1;
         }
       }
       if (!ok) break;
-      tc_commit(&tfull_bar[buf]);
-      tph ^= 1u << buf;
-      buf ^= 1;
     }
   } else if (warp >= 2) {
-    // ---------------- epilogue ----------------
+    // ---------------- epilogue: drain every k-step block into FP32 registers ----------------
     const int quad = warp & 3;
+    const int half = (warp - 2) >> 2;  // 0: real columns, 1: imaginary columns
     const int row = quad * 32 + lane;
-    uint32_t buf = 0;
-    uint32_t tph = 0;  // bit b: phase of accumulator b
+    uint32_t buf = 0, dph = 0;
+    float acc[128];
+#pragma unroll
+    for (int j = 0; j < 128; ++j) acc[j] = 0.f;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      // every lane waits; the vote keeps the warp converged for tcgen05.ld
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull_bar[buf], (tph >> buf) & 1u, kWaitLimitNs));
+      const int s = u / n_tiles;
+      const int64_t k0 = (int64_t)s * k_chunk;
+      const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
+      const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
+      bool ok = true;
+      for (int ks = 0; ks < nks; ++ks) {
+        // every lane waits; the vote keeps the warp converged for tcgen05.ld
+        ok = __all_sync(0xffffffffu, mbar_wait(&dfull_bar[buf], (dph >> buf) & 1u, kWaitLimitNs));
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t taddr = tbase + ((uint32_t)(quad * 32) << 16) + buf * 256 + half * 128;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          uint32_t v[16];
+          tmem_ld16(taddr + c * 16, v);
+          tmem_ld_wait();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[c * 16 + j] += __uint_as_float(v[j]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&dempty_bar[buf]);
+        dph ^= 1u << buf;
+        buf ^= 1u;
+      }
       if (!ok) {
         if (lane == 0) atomicOr(status, MVB_DEV_TIMEOUT);
         abort_flag = 1;
         break;
       }
-      tc_fence_after();
-      float *dst = partials + (size_t)u * (256 * 128);
-      const uint32_t taddr = tbase + ((uint32_t)(quad * 32) << 16) + buf * 256;
-#pragma unroll 1
-      for (int c = 0; c < 8; ++c) {
-        uint32_t v[32];
-        tmem_ld32(taddr + c * 32, v);
-        tmem_ld_wait();
+      float *dst = partials + (size_t)u * (256 * 128) + (size_t)half * 128 * 128;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) dst[(c * 32 + j) * 128 + row] = __uint_as_float(v[j]);
+      for (int j = 0; j < 128; ++j) {
+        dst[j * 128 + row] = acc[j];
+        acc[j] = 0.f;
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
-      tph ^= 1u << buf;
-      buf ^= 1;
     }
   }
 

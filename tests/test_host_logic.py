@@ -1,0 +1,150 @@
+"""Host-side logic that needs no GPU: chunk planning, sharding (2 gloo ranks),
+synthetic generators, parameter plumbing."""
+
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from matvis_b200 import _utils, sharding, workloads
+from matvis_b200.engine import JobSpec, _norm_matprod
+from matvis_b200.matprod import choose_k_chunk
+from oracle import oracle as orc
+
+from .conftest import golden
+
+
+def test_chunk_planning_matches_reference_table():
+    for row in golden("chunks")["table"]:
+        fm, nax, nfeed, nant, nsrc, nbeam, npix, prec, sb, mb, ch = row
+        got = _utils.get_required_chunks(fm, int(nax), int(nfeed), int(nant), int(nsrc), int(nbeam), int(npix),
+                                         int(prec), sb, mb)
+        assert got == int(ch)
+    with pytest.raises(ValueError):
+        _utils.get_required_chunks(1, 1, 1, 1, 1, 1, 1, 1, 1.0, 0.0)
+
+
+def test_desired_chunks_counts_grid_pixels():
+    beams = workloads.dipole_beams(np.random.default_rng(0), 2, dgrid_deg=10.0)
+    n, per = _utils.get_desired_chunks(2**40, 3, beams, 2, 2, 10, 1000, 1)
+    assert n == 3 and per == 334
+
+
+def test_get_dtypes():
+    assert _utils.get_dtypes(1) == (np.float32, np.complex64)
+    assert _utils.get_dtypes(2) == (np.float64, np.complex128)
+
+
+def test_matprod_names():
+    for n in ("MatMul", "CPUMatMul", "GPUMatMul", "B200MatMul"):
+        assert _norm_matprod(n) == "MatMul"
+    for n in ("VectorDot", "VectorLoop", "GPUVectorLoop", "CPUVectorDot"):
+        assert _norm_matprod(n) == "VectorDot"
+    with pytest.raises(ValueError):
+        _norm_matprod("Einsum")
+
+
+def test_choose_k_chunk():
+    kc = choose_k_chunk(21, 196608, 148)
+    assert kc % 64 == 0 and 1024 <= kc <= 8192
+    assert choose_k_chunk(1, 100, 148) == 1024
+
+
+def test_healpix_centres_equal_area():
+    ra, dec = workloads.healpix_ring_centres(16)
+    assert len(ra) == 12 * 16 * 16
+    z = np.sin(dec)
+    assert abs(z.mean()) < 1e-12  # symmetric about the equator
+    # every ring of the equatorial belt has 4 nside pixels
+    assert np.sum(np.isclose(z, 0.0)) == 4 * 16
+
+
+def test_hex_array_spacing():
+    a = workloads.hex_array(320, 14.6)
+    assert a.shape == (320, 3)
+    d = np.linalg.norm(a[:, None, :2] - a[None, :, :2], axis=-1)
+    d[np.diag_indices(320)] = np.inf
+    assert np.isclose(d.min(), 14.6)
+    assert len(np.unique(np.round(a, 6), axis=0)) == 320
+
+
+def test_powerlaw_flux_bounds():
+    s = workloads.powerlaw_flux(np.random.default_rng(0), 100000)
+    assert s.min() >= 0.05 and s.max() <= 100.0
+    # N(>S) ~ S^-1.5: the fraction above 1 Jy
+    frac = np.mean(s > 1.0)
+    expect = (1.0**-1.5 - 100**-1.5) / (0.05**-1.5 - 100**-1.5)
+    assert abs(frac - expect) < 0.01
+
+
+def test_frequency_shards_cover_once():
+    for nf in (1, 7, 64, 256):
+        for w in (1, 2, 3, 8):
+            sh = sharding.frequency_shards(nf, w)
+            got = [f for a, b in sh for f in range(a, b)]
+            assert got == list(range(nf))
+            sizes = [b - a for a, b in sh]
+            assert max(sizes) - min(sizes) <= 1
+
+
+def test_cosine_metric_detects_error():
+    rng = np.random.default_rng(0)
+    z = rng.normal(size=(6, 50)) + 1j * rng.normal(size=(6, 50))
+    v = orc.matmul_vis(z, 3, 2)
+    assert orc.cosine_error_metric(v, v, 2) == 0
+    w = v.copy()
+    w[1, 0, 1] += 1e-3
+    assert orc.cosine_error_metric(w, v, 2) > 1e-5
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _gather_worker(rank, world, port, nfreq, q):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        f0, f1 = sharding.frequency_shards(nfreq, world)[rank]
+        # stand-in for the per-rank visibilities: each frequency slice filled with its index
+        local = np.arange(f0, f1, dtype=np.float64)[:, None, None] * np.ones((1, 3, 4))
+        out = sharding.gather_frequency_shards(local, rank, world, nfreq)
+        if rank == 0:
+            q.put(out)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("nfreq", [5, 64])
+def test_gather_two_gloo_ranks(nfreq):
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, nfreq, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out.shape == (nfreq, 3, 4)
+    np.testing.assert_array_equal(out[:, 0, 0], np.arange(nfreq))
+
+
+def test_shard_spec_slices_fluxes():
+    spec = JobSpec(antpos=np.zeros((2, 3)), eci=np.zeros((3, 4)), fluxes=np.arange(20.0).reshape(4, 5),
+                   freqs=np.arange(5.0), lsts=np.zeros(1), latitude=0.0, beams=[])
+    s1, (f0, f1) = sharding.shard_spec(spec, 1, 2)
+    assert (f0, f1) == (3, 5)
+    np.testing.assert_array_equal(s1.fluxes, spec.fluxes[:, 3:5])
+    np.testing.assert_array_equal(s1.freqs, [3.0, 4.0])
