@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--k-chunk", type=int, default=None)
     ap.add_argument("--nfreq", type=int, default=64)
     ap.add_argument("--ntimes", type=int, default=16)
+    ap.add_argument("--nside", type=int, default=128, help="sky pixelisation (128: 196,608 sources)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
@@ -252,7 +253,7 @@ def run_b200(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
 
-    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes)
+    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes, nside=args.nside)
     terms, counts = terms_per_job(cfg)
     spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
                            lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
@@ -337,7 +338,7 @@ def run_b200(args, rank, world, local_rank):
         "dtype": "bf16" if args.gemm_mode.startswith("bf16") else "tf32",
         "data": "synthetic (seeded; HEALPix nside=128 centres, HERA-350-like array, dipole-like beams)",
         "config": {
-            "workload": f"config2 HERA-350-like: 350 ant x 196608 src x {len(cfg['freqs'])} freq x "
+            "workload": f"config2 HERA-350-like: 350 ant x {len(cfg['ra'])} src x {len(cfg['freqs'])} freq x "
                         f"{len(cfg['lsts'])} LST, polarised 2x2, 4 gridded beams + beam_idx; one job per step",
             "gemm_mode": args.gemm_mode, "k_chunk": kc, "terms_per_job": terms,
             "above_horizon_per_time": [int(c) for c in counts],

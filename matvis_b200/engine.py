@@ -146,38 +146,52 @@ class VisEngine:
     # ----------------------------------------------------------------- launch
     def enqueue(self, stream=None):
         """Enqueue every kernel of the job on ``stream`` (no host synchronisation)."""
+        for t in range(len(self.lsts)):
+            self.enqueue_time(t, stream)
+
+    def enqueue_time(self, t: int, stream=None):
+        """Enqueue the kernels of time index t (all chunks and frequencies)."""
         L = _lib.lib
         sh = _lib.stream_handle(stream)
         chk = _lib.check
         A = self.nant
         F, X = self.nfeed, self.nax
         panel = self.zcalc.z
-        for t in range(len(self.lsts)):
-            R = np.ascontiguousarray(self.rot[t])
-            chk(L.mvb_rotate(_lib.ptr(self.eci), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
-            for c in range(self.nchunks):
-                c0 = min(c * self.chunk_size, self.nsrc)
-                c1 = min((c + 1) * self.chunk_size, self.nsrc)
-                chk(L.mvb_horizon_compact(
-                    _lib.ptr(self.topo), self.nsrc, c0, c1, None, _lib.ptr(self.crd), _lib.ptr(self.kept), None,
-                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.status), _lib.ptr(self.ws_compact),
-                    self.ws_compact.numel(), sh))
-                self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, self.bmfunc.interpolated_beam,
-                                   stream=stream, status=self.status)
-                beam = self.bmfunc.interpolated_beam
-                for f in range(len(self.freqs)):
-                    chk(L.mvb_tau_z(
-                        _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
-                        _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f]), _lib.ptr(self.kept), _lib.ptr(beam),
-                        beam.shape[-1], beam.shape[0], _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode,
-                        _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
-                    panel.n_dev = self.n_above
-                    panel.n_host = self.cap
-                    out = self.vis[f, t]
-                    if self.method == "MatMul":
-                        self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream, k_chunk=self.k_chunk)
-                    else:
-                        self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream)
+        R = np.ascontiguousarray(self.rot[t])
+        chk(L.mvb_rotate(_lib.ptr(self.eci), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
+        for c in range(self.nchunks):
+            c0 = min(c * self.chunk_size, self.nsrc)
+            c1 = min((c + 1) * self.chunk_size, self.nsrc)
+            chk(L.mvb_horizon_compact(
+                _lib.ptr(self.topo), self.nsrc, c0, c1, None, _lib.ptr(self.crd), _lib.ptr(self.kept), None,
+                _lib.ptr(self.n_above), self.cap, _lib.ptr(self.status), _lib.ptr(self.ws_compact),
+                self.ws_compact.numel(), sh))
+            self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, self.bmfunc.interpolated_beam,
+                               stream=stream, status=self.status)
+            beam = self.bmfunc.interpolated_beam
+            for f in range(len(self.freqs)):
+                chk(L.mvb_tau_z(
+                    _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
+                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f]), _lib.ptr(self.kept), _lib.ptr(beam),
+                    beam.shape[-1], beam.shape[0], _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode,
+                    _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
+                panel.n_dev = self.n_above
+                panel.n_host = self.cap
+                out = self.vis[f, t]
+                if self.method == "MatMul":
+                    self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream, k_chunk=self.k_chunk)
+                else:
+                    self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream)
+
+    def device_bytes(self) -> int:
+        """Device memory this job holds once allocated."""
+        if not self._allocated:
+            return estimate_device_bytes(self.spec)
+        tensors = [self.eci, self.antpos, self.sflux, self.topo, self.crd, self.kept, self.ws_compact, self.vis,
+                   self.zcalc.z.data, self.bmfunc.interpolated_beam]
+        n = sum(t.numel() * t.element_size() for t in tensors)
+        ws = getattr(self.matprod, "_ws", None)
+        return n + (ws.numel() if ws is not None else 0)
 
     def launches_per_run(self) -> int:
         per_f = 3 if self.method == "MatMul" else 2
@@ -227,3 +241,33 @@ def job_from_arrays(*, ants, fluxes, ra, dec, freqs, lsts, latitude, beams, **kw
         antpos = np.asarray(ants, dtype=np.float64)
     return JobSpec(antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=np.asarray(fluxes), freqs=np.asarray(freqs),
                    lsts=np.asarray(lsts), latitude=float(latitude), beams=list(beams), **kw)
+
+
+def estimate_device_bytes(spec: JobSpec) -> int:
+    """HBM footprint of a job (admission control): inputs, per-time buffers, Z panel,
+    product workspace and the output."""
+    A = len(spec.antpos)
+    N = np.asarray(spec.eci).shape[1]
+    Nf, Nt = len(spec.freqs), len(spec.lsts)
+    F = X = 2 if spec.polarized else 1
+    nch = max(1, int(spec.nchunks))
+    chunk = int(np.ceil(N / nch)) if N else 1
+    cap = max(1, int(chunk * spec.source_buffer) if chunk > 1000 else chunk)
+    npairs = len(spec.antpairs) if spec.antpairs is not None else A * A
+    csize = 8 if spec.precision == 1 else 16
+    method = _norm_matprod(spec.matprod)
+    if method == "MatMul":
+        mode = _lib.GEMM_MODES[spec.gemm_mode] if isinstance(spec.gemm_mode, str) else int(spec.gemm_mode)
+    else:
+        mode = _lib.Z_C64
+    mpad, kcap = _lib.zpanel_shape(mode, A * F, cap * X)
+    panel = _lib.lib.mvb_zpanel_bytes(mode, mpad, kcap)
+    if method == "MatMul":
+        T = mpad // _lib.TILE
+        kc = spec.k_chunk or choose_k_chunk(T * (T + 1) // 2, kcap)
+        ws = _lib.lib.mvb_herk_ws_bytes(mpad, kcap, kc)
+    else:
+        ws = _lib.lib.mvb_vecdot_ws_bytes(npairs, F, kcap, spec.k_chunk or 4096)
+    nbeam = len(spec.beams)
+    return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + 8 * nbeam * F * X * cap + panel + ws
+               + Nf * Nt * npairs * F * F * csize)
