@@ -82,6 +82,23 @@ int mvb_horizon_compact(const double *topo, int64_t ld, int64_t c0, int64_t c1, 
                         int32_t *idx_out, double *flux_out, int32_t *n_out, int64_t cap, int32_t *status, void *ws,
                         size_t ws_bytes, void *stream);
 
+/* Allocation-free form of mvb_horizon_compact; this entry point has no
+ * counterpart in the reference.  It is for callers that cannot allocate device
+ * memory when they select sources (memory planned once at start-up with
+ * allocation forbidden afterwards, since cudaMalloc / cudaFree can synchronise
+ * the device; or a host handed only a stream and its buffers by another
+ * library).  The per-block scratch is a 16 KB static device array inside the
+ * library, held by every GPU that loads it until exit; chunks are limited to
+ * 4,194,304 sources (c1 - c0), larger ones are rejected with MVB_ERR_ARG.  The
+ * first call on a device looks up the array's device address (with that device
+ * current) and caches it, so that first call should come before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU race,
+ * so serialise them (one stream, or events).  Inputs, outputs and semantics are
+ * those of mvb_horizon_compact; it calls no allocator. */
+int mvb_horizon_compact_static(const double *topo, int64_t ld, int64_t c0, int64_t c1, const double *flux,
+                               double *crd_out, int32_t *idx_out, double *flux_out, int32_t *n_out, int64_t cap,
+                               int32_t *status, void *stream);
+
 /* ---- A5: beam interpolation ---------------------------------------------- */
 /* Bilinear interpolation (order-1 map_coordinates, 0 outside [0, n-1] on either
  * axis) of grids (nbeam, nax, nfeed, nza, naz) at the sources of crd (SoA,

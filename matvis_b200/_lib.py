@@ -48,6 +48,10 @@ _SIGNATURES = {
         c_int,
         [_p, c_int64, c_int64, c_int64, _p, _p, _p, _p, _p, c_int64, _p, _p, c_size_t, _p],
     ),
+    "mvb_horizon_compact_static": (
+        c_int,
+        [_p, c_int64, c_int64, c_int64, _p, _p, _p, _p, _p, c_int64, _p, _p],
+    ),
     "mvb_beam_interp": (
         c_int,
         [_p, c_int, c_int, c_int, c_int, c_int, c_int, _p, _p, c_int64, _p, c_int64, _p, c_int, c_int64, _p, _p],

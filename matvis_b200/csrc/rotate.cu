@@ -12,6 +12,8 @@
 // (ballot + popc) and a scatter pass in which each block sums the counts of the
 // blocks before it, then ranks its own sources with warp ballots.  No block
 // waits on another, so there is no inter-block spin.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace mvb {
@@ -176,5 +178,74 @@ extern "C" int mvb_horizon_compact(const double *topo, int64_t ld, int64_t c0, i
   const int grid = std::max(nblocks, 1);
   horizon_scatter_kernel<<<grid, kCompactThreads, 0, s>>>(topo, ld, c0, count, counts, nblocks, flux, crd_out, idx_out,
                                                          flux_out, n_out, cap, status);
+  return check_launch("horizon_scatter_kernel");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of mvb_horizon_compact.
+//
+// Some callers cannot allocate device memory at the moment they select sources:
+// a pipeline that plans all of its device memory once at start-up and forbids
+// allocation afterwards (cudaMalloc / cudaFree can synchronise the device and
+// stall every other stream), or a host that is handed only a stream and its
+// input / output buffers by another library.  For them the per-block counts
+// live in this fixed device array instead of a caller workspace.  Every GPU that
+// loads the library holds it (16 KB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace mvb {
+
+constexpr int kStaticCompactBlocks = 4096;  // chunks of up to 4096 x 1024 sources
+static __device__ __align__(256) int32_t g_compact_counts[kStaticCompactBlocks];
+
+// Device address of g_compact_counts for the current device, looked up once
+// per device (with that device current) and cached.
+static int static_counts_ptr(int32_t **out) {
+  static int32_t *cache[64] = {};
+  static std::mutex mu;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(MVB_ERR_CUDA, "mvb_horizon_compact_static: cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return fail(MVB_ERR_UNSUPPORTED, "mvb_horizon_compact_static: device ordinal %d", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (cache[dev] == nullptr) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_compact_counts);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(MVB_ERR_CUDA, "mvb_horizon_compact_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    cache[dev] = static_cast<int32_t *>(p);
+  }
+  *out = cache[dev];
+  return MVB_OK;
+}
+
+}  // namespace mvb
+
+extern "C" int mvb_horizon_compact_static(const double *topo, int64_t ld, int64_t c0, int64_t c1, const double *flux,
+                                          double *crd_out, int32_t *idx_out, double *flux_out, int32_t *n_out,
+                                          int64_t cap, int32_t *status, void *stream) {
+  const int64_t count = c1 - c0;
+  if (count < 0 || c0 < 0 || c1 > ld || cap < 0 || !n_out || (count > 0 && !topo) ||
+      (cap > 0 && (!crd_out || !idx_out)) || (flux && cap > 0 && !flux_out))
+    return fail(MVB_ERR_ARG, "mvb_horizon_compact_static: bad arguments");
+  const int64_t nblocks = ceil_div(count, kCompactBlock);
+  if (nblocks > kStaticCompactBlocks)
+    return fail(MVB_ERR_ARG,
+                "mvb_horizon_compact_static: chunk of %lld sources exceeds the static limit of %lld sources "
+                "(use mvb_horizon_compact with a workspace)",
+                (long long)count, (long long)kStaticCompactBlocks * kCompactBlock);
+  int32_t *counts = nullptr;
+  int rc = static_counts_ptr(&counts);
+  if (rc) return rc;
+  // Every count the scatter pass reads is written by the count pass first, so
+  // nothing in the shared array has to start at zero.
+  cudaStream_t s = as_stream(stream);
+  if (nblocks > 0) {
+    horizon_count_kernel<<<(unsigned)nblocks, kCompactThreads, 0, s>>>(topo + 2 * ld + c0, count, counts);
+    rc = check_launch("horizon_count_kernel");
+    if (rc) return rc;
+  }
+  const int grid = (int)std::max<int64_t>(nblocks, 1);
+  horizon_scatter_kernel<<<grid, kCompactThreads, 0, s>>>(topo, ld, c0, count, counts, (int)nblocks, flux, crd_out,
+                                                         idx_out, flux_out, n_out, cap, status);
   return check_launch("horizon_scatter_kernel");
 }
