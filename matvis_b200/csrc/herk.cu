@@ -32,10 +32,13 @@
 //                   split/component planes of 128 rows x 32 bytes, SWIZZLE_32B);
 //   warp 1        : TMEM owner (512 columns = two k-step blocks); lane 0 issues
 //                   the UMMAs and tcgen05.commit's the stage / block barriers;
-//   warps 2..9    : epilogue; warp w drains TMEM lane quadrant (w % 4), column
-//                   half (w - 2) / 4 (real / imaginary), 128 FP32 register
-//                   sums per thread, and at the end of a unit stores them
-//                   coalesced to the workspace [u][256 columns][128 rows].
+//   warps 2..17   : epilogue; warp w drains TMEM lane quadrant (w % 4), column
+//                   quarter (w - 2) / 4 (64 of the 256 columns), 64 FP32
+//                   register sums per thread, and at the end of a unit stores
+//                   them coalesced to the workspace [u][256 columns][128 rows].
+// K_valid is cut into equal k-slices (multiples of 64 columns, at most k_chunk)
+// whose number is chosen on the device, from the device-side source count, to
+// fill whole waves of SMs (plan_splits).
 // Every mbarrier wait is bounded by wall time; on expiry the CTA records
 // MVB_DEV_TIMEOUT in the status word, stops issuing work, drains the copies and
 // MMAs it issued, frees TMEM and returns.
@@ -48,7 +51,8 @@
 
 namespace mvb {
 
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 16;
+constexpr int kPlanExtra = 32;  // extra k-slices the split planner may add to fill the SMs
 constexpr int kHerkThreads = 64 + 32 * kEpiWarps;
 constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s
 constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
@@ -80,6 +84,36 @@ __device__ __forceinline__ void product_terms(int nprod, int q, uint32_t &pa, ui
   pb = (tb >> (4 * q)) & 0xFu;
 }
 
+// Splits K_valid into nsplit equal slices of kc columns (a multiple of 64, at
+// most kmax), choosing nsplit in [ceil(K/kmax), +kPlanExtra] so that
+// n_tiles * nsplit work units fill whole waves of nsm SMs as evenly as possible
+// (ties: fewer slices).  Used identically by the product and its reduction.
+__host__ __device__ inline void plan_splits(int64_t kvalid, int n_tiles, int kmax, int nsm, int &nsplit, int64_t &kc) {
+  if (kvalid <= 0) {
+    nsplit = 0;
+    kc = kmax;
+    return;
+  }
+  const int64_t nmin = (kvalid + kmax - 1) / kmax;
+  double best_eff = -1.0;
+  nsplit = (int)nmin;
+  kc = kmax;
+  for (int64_t n = nmin; n <= nmin + kPlanExtra; ++n) {
+    int64_t c = (kvalid + n - 1) / n;
+    c = ((c + 63) / 64) * 64;
+    const int64_t ne = (kvalid + c - 1) / c;
+    const int64_t units = (int64_t)n_tiles * ne;
+    const int64_t waves = (units + nsm - 1) / nsm;
+    const double eff = (double)units / (double)(waves * nsm);
+    if (eff > best_eff + 1e-3) {
+      best_eff = eff;
+      nsplit = (int)ne;
+      kc = c;
+    }
+    if (c <= 64) break;
+  }
+}
+
 // Valid K columns: (source count) x (columns per source), clamped to the panel.
 __device__ __forceinline__ int64_t valid_k(const int32_t *n_dev, int64_t n_host, int kmul, int64_t Kcap) {
   int64_t n = n_dev ? (int64_t)*n_dev : n_host;
@@ -108,7 +142,7 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
 template <int MODE>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const __grid_constant__ CUtensorMap zmap, int T, int n_tiles, const int32_t *__restrict__ n_dev,
-                int64_t n_host, int kmul, int64_t Kcap, int k_chunk, float *__restrict__ partials,
+                int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, float *__restrict__ partials,
                 int32_t *__restrict__ status) {
   using C = HerkCfg<MODE>;
   extern __shared__ uint8_t smem_raw[];
@@ -122,7 +156,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
-  const int nsplit = (int)((kvalid + k_chunk - 1) / k_chunk);
+  int nsplit;
+  int64_t kc;
+  plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
   const int n_units = n_tiles * nsplit;
   if ((int)blockIdx.x >= n_units) return;  // uniform over the CTA
 
@@ -159,8 +195,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int s = u / n_tiles, t = u % n_tiles;
       int I, J;
       decode_tile(t, T, I, J);
-      const int64_t k0 = (int64_t)s * k_chunk;
-      const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
+      const int64_t k0 = (int64_t)s * kc;
+      const int64_t klen = min(kc, kvalid - k0);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
       const uint32_t bytes = diag ? C::OPER_BYTES : 2 * C::OPER_BYTES;
@@ -189,8 +225,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int s = u / n_tiles, t = u % n_tiles;
       int I, J;
       decode_tile(t, T, I, J);
-      const int64_t k0 = (int64_t)s * k_chunk;
-      const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
+      const int64_t k0 = (int64_t)s * kc;
+      const int64_t klen = min(kc, kvalid - k0);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
       bool ok = true;
@@ -232,16 +268,16 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   } else if (warp >= 2) {
     // ---------------- epilogue: drain every k-step block into FP32 registers ----------------
     const int quad = warp & 3;
-    const int half = (warp - 2) >> 2;  // 0: real columns, 1: imaginary columns
+    const int quarter = (warp - 2) >> 2;  // columns [64 quarter, 64 quarter + 64)
     const int row = quad * 32 + lane;
     uint32_t buf = 0, dph = 0;
-    float acc[128];
+    float acc[64];
 #pragma unroll
-    for (int j = 0; j < 128; ++j) acc[j] = 0.f;
+    for (int j = 0; j < 64; ++j) acc[j] = 0.f;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
       const int s = u / n_tiles;
-      const int64_t k0 = (int64_t)s * k_chunk;
-      const int64_t klen = min((int64_t)k_chunk, kvalid - k0);
+      const int64_t k0 = (int64_t)s * kc;
+      const int64_t klen = min(kc, kvalid - k0);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       bool ok = true;
       for (int ks = 0; ks < nks; ++ks) {
@@ -249,9 +285,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         ok = __all_sync(0xffffffffu, mbar_wait(&dfull_bar[buf], (dph >> buf) & 1u, kWaitLimitNs));
         if (!ok) break;
         tc_fence_after();
-        const uint32_t taddr = tbase + ((uint32_t)(quad * 32) << 16) + buf * 256 + half * 128;
+        const uint32_t taddr = tbase + ((uint32_t)(quad * 32) << 16) + buf * 256 + quarter * 64;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
+        for (int c = 0; c < 4; ++c) {
           uint32_t v[16];
           tmem_ld16(taddr + c * 16, v);
           tmem_ld_wait();
@@ -269,9 +305,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         abort_flag = 1;
         break;
       }
-      float *dst = partials + (size_t)u * (256 * 128) + (size_t)half * 128 * 128;
+      float *dst = partials + (size_t)u * (256 * 128) + (size_t)quarter * 64 * 128;
 #pragma unroll
-      for (int j = 0; j < 128; ++j) {
+      for (int j = 0; j < 64; ++j) {
         dst[j * 128 + row] = acc[j];
         acc[j] = 0.f;
       }
@@ -323,15 +359,17 @@ __device__ __forceinline__ void store_out(void *out, int64_t idx, double re, dou
 template <typename OT>
 __global__ void __launch_bounds__(256)
     herk_reduce_all_kernel(const float *__restrict__ part, int T, int n_tiles, const int32_t *__restrict__ n_dev,
-                           int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int A, int F, void *__restrict__ out,
-                           int accumulate) {
+                           int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, int A, int F,
+                           void *__restrict__ out, int accumulate) {
   __shared__ double sre[kRedRows][kRedCols + 1], sim[kRedRows][kRedCols + 1];
   const int t = blockIdx.x / 16, sub = blockIdx.x % 16;
   int I, J;
   decode_tile(t, T, I, J);
   const int r0 = (sub / 4) * kRedRows, c0 = (sub % 4) * kRedCols;
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
-  const int nsplit = (int)((kvalid + k_chunk - 1) / k_chunk);
+  int nsplit;
+  int64_t kc;
+  plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
   const int M = A * F;
   const int mbase = I * 128 + r0, nbase = J * 128 + c0;
   if (mbase >= M || nbase >= M) return;
@@ -378,11 +416,14 @@ __global__ void __launch_bounds__(256)
 template <typename OT>
 __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, int n_tiles,
                                          const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap,
-                                         int k_chunk, int F, const int32_t *__restrict__ pairs, int64_t npairs,
+                                         int k_chunk, int nsm, int F, const int32_t *__restrict__ pairs,
+                                         int64_t npairs,
                                          void *__restrict__ out, int accumulate) {
   const int64_t total = npairs * F * F;
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
-  const int nsplit = (int)((kvalid + k_chunk - 1) / k_chunk);
+  int nsplit;
+  int64_t kc;
+  plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pr = e / (F * F);
     const int p = (int)((e / F) % F), q = (int)(e % F);
@@ -453,13 +494,14 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   if (r != CUDA_SUCCESS) return fail(MVB_ERR_CUDA, "mvb_herk: cuTensorMapEncodeTiled failed (%d)", (int)r);
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
-  const int64_t max_units = (int64_t)n_tiles * ceil_div(Kcap, k_chunk);
-  const int grid = (int)std::min<int64_t>(max_units, num_sms());
+  const int nsm = num_sms();
+  const int64_t max_units = (int64_t)n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
+  const int grid = (int)std::min<int64_t>(max_units, nsm);
   const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
   int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE>), (int)smem, MODE);
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
-  herk_kernel<MODE><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, partials,
+  herk_kernel<MODE><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials,
                                                      status);
   return check_launch("herk_kernel");
 }
@@ -471,7 +513,7 @@ using namespace mvb;
 extern "C" size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk) {
   if (Mpad <= 0 || Kcap <= 0 || k_chunk <= 0) return 0;
   const int64_t T = Mpad / 128;
-  return (size_t)(T * (T + 1) / 2) * (size_t)ceil_div(Kcap, k_chunk) * 256 * 128 * sizeof(float);
+  return (size_t)(T * (T + 1) / 2) * (size_t)(ceil_div(Kcap, k_chunk) + kPlanExtra) * 256 * 128 * sizeof(float);
 }
 
 extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
@@ -504,15 +546,16 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
     return fail(MVB_ERR_ARG, "mvb_herk_reduce: bad arguments");
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
+  const int nsm = num_sms();
   const float *part = static_cast<const float *>(ws);
   cudaStream_t s = as_stream(stream);
   if (!pairs) {
     const int grid = n_tiles * 16;
     if (out_c128)
-      herk_reduce_all_kernel<double2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nant,
+      herk_reduce_all_kernel<double2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, nant,
                                                            nfeed, out, accumulate);
     else
-      herk_reduce_all_kernel<float2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nant,
+      herk_reduce_all_kernel<float2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, nant,
                                                           nfeed, out, accumulate);
   } else {
     if (npairs == 0) return MVB_OK;
@@ -520,11 +563,11 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
     const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), (int64_t)num_sms() * 8);
     if (out_c128)
       herk_reduce_pairs_kernel<double2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
-                                                                         k_chunk, nfeed, pairs, npairs, out,
+                                                                         k_chunk, nsm, nfeed, pairs, npairs, out,
                                                                          accumulate);
     else
       herk_reduce_pairs_kernel<float2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
-                                                                        k_chunk, nfeed, pairs, npairs, out,
+                                                                        k_chunk, nsm, nfeed, pairs, npairs, out,
                                                                         accumulate);
   }
   return check_launch("herk_reduce");

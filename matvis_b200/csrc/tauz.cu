@@ -28,8 +28,51 @@ __device__ __forceinline__ float tf32_rna(float v) {
   return __uint_as_float(r);
 }
 
-// Writes X consecutive values (one per axis) of the P split terms of one real
-// component into planes [2p + comp] of a panel row.
+// Writes NV consecutive real values of one component (c = 0 real, 1 imaginary)
+// as the P split terms into planes [2p + c] of a panel row, with vector stores:
+// NV = 8 bf16 (16 bytes) or NV = 4 bf16 (8 bytes), NV float32 (16-byte stores).
+template <int MODE, int NV>
+__device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t off, int comp, const float *v) {
+  if constexpr (MODE == MVB_GEMM_TF32_3) {
+    float hi[NV], lo[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      hi[i] = tf32_rna(v[i]);
+      lo[i] = tf32_rna(v[i] - hi[i]);
+    }
+    float *p0 = static_cast<float *>(z) + off + (int64_t)(0 + comp) * plane_stride;
+    float *p1 = static_cast<float *>(z) + off + (int64_t)(2 + comp) * plane_stride;
+#pragma unroll
+    for (int i = 0; i < NV; i += 4) {
+      *reinterpret_cast<float4 *>(p0 + i) = make_float4(hi[i], hi[i + 1], hi[i + 2], hi[i + 3]);
+      *reinterpret_cast<float4 *>(p1 + i) = make_float4(lo[i], lo[i + 1], lo[i + 2], lo[i + 3]);
+    }
+  } else {
+    constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
+    float r[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) r[i] = v[i];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      uint32_t w[NV / 2];
+#pragma unroll
+      for (int i = 0; i < NV; i += 2) {
+        const __nv_bfloat16 t0 = __float2bfloat16_rn(r[i]);
+        const __nv_bfloat16 t1 = __float2bfloat16_rn(r[i + 1]);
+        r[i] -= __bfloat162float(t0);
+        r[i + 1] -= __bfloat162float(t1);
+        w[i / 2] = (uint32_t)__bfloat16_as_ushort(t0) | ((uint32_t)__bfloat16_as_ushort(t1) << 16);
+      }
+      __nv_bfloat16 *pp = static_cast<__nv_bfloat16 *>(z) + off + (int64_t)(2 * p + comp) * plane_stride;
+      if constexpr (NV == 8)
+        *reinterpret_cast<uint4 *>(pp) = make_uint4(w[0], w[1], w[2], w[3]);
+      else
+        *reinterpret_cast<uint2 *>(pp) = make_uint2(w[0], w[1]);
+    }
+  }
+}
+
+// Single-value writer kept for the pack kernel (2 consecutive values).
 template <int MODE>
 struct PanelWriter {
   static constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
@@ -78,84 +121,107 @@ struct PanelWriter {
   }
 };
 
-constexpr int kTauZThreads = 128;
+constexpr int kTauZThreads = 64;
+constexpr int kTauZSrc = 4;      // consecutive sources per thread
 constexpr int kTauZAnts = 8;     // antennas per CTA
 constexpr int kTauZMaxBFX = 16;  // nbeam * F * X staged per source
+constexpr int kTauZBlockSrc = kTauZThreads * kTauZSrc;
 
-// grid.x: source blocks of kTauZThreads, grid.y: antenna blocks.
+// grid.x: blocks of kTauZBlockSrc sources, grid.y: antenna blocks.
 // EXT = 0: phase from antpos . crd (fused tau); EXT = 1 / 2: phase factor read
 // from a caller exptau (A, e_ld) in complex64 / complex128, multiplied by sflux.
-template <int MODE, int EXT = 0>
+template <int MODE, int X, int EXT = 0>
 __global__ void __launch_bounds__(kTauZThreads)
     tau_z_kernel(const double *__restrict__ antpos, int A, double f_over_c, const double *__restrict__ crd, int64_t ld,
                  const int32_t *__restrict__ n_dev, int64_t nsrc, const float *__restrict__ sflux,
                  const int32_t *__restrict__ sidx, const float2 *__restrict__ beam, int64_t beam_ld, int nbeam,
-                 const int32_t *__restrict__ beam_idx, int F, int X, void *__restrict__ z, int64_t Mpad,
-                 int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
-  __shared__ float2 bsm[kTauZMaxBFX][kTauZThreads];
+                 const int32_t *__restrict__ beam_idx, int F, void *__restrict__ z, int64_t Mpad, int64_t Kcap,
+                 const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
+  __shared__ float2 bsm[kTauZMaxBFX][kTauZThreads][kTauZSrc];
   const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
   const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
-  const int64_t s = (int64_t)blockIdx.x * kTauZThreads + threadIdx.x;
-  if ((int64_t)blockIdx.x * kTauZThreads >= s_end) return;  // uniform per CTA
-  const bool live = s < n;
-  const bool write = s < s_end;
+  const int64_t s0 = ((int64_t)blockIdx.x * kTauZThreads + threadIdx.x) * kTauZSrc;
+  if ((int64_t)blockIdx.x * kTauZBlockSrc >= s_end) return;  // uniform per CTA
+  const bool write = s0 < s_end;  // s_end is a multiple of kTauZSrc (64 / X)
 
-  double cx = 0, cy = 0, cz = 0;
-  float sf = 0.f;
-  if (live) {
-    if (EXT == 0) {
-      cx = crd[s];
-      cy = crd[ld + s];
-      cz = crd[2 * ld + s];
+  double cx[kTauZSrc], cy[kTauZSrc], cz[kTauZSrc];
+  float sf[kTauZSrc];
+#pragma unroll
+  for (int j = 0; j < kTauZSrc; ++j) {
+    const int64_t s = s0 + j;
+    const bool live = s < n;
+    cx[j] = cy[j] = cz[j] = 0.0;
+    sf[j] = 0.f;
+    if (live) {
+      if (EXT == 0) {
+        cx[j] = crd[s];
+        cy[j] = crd[ld + s];
+        cz[j] = crd[2 * ld + s];
+      }
+      sf[j] = sflux[sidx ? sidx[s] : s];
     }
-    sf = sflux[sidx ? sidx[s] : s];
   }
   const int nbfx = nbeam * F * X;
-  for (int q = 0; q < nbfx; ++q) bsm[q][threadIdx.x] = live ? beam[(int64_t)q * beam_ld + s] : make_float2(0.f, 0.f);
-  // (each thread reads only its own column of bsm: no barrier needed)
+  for (int q = 0; q < nbfx; ++q)
+#pragma unroll
+    for (int j = 0; j < kTauZSrc; ++j)
+      bsm[q][threadIdx.x][j] = (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
+  // (each thread reads only its own entries of bsm: no barrier needed)
 
   const int a0 = blockIdx.y * kTauZAnts;
   const int a1 = min(a0 + kTauZAnts, A);
   const int64_t plane = Mpad * Kcap;
   for (int a = a0; a < a1; ++a) {
-    float er = 0.f, ei = 0.f;
-    if (live && EXT == 1) {
-      const float2 e = static_cast<const float2 *>(ext)[(int64_t)a * e_ld + s];
-      er = e.x * sf;
-      ei = e.y * sf;
-    } else if (live && EXT == 2) {
-      const double2 e = static_cast<const double2 *>(ext)[(int64_t)a * e_ld + s];
-      er = (float)(e.x * (double)sf);
-      ei = (float)(e.y * (double)sf);
-    } else if (live) {
-      const double dx = antpos[3 * a], dy = antpos[3 * a + 1], dz = antpos[3 * a + 2];
-      const double t = (dx * cx + dy * cy + dz * cz) * f_over_c;
-      const double r = t - rint(t);
-      float sn, cs;
-      sincospif((float)(2.0 * r), &sn, &cs);
-      er = cs * sf;
-      ei = sn * sf;
+    float er[kTauZSrc], ei[kTauZSrc];
+    double dx = 0, dy = 0, dz = 0;
+    if (EXT == 0) {
+      dx = antpos[3 * a];
+      dy = antpos[3 * a + 1];
+      dz = antpos[3 * a + 2];
+    }
+#pragma unroll
+    for (int j = 0; j < kTauZSrc; ++j) {
+      er[j] = ei[j] = 0.f;
+      if (s0 + j >= n) continue;
+      if (EXT == 1) {
+        const float2 e = static_cast<const float2 *>(ext)[(int64_t)a * e_ld + s0 + j];
+        er[j] = e.x * sf[j];
+        ei[j] = e.y * sf[j];
+      } else if (EXT == 2) {
+        const double2 e = static_cast<const double2 *>(ext)[(int64_t)a * e_ld + s0 + j];
+        er[j] = (float)(e.x * (double)sf[j]);
+        ei[j] = (float)(e.y * (double)sf[j]);
+      } else {
+        const double t = (dx * cx[j] + dy * cy[j] + dz * cz[j]) * f_over_c;
+        const double r = t - rint(t);
+        float sn, cs;
+        sincospif((float)(2.0 * r), &sn, &cs);
+        er[j] = cs * sf[j];
+        ei[j] = sn * sf[j];
+      }
     }
     const int b = beam_idx ? beam_idx[a] : 0;
     for (int f = 0; f < F; ++f) {
-      float vr[2], vi[2];
-      for (int x = 0; x < X; ++x) {
-        const float2 bv = bsm[(b * F + f) * X + x][threadIdx.x];
-        vr[x] = er * bv.x - ei * bv.y;
-        vi[x] = er * bv.y + ei * bv.x;
-      }
+      float vr[kTauZSrc * X], vi[kTauZSrc * X];
+#pragma unroll
+      for (int j = 0; j < kTauZSrc; ++j)
+#pragma unroll
+        for (int x = 0; x < X; ++x) {
+          const float2 bv = bsm[(b * F + f) * X + x][threadIdx.x][j];
+          vr[j * X + x] = er[j] * bv.x - ei[j] * bv.y;
+          vi[j * X + x] = er[j] * bv.y + ei[j] * bv.x;
+        }
       if (!write) continue;
       const int64_t m = (int64_t)a * F + f;
-      const int64_t off = m * Kcap + s * X;
+      const int64_t off = m * Kcap + s0 * X;
       if constexpr (MODE == MVB_Z_C64) {
         float2 *zp = static_cast<float2 *>(z) + off;
-        if (X == 2)
-          *reinterpret_cast<float4 *>(zp) = make_float4(vr[0], vi[0], vr[1], vi[1]);
-        else
-          *zp = make_float2(vr[0], vi[0]);
+#pragma unroll
+        for (int i = 0; i < kTauZSrc * X; i += 2)
+          *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
       } else {
-        PanelWriter<MODE>::put(z, plane, off, 0, vr, X);
-        PanelWriter<MODE>::put(z, plane, off, 1, vi, X);
+        put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr);
+        put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi);
       }
     }
   }
@@ -253,19 +319,25 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z: Kcap too small for nsrc * nax");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
-  dim3 grid((unsigned)ceil_div(s_max, kTauZThreads), (unsigned)ceil_div(A, kTauZAnts));
+  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
   const double foc = freq * kInvC;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_TAUZ(M)                                                                                                  \
-  tau_z_kernel<M><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, \
-                                                beam_idx, F, X, z, Mpad, Kcap)
+#define MVB_TAUZ(M, XX)                                                                                              \
+  tau_z_kernel<M, XX><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld,   \
+                                                    nbeam, beam_idx, F, z, Mpad, Kcap)
+#define MVB_TAUZ2(M) \
+  if (X == 2)        \
+    MVB_TAUZ(M, 2);  \
+  else               \
+    MVB_TAUZ(M, 1)
   switch (mode) {
-    case MVB_GEMM_BF16_3: MVB_TAUZ(MVB_GEMM_BF16_3); break;
-    case MVB_GEMM_BF16_6: MVB_TAUZ(MVB_GEMM_BF16_6); break;
-    case MVB_GEMM_TF32_3: MVB_TAUZ(MVB_GEMM_TF32_3); break;
-    default: MVB_TAUZ(MVB_Z_C64); break;
+    case MVB_GEMM_BF16_3: MVB_TAUZ2(MVB_GEMM_BF16_3); break;
+    case MVB_GEMM_BF16_6: MVB_TAUZ2(MVB_GEMM_BF16_6); break;
+    case MVB_GEMM_TF32_3: MVB_TAUZ2(MVB_GEMM_TF32_3); break;
+    default: MVB_TAUZ2(MVB_Z_C64); break;
   }
+#undef MVB_TAUZ2
 #undef MVB_TAUZ
   return check_launch("tau_z_kernel");
 }
@@ -310,17 +382,22 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_z_from_exptau: Kcap too small");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
-  dim3 grid((unsigned)ceil_div(s_max, kTauZThreads), (unsigned)ceil_div(A, kTauZAnts));
+  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_ZX(M, E)                                                                                                  \
-  tau_z_kernel<M, E><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, nullptr, bm,     \
-                                                   beam_ld, nbeam, beam_idx, F, X, z, Mpad, Kcap, exptau, e_ld)
-#define MVB_ZX2(M) \
-  if (e_c128)      \
-    MVB_ZX(M, 2);  \
-  else             \
-    MVB_ZX(M, 1)
+#define MVB_ZX(M, XX, E)                                                                                              \
+  tau_z_kernel<M, XX, E><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, nullptr, bm, \
+                                                       beam_ld, nbeam, beam_idx, F, z, Mpad, Kcap, exptau, e_ld)
+#define MVB_ZX3(M, E) \
+  if (X == 2)         \
+    MVB_ZX(M, 2, E);  \
+  else                \
+    MVB_ZX(M, 1, E)
+#define MVB_ZX2(M)    \
+  if (e_c128)         \
+    MVB_ZX3(M, 2);    \
+  else                \
+    MVB_ZX3(M, 1)
   switch (mode) {
     case MVB_GEMM_BF16_3: MVB_ZX2(MVB_GEMM_BF16_3); break;
     case MVB_GEMM_BF16_6: MVB_ZX2(MVB_GEMM_BF16_6); break;
@@ -328,6 +405,7 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
     default: MVB_ZX2(MVB_Z_C64); break;
   }
 #undef MVB_ZX2
+#undef MVB_ZX3
 #undef MVB_ZX
   return check_launch("tau_z_kernel(exptau)");
 }

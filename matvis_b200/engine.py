@@ -25,7 +25,12 @@ from . import _lib
 from .beams import B200BeamInterpolator, GaussianBeam, GridBeam
 from .coordinates import eci_to_enu_matrix, point_source_crd_eq
 from .getz import ZMatrixCalc
+from .autotune import tune_k_chunk
 from .matprod import B200MatMul, B200VectorDot, choose_k_chunk
+
+#: k-slice of the Hermitian product before autotuning (fastest at the
+#: HERA-350-like slice: 2.37 ms at 2048 vs 2.61 ms at 8192 columns).
+DEFAULT_K_CHUNK = 2048
 
 
 @dataclass
@@ -128,7 +133,7 @@ class VisEngine:
                                device=dev)
         if self.method == "MatMul":
             panel = self.zcalc.z
-            self.k_chunk = self.matprod.resolve_k_chunk(panel)
+            self.k_chunk = int(s.k_chunk) if s.k_chunk else DEFAULT_K_CHUNK
             self.matprod.workspace(panel, self.k_chunk)
         self._allocated = True
 
@@ -218,6 +223,11 @@ class VisEngine:
             self.upload()
         self.enqueue()  # warm-up: function attributes, lazy module loading
         torch.cuda.synchronize()
+        if self.method == "MatMul" and not self.spec.k_chunk:
+            # the panel holds the last slice: time the k-slice candidates on it
+            self.k_chunk = tune_k_chunk(self.zcalc.z, self.matprod.mode, self.status)
+            self.matprod.workspace(self.zcalc.z, self.k_chunk)
+            torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())

@@ -146,7 +146,8 @@ class B200MatMul(MatProd):
             return int(self.k_chunk)
         T = panel.Mpad // _lib.TILE
         sm = torch.cuda.get_device_properties(self.device).multi_processor_count
-        return choose_k_chunk(T * (T + 1) // 2, panel.Kcap, sm)
+        kvalid = panel.n_host * panel.nax if panel.n_dev is None else panel.Kcap
+        return choose_k_chunk(T * (T + 1) // 2, kvalid, sm, hi=4096)
 
     def enqueue(self, panel: ZPanel, out: torch.Tensor, accumulate: bool = False, stream=None, k_chunk=None):
         kc = k_chunk or self.resolve_k_chunk(panel)

@@ -1,0 +1,229 @@
+"""Served form: a request loop with continuous batching on one GPU.
+
+Jobs (``JobSpec``) arrive at any time.  The server
+
+* admits a job when its HBM footprint (``engine.estimate_device_bytes``) fits
+  the remaining budget and an execution slot is free -- jobs that arrive while
+  others are on the GPU are admitted as soon as slots and memory free up;
+* keeps every admitted job's sky, beams, Z panel and partial visibilities
+  resident on the device, and gives it its own CUDA stream;
+* advances the active jobs one time step at a time, round robin, so their
+  kernels overlap on the device;
+* copies each finished job's visibilities to pinned host memory, records its
+  latency (submission to result on the host), and frees its memory.
+
+Each job's arithmetic is exactly the single-job path (same kernels, same
+deterministic reduction order), so a result is bit-identical alone and in a
+mix.  ``latency_summary`` reports p50 / p99 and the throughput.
+"""
+
+from __future__ import annotations
+
+import threading
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import JobSpec, VisEngine, estimate_device_bytes
+
+
+@dataclass
+class _Job:
+    jid: int
+    spec: JobSpec
+    t_submit: float
+    engine: VisEngine | None = None
+    stream: torch.cuda.Stream | None = None
+    next_t: int = 0
+    done_event: torch.cuda.Event | None = None
+    host: torch.Tensor | None = None
+    footprint: int = 0
+    t_admit: float = 0.0
+    t_done: float = 0.0
+    terms: float = 0.0
+    error: str | None = None
+
+
+@dataclass
+class JobResult:
+    jid: int
+    vis: np.ndarray | None
+    latency_s: float
+    queue_s: float
+    terms: float
+    error: str | None = None
+
+
+class VisServer:
+    """Continuous-batching visibility server on one device."""
+
+    def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 8, steps_per_turn: int = 1):
+        self.device = _lib.require_cuda(device)
+        free = torch.cuda.mem_get_info(self.device)[0]
+        self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
+        self.max_active = max_active
+        self.steps_per_turn = steps_per_turn
+        self._pending: deque[_Job] = deque()
+        self._active: list[_Job] = []
+        self._finishing: list[_Job] = []
+        self._results: dict[int, JobResult] = {}
+        self._lock = threading.Lock()
+        self._next_id = 0
+        self.in_use = 0
+        self.peak_in_use = 0
+        self.max_concurrent = 0
+
+    # ------------------------------------------------------------------ API
+    def submit(self, spec: JobSpec, t_submit: float | None = None) -> int:
+        fp = estimate_device_bytes(spec)
+        if fp > self.budget:
+            raise ValueError(f"job needs {fp / 1e9:.2f} GB of HBM, more than the server budget {self.budget / 1e9:.2f} GB")
+        with self._lock:
+            jid = self._next_id
+            self._next_id += 1
+            self._pending.append(_Job(jid=jid, spec=spec, t_submit=time.perf_counter() if t_submit is None else t_submit,
+                                      footprint=fp))
+        return jid
+
+    def result(self, jid: int) -> JobResult | None:
+        return self._results.get(jid)
+
+    @property
+    def results(self) -> dict[int, JobResult]:
+        return self._results
+
+    def idle(self) -> bool:
+        with self._lock:
+            return not self._pending and not self._active and not self._finishing
+
+    # ------------------------------------------------------------ scheduling
+    def _admit(self):
+        with self._lock:
+            while self._pending and len(self._active) < self.max_active:
+                job = self._pending[0]
+                if self.in_use + job.footprint > self.budget:
+                    break
+                self._pending.popleft()
+                self.in_use += job.footprint
+                self.peak_in_use = max(self.peak_in_use, self.in_use)
+                job.t_admit = time.perf_counter()
+                job.stream = torch.cuda.Stream(device=self.device)
+                with torch.cuda.stream(job.stream):
+                    job.engine = VisEngine(job.spec, device=self.device)
+                    job.engine.allocate()
+                    job.engine.upload()
+                    job.engine.status.zero_()
+                self._active.append(job)
+        self.max_concurrent = max(self.max_concurrent, len(self._active))
+
+    def _advance(self):
+        still = []
+        for job in self._active:
+            eng = job.engine
+            nt = len(eng.lsts)
+            with torch.cuda.stream(job.stream):
+                for _ in range(self.steps_per_turn):
+                    if job.next_t >= nt:
+                        break
+                    eng.enqueue_time(job.next_t, stream=job.stream)
+                    job.next_t += 1
+                if job.next_t >= nt:
+                    job.host = torch.empty(eng.vis.shape, dtype=eng.vis.dtype, pin_memory=True)
+                    job.host.copy_(eng.vis, non_blocking=True)
+                    job.done_event = torch.cuda.Event()
+                    job.done_event.record(job.stream)
+                    self._finishing.append(job)
+                    continue
+            still.append(job)
+        self._active = still
+
+    def _retire(self):
+        keep = []
+        for job in self._finishing:
+            if not job.done_event.query():
+                keep.append(job)
+                continue
+            job.t_done = time.perf_counter()
+            eng = job.engine
+            err = None
+            try:
+                _lib.check_status_word(eng.status, f"job {job.jid}")
+            except Exception as exc:  # recorded per job; the server keeps running
+                err = str(exc)
+            vis = job.host.numpy()
+            if not job.spec.polarized:
+                vis = vis[..., 0, 0]
+            A = eng.nant
+            terms = float(A * A * len(eng.freqs)) * self._n_above_total(job)
+            self._results[job.jid] = JobResult(jid=job.jid, vis=None if err else vis, latency_s=job.t_done - job.t_submit,
+                                               queue_s=job.t_admit - job.t_submit, terms=terms, error=err)
+            with self._lock:
+                self.in_use -= job.footprint
+            job.engine = None
+            job.stream = None
+        self._finishing = keep
+
+    @staticmethod
+    def _n_above_total(job: _Job) -> float:
+        """Sum over times of the above-horizon counts (host FP64 rotation, same op order)."""
+        eng = job.engine
+        eci = eng.eci_host
+        tot = 0
+        for R in eng.rot:
+            z = (R[2, 0] * eci[0] + R[2, 1] * eci[1]) + R[2, 2] * eci[2]
+            tot += int((z > 0).sum())
+        return float(tot)
+
+    def poll(self):
+        """One scheduling turn: admit, advance every active job by a time step, retire."""
+        self._admit()
+        self._advance()
+        self._retire()
+
+    def run_until_idle(self, timeout_s: float = 3600.0):
+        t0 = time.perf_counter()
+        while not self.idle():
+            self.poll()
+            if not self._active and self._finishing:
+                time.sleep(0.0005)
+            if time.perf_counter() - t0 > timeout_s:
+                raise TimeoutError("server did not drain in time")
+
+    def serve_stream(self, arrivals: list[tuple[float, JobSpec]], timeout_s: float = 3600.0) -> list[int]:
+        """Submit jobs at their arrival offsets (seconds from now) while serving."""
+        t0 = time.perf_counter()
+        ids = []
+        i = 0
+        arrivals = sorted(arrivals, key=lambda a: a[0])
+        while i < len(arrivals) or not self.idle():
+            now = time.perf_counter() - t0
+            while i < len(arrivals) and arrivals[i][0] <= now:
+                ids.append(self.submit(arrivals[i][1], t_submit=t0 + arrivals[i][0]))
+                i += 1
+            if self.idle() and i < len(arrivals):
+                time.sleep(min(0.001, max(0.0, arrivals[i][0] - now)))
+                continue
+            self.poll()
+            if time.perf_counter() - t0 > timeout_s:
+                raise TimeoutError("serve_stream did not finish in time")
+        return ids
+
+
+def latency_summary(results: dict[int, JobResult]) -> dict:
+    ok = [r for r in results.values() if r.error is None]
+    if not ok:
+        return {"jobs": 0}
+    lat = np.array([r.latency_s for r in ok])
+    q = np.array([r.queue_s for r in ok])
+    return {
+        "jobs": len(ok),
+        "errors": len(results) - len(ok),
+        "p50_s": float(np.percentile(lat, 50)),
+        "p99_s": float(np.percentile(lat, 99)),
+        "mean_queue_s": float(q.mean()),
+        "terms": float(sum(r.terms for r in ok)),
+    }
