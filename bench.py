@@ -60,6 +60,11 @@ def parse():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--serve", action="store_true", help="served form: Poisson job stream, p50/p99 latency")
+    ap.add_argument("--serve-jobs", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-nsrc-max", type=int, default=500_000)
+    ap.add_argument("--serve-max-active", type=int, default=8)
     return ap.parse_args()
 
 
@@ -308,20 +313,20 @@ def run_b200(args, rank, world, local_rank):
             if r == 2:
                 h0.record(hs)
             _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), eng.matprod.mode, panel.Mpad, panel.Kcap,
-                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, _lib.ptr(ws), ws.numel(),
+                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, 0, _lib.ptr(ws), ws.numel(),
                                          _lib.ptr(eng.status), _lib.stream_handle(hs)))
         h1.record(hs)
     torch.cuda.synchronize()
     herk_ms = h0.elapsed_time(h1) / reps
     algo_flops = 4.0 * M * (M + 1) * kvalid
     T = panel.Mpad // 128
-    nprod = {"bf16x3": 3, "bf16x6": 6, "tf32x3": 3}[args.gemm_mode]
+    nprod = _lib.GEMM_PRODUCTS[_lib.GEMM_MODES[args.gemm_mode]]
     exec_flops = 8.0 * (T * (T + 1) // 2) * 128 * 128 * kvalid * nprod
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     bf16_peak = peaks.get("bf16_tflops", 1590.0)
     peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
     achieved = algo_flops / (herk_ms / 1000.0) / 1e12
-    tensor_peak = bf16_peak if args.gemm_mode.startswith("bf16") else bf16_peak / 2
+    tensor_peak = bf16_peak / 2 if args.gemm_mode.startswith("tf32") else bf16_peak
     roofline = {
         "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
         "traffic": None, "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
@@ -335,7 +340,7 @@ def run_b200(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16" if args.gemm_mode.startswith("bf16") else "tf32",
+        "dtype": args.gemm_mode[:4],
         "data": "synthetic (seeded; HEALPix nside=128 centres, HERA-350-like array, dipole-like beams)",
         "config": {
             "workload": f"config2 HERA-350-like: 350 ant x {len(cfg['ra'])} src x {len(cfg['freqs'])} freq x "
@@ -393,8 +398,43 @@ def run_b200(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_serve(args, local_rank):
+    """Served form (config 5): Poisson arrivals into the continuous-batching server."""
+    import torch
+
+    from matvis_b200 import workloads as wl
+    from matvis_b200.serve import VisServer, latency_summary
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    jobs = wl.config5_jobs(njobs=args.serve_jobs, rate_hz=args.serve_rate, nsrc_max=args.serve_nsrc_max)
+    for _, spec in jobs:
+        spec.gemm_mode = args.gemm_mode
+    warm = VisServer(device=dev, max_active=args.serve_max_active)
+    warm.serve_stream([(0.0, jobs[0][1])])  # kernel warm-up, not timed
+    srv = VisServer(device=dev, max_active=args.serve_max_active)
+    t0 = time.perf_counter()
+    srv.serve_stream(jobs)
+    wall = time.perf_counter() - t0
+    summ = latency_summary(srv.results)
+    line = {
+        "metric": "served form: job latency p50/p99 and throughput", "impl": "b200", "unit": UNIT,
+        "throughput": summ["terms"] / wall, "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
+        "mean_queue_s": summ["mean_queue_s"], "jobs": summ["jobs"], "errors": summ["errors"], "wall_s": wall,
+        "arrival_span_s": jobs[-1][0], "max_concurrent": srv.max_concurrent, "peak_hbm_gb": srv.peak_in_use / 1e9,
+        "config": {"workload": f"config5 stream: {args.serve_jobs} jobs, Poisson {args.serve_rate}/s, Nant log-U[16,512], "
+                               f"Nsrc log-U[1e3,{args.serve_nsrc_max}], Nf U{{1..32}}, Nt U{{1..16}}, Gaussian or "
+                               f"polarised grid beam", "gemm_mode": args.gemm_mode,
+                   "max_active": args.serve_max_active},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.serve:
+        run_serve(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

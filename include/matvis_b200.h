@@ -22,7 +22,10 @@
  *     with plane q = 2 p + c holding split term p (p = 0 most significant)
  *     of component c (0 = real, 1 = imaginary).  Row m = ant * nfeed + feed,
  *     column k = src * nax + ax.  Rows >= M and columns >= K_valid are zero.
- *     Element type: bfloat16 for MVB_GEMM_BF16_*, float32 for MVB_GEMM_TF32_3.
+ *     Element type: bfloat16 for MVB_GEMM_BF16_*, float32 for MVB_GEMM_TF32_3,
+ *     float16 for MVB_GEMM_F16_3, whose panel holds s*Z for a power-of-two
+ *     scale s (zscale) chosen by the caller so that max |s Z| < 2^15; the
+ *     product's reduction multiplies by vscale = 1 / s^2.
  */
 #ifndef MATVIS_B200_H
 #define MATVIS_B200_H
@@ -53,6 +56,7 @@ extern "C" {
 #define MVB_GEMM_BF16_6 1 /* 3-term bf16 split, 6 products (order <= 2)      */
 #define MVB_GEMM_TF32_3 2 /* 2-term tf32 split, 3 products (3xTF32)          */
 #define MVB_Z_C64 3       /* plain complex64 Z (M, Kcap), for the pair loop */
+#define MVB_GEMM_F16_3 4  /* 2-term fp16 split of s*Z (s a power of two), 3 products */
 
 /* ---- library ----------------------------------------------------------- */
 int mvb_version(void);
@@ -68,6 +72,15 @@ int mvb_device_info(int *sm_count, int *cc_major, int *cc_minor);
  * coordinates.eci_to_enu_matrix @ point_source_crd_eq, coordinates.py:91-125,
  * 174-200).  eci and topo are SoA with leading dimension N. */
 int mvb_rotate(const double *eci, int64_t N, const double *R, double *topo, void *stream);
+
+/* ERFA-style apparent place of every source (SoA (3, N) in and out, FP64):
+ * light deflection by the Sun, aberration and bias-precession-nutation, the
+ * cached "BCRS" directions of CoordinateRotationERFA._set_bcrs
+ * (cpu/coords.py:118-215; the per-source _ld kernel of gpu/coords.py:7-53).
+ * astrom: 18 host doubles {eh[3], em, dlim, v[3], bm1, bpn[9] (row-major)},
+ * the pyerfa apco quantities.  The CIRS -> ENU step (_atioq) is a 3x3 applied
+ * with mvb_rotate. */
+int mvb_bcrs(const double *eci, int64_t N, const double *astrom, double *bcrs, void *stream);
 
 /* ---- A4: horizon selection ---------------------------------------------- */
 /* Bytes of workspace mvb_horizon_compact needs for a chunk of `count` sources. */
@@ -144,7 +157,8 @@ size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap);
  * core/getz.py:52-105) with no exptau round trip through HBM. */
 int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
               int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld, int nbeam,
-              const int32_t *beam_idx, int F, int X, int mode, void *z, int64_t Mpad, int64_t Kcap, void *stream);
+              const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap,
+              void *stream);
 /* Z panel (or plain complex64 Z) from a caller exptau (A, e_ld), complex64
  * (e_c128 = 0) or complex128: Z[a*F+f, s*X+x] = exptau[a, s] * sflux[s] *
  * beam[bidx[a], f, x, s] for s < nsrc, zeros up to roundup(nsrc*X, 64)/X.
@@ -152,13 +166,16 @@ int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64
  * not modified (the reference scales it in place). */
 int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, int A, int64_t nsrc, const float *sflux,
                       const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X, int mode,
-                      void *z, int64_t Mpad, int64_t Kcap, void *stream);
+                      float zscale, void *z, int64_t Mpad, int64_t Kcap, void *stream);
 /* Z panel (or plain complex64 Z) from a caller complex matrix z (M, K) with row
  * pitch ldz elements, complex64 (z_c128 = 0) or complex128.  Columns in
  * [K, roundup(K, 64)) are zero-filled.  Serves MatProd.__call__(z, chunk)
  * on an externally built Z (core/matprod.py:83-101). */
-int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, void *z, int64_t Mpad,
-               int64_t Kcap, void *stream);
+int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, float zscale, void *z,
+               int64_t Mpad, int64_t Kcap, void *stream);
+/* max |z| over n complex values (complex64 or complex128) -> *out (device
+ * float32, caller-zeroed); used to choose the MVB_GEMM_F16_3 scale. */
+int mvb_absmax(const void *z, int z_c128, int64_t n, float *out, void *stream);
 
 /* ---- A7: Hermitian product on the tensor cores ------------------------------ */
 /* In the entry points below the valid K extent of the panel is
@@ -171,21 +188,26 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
  * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05
  * tensor cores with TMEM accumulators, fed by TMA (cp.async.bulk.tensor,
  * 32-byte swizzle); mode MVB_GEMM_* selects the split precision.
+ * drain_ksteps (1 or 2; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
+ * number of 32-byte k-steps summed in one TMEM block before the block is added
+ * to FP32 registers: the tensor core rounds its accumulator toward zero at every
+ * instruction, so short blocks bound that drift.
  * Replaces GPUMatMul.compute -> zdotz -> cublas.c/zgemm (gpu/matprod.py:31-36,
  * gpu/_cublas.py:7-65) and CPUMatMul.compute's z.conj().dot(z.T)
  * (cpu/matprod.py:11-32); computes only the upper-triangle tiles. */
 int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
-             int k_chunk, void *ws, size_t ws_bytes, int32_t *status, void *stream);
+             int k_chunk, int drain_ksteps, void *ws, size_t ws_bytes, int32_t *status, void *stream);
 /* Reduces the FP32 partial tiles in FP64 and writes the visibilities in the
  * reference layout out[pair, p, q] = V[ant_i*F + q, ant_j*F + p]
  * (cpu/matprod.py:21-30): all nant^2 pairs (pairs = NULL, i slow) or the
  * npairs listed in pairs (int32 [npairs][2]).  out: complex64 (out_c128 = 0)
- * or complex128; accumulate != 0 adds to out (the sum over source chunks).
+ * or complex128, each sum multiplied by vscale (1 / s^2 for MVB_GEMM_F16_3,
+ * else 1); accumulate != 0 adds to out (the sum over source chunks).
  * Replaces MatProd.sum_chunks and the host transpose/gather of
  * GPUMatMul.sum_chunks (core/matprod.py:103-115, gpu/matprod.py:38-63). */
 int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
                     int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs, void *out, int out_c128,
-                    int accumulate, void *stream);
+                    double vscale, int accumulate, void *stream);
 
 /* ---- A8: per-pair source sums ----------------------------------------------- */
 size_t mvb_vecdot_ws_bytes(int64_t npairs, int nfeed, int64_t Kcap, int k_chunk);

@@ -12,7 +12,7 @@ from ._lib import GEMM_MODES, MatvisB200Error
 from ._utils import get_desired_chunks, get_dtypes, get_required_chunks
 from .beams import B200BeamInterpolator, BeamInterpolator, GaussianBeam, GridBeam
 from .coordinates import SkyCoords, eci_to_enu_matrix, enu_to_az_za, enu_to_eci_matrix, point_source_crd_eq
-from .coords import CoordinateRotation, CoordinateRotationLST
+from .coords import CoordinateRotation, CoordinateRotationERFA, CoordinateRotationLST
 from .engine import JobSpec, VisEngine
 from .getz import ZMatrixCalc, ZPanel
 from .matprod import B200MatMul, B200VectorDot, MatProd
@@ -27,6 +27,7 @@ __all__ = [
     "B200VectorDot",
     "BeamInterpolator",
     "CoordinateRotation",
+    "CoordinateRotationERFA",
     "CoordinateRotationLST",
     "GEMM_MODES",
     "GaussianBeam",

@@ -8,7 +8,7 @@ Device buffers are torch tensors; only their raw pointers cross the boundary.
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_double, c_int, c_int32, c_int64, c_size_t, c_void_p
+from ctypes import c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
 from pathlib import Path
 
 import torch
@@ -31,8 +31,11 @@ GEMM_BF16_3 = 0
 GEMM_BF16_6 = 1
 GEMM_TF32_3 = 2
 Z_C64 = 3
+GEMM_F16_3 = 4
 
-GEMM_MODES = {"bf16x3": GEMM_BF16_3, "bf16x6": GEMM_BF16_6, "tf32x3": GEMM_TF32_3}
+GEMM_MODES = {"bf16x3": GEMM_BF16_3, "bf16x6": GEMM_BF16_6, "tf32x3": GEMM_TF32_3, "fp16x3": GEMM_F16_3}
+#: tensor-core products per complex multiply-accumulate term, per mode
+GEMM_PRODUCTS = {GEMM_BF16_3: 3, GEMM_BF16_6: 6, GEMM_TF32_3: 3, GEMM_F16_3: 3}
 
 K_ALIGN = 64
 TILE = 128
@@ -43,6 +46,7 @@ _SIGNATURES = {
     "mvb_last_error": (ctypes.c_char_p, []),
     "mvb_device_info": (c_int, [_p, _p, _p]),
     "mvb_rotate": (c_int, [_p, c_int64, _p, _p, _p]),
+    "mvb_bcrs": (c_int, [_p, c_int64, _p, _p, _p]),
     "mvb_horizon_ws_bytes": (c_size_t, [c_int64]),
     "mvb_horizon_compact": (
         c_int,
@@ -64,19 +68,21 @@ _SIGNATURES = {
     "mvb_zpanel_bytes": (c_size_t, [c_int, c_int64, c_int64]),
     "mvb_tau_z": (
         c_int,
-        [_p, c_int, c_double, _p, c_int64, _p, c_int64, _p, _p, _p, c_int64, c_int, _p, c_int, c_int, c_int, _p,
-         c_int64, c_int64, _p],
+        [_p, c_int, c_double, _p, c_int64, _p, c_int64, _p, _p, _p, c_int64, c_int, _p, c_int, c_int, c_int, c_float,
+         _p, c_int64, c_int64, _p],
     ),
     "mvb_z_from_exptau": (
         c_int,
-        [_p, c_int, c_int64, c_int, c_int64, _p, _p, c_int64, c_int, _p, c_int, c_int, c_int, _p, c_int64, c_int64, _p],
+        [_p, c_int, c_int64, c_int, c_int64, _p, _p, c_int64, c_int, _p, c_int, c_int, c_int, c_float, _p, c_int64,
+         c_int64, _p],
     ),
-    "mvb_z_pack": (c_int, [_p, c_int, c_int64, c_int64, c_int64, c_int, _p, c_int64, c_int64, _p]),
+    "mvb_z_pack": (c_int, [_p, c_int, c_int64, c_int64, c_int64, c_int, c_float, _p, c_int64, c_int64, _p]),
+    "mvb_absmax": (c_int, [_p, c_int, c_int64, _p, _p]),
     "mvb_herk_ws_bytes": (c_size_t, [c_int64, c_int64, c_int]),
-    "mvb_herk": (c_int, [_p, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, _p, c_size_t, _p, _p]),
+    "mvb_herk": (c_int, [_p, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, _p, c_size_t, _p, _p]),
     "mvb_herk_reduce": (
         c_int,
-        [_p, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, c_int, _p, c_int64, _p, c_int, c_int, _p],
+        [_p, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, c_int, _p, c_int64, _p, c_int, c_double, c_int, _p],
     ),
     "mvb_vecdot_ws_bytes": (c_size_t, [c_int64, c_int, c_int64, c_int]),
     "mvb_vecdot": (
@@ -163,10 +169,19 @@ def zpanel_shape(mode: int, M: int, K: int) -> tuple[int, int]:
 
 
 def zpanel_dtype(mode: int) -> torch.dtype:
-    return {GEMM_BF16_3: torch.bfloat16, GEMM_BF16_6: torch.bfloat16, GEMM_TF32_3: torch.float32, Z_C64: torch.complex64}[
-        mode
-    ]
+    return {GEMM_BF16_3: torch.bfloat16, GEMM_BF16_6: torch.bfloat16, GEMM_TF32_3: torch.float32,
+            GEMM_F16_3: torch.float16, Z_C64: torch.complex64}[mode]
 
 
 def zpanel_planes(mode: int) -> int:
-    return {GEMM_BF16_3: 4, GEMM_BF16_6: 6, GEMM_TF32_3: 4, Z_C64: 1}[mode]
+    return {GEMM_BF16_3: 4, GEMM_BF16_6: 6, GEMM_TF32_3: 4, GEMM_F16_3: 4, Z_C64: 1}[mode]
+
+
+def f16_scale(maxabs: float) -> float:
+    """Power-of-two scale s with max |s Z| < 2^15 (fp16 range), for the fp16x3 panel."""
+    import math
+
+    if not maxabs > 0 or not math.isfinite(maxabs):
+        return 1.0
+    e = math.floor(math.log2(2.0**14 / maxabs))
+    return float(2.0 ** max(min(e, 100), -100))

@@ -48,7 +48,7 @@ def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidat
                 if r == 1:
                     e0.record(s)
                 _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), mode, panel.Mpad, panel.Kcap, _lib.ptr(panel.n_dev),
-                                             panel.n_host, panel.nax, c, _lib.ptr(ws), ws.numel(), _lib.ptr(status),
+                                             panel.n_host, panel.nax, c, 0, _lib.ptr(ws), ws.numel(), _lib.ptr(status),
                                              _lib.stream_handle(s)))
             e1.record(s)
             e1.synchronize()

@@ -101,3 +101,42 @@ class SkyCoords:
 
     def __len__(self):
         return len(self.ra)
+
+
+ASTROM_KEYS = ("eh", "em", "v", "bm1", "bpn", "eral", "xpl", "ypl", "sphi", "cphi")
+
+
+def atioq_matrix(astrom) -> np.ndarray:
+    """CIRS -> ENU rotation of the apparent-place step (the reference's
+    CoordinateRotationERFA._atioq, cpu/coords.py:89-116): Earth rotation angle,
+    polar motion, then hour-angle/declination -> ENU at the observer latitude."""
+    ce, se = np.cos(astrom["eral"]), np.sin(astrom["eral"])
+    c2h = np.array([[ce, se, 0], [-se, ce, 0], [0, 0, 1]], dtype=np.float64)
+    sx, cx = np.sin(astrom["xpl"]), np.cos(astrom["xpl"])
+    sy, cy = np.sin(astrom["ypl"]), np.cos(astrom["ypl"])
+    pm = np.array([[cx, 0, sx], [sx * sy, cy, -cx * sy], [-sx * cy, sy, cx * cy]], dtype=np.float64)
+    enu = np.array([[0, 1, 0], [-astrom["sphi"], 0, astrom["cphi"]], [astrom["cphi"], 0, astrom["sphi"]]],
+                   dtype=np.float64)
+    return enu.dot(pm.dot(c2h))
+
+
+def pack_astrom(astrom, dlim: float = 1e-6) -> np.ndarray:
+    """The 18 doubles mvb_bcrs takes: eh[3], em, dlim, v[3], bm1, bpn[9]."""
+    return np.ascontiguousarray(np.concatenate([
+        np.asarray(astrom["eh"], dtype=np.float64).reshape(3), [float(astrom["em"]), dlim],
+        np.asarray(astrom["v"], dtype=np.float64).reshape(3), [float(astrom["bm1"])],
+        np.asarray(astrom["bpn"], dtype=np.float64).reshape(9)]))
+
+
+def bcrs_refresh_plan(time_s, update_every: float) -> list[bool]:
+    """Which time steps recompute the apparent-place directions: the first, and
+    any step more than update_every seconds after the last refresh
+    (cpu/coords.py:194-199)."""
+    plan, last = [], None
+    for t, ts in enumerate(np.asarray(time_s, dtype=np.float64)):
+        if last is None or ts - time_s[last] > update_every:
+            plan.append(True)
+            last = t
+        else:
+            plan.append(False)
+    return plan

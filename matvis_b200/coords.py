@@ -7,9 +7,11 @@ above-horizon coordinates, fluxes and count.  Coordinates stay in float64 on the
 device at both precisions (the reference stores float32 at precision=1,
 core/coords.py:84-97).
 
-The rotation provided here is the rigid LST rotation
+Two rotations are provided: the rigid LST rotation
 ``eci_to_enu_matrix(lst, lat) @ point_source_crd_eq(ra, dec)``
-(coordinates.py:91-125, 174-200), with ``times`` given as LSTs in radians.
+(coordinates.py:91-125, 174-200), with ``times`` given as LSTs in radians, and
+the ERFA-style apparent place (cpu/coords.py:41-230) from per-time astrometry
+parameters, with ``times`` in seconds.
 """
 
 from __future__ import annotations
@@ -21,7 +23,15 @@ import torch
 
 from . import _lib
 from ._lib import check, ptr, stream_handle
-from .coordinates import eci_to_enu_matrix, latitude_of, lsts_of, point_source_crd_eq, radec_of
+from .coordinates import (
+    atioq_matrix,
+    eci_to_enu_matrix,
+    latitude_of,
+    lsts_of,
+    pack_astrom,
+    point_source_crd_eq,
+    radec_of,
+)
 
 
 class CoordinateRotation(ABC):
@@ -135,6 +145,47 @@ class CoordinateRotationLST(CoordinateRotation):
                 stream_handle(stream),
             )
         )
+
+    def rotate(self, t: int):
+        self.enqueue_rotate(t)
+
+
+class CoordinateRotationERFA(CoordinateRotation):
+    """ERFA-style apparent place on the GPU (the reference's CoordinateRotationERFA /
+    GPUCoordinateRotationERFA, cpu/coords.py:41-230, gpu/coords.py:37-53).
+
+    pyerfa is not a dependency, so the per-time astrometry parameters (the
+    ``apco`` output: eh, em, v, bm1, bpn, eral, xpl, ypl, sphi, cphi) are given as
+    ``astrom`` (one dict per time).  ``times`` are the times in seconds (for
+    ``update_bcrs_every``).  Light deflection, aberration and BPN run per source in
+    ``mvb_bcrs`` and are cached until ``update_bcrs_every`` seconds have passed;
+    the CIRS -> ENU rotation runs in ``mvb_rotate``.
+    """
+
+    def __init__(self, update_bcrs_every: float = 0.0, *args, astrom=None, **kwargs):
+        super().__init__(*args, **kwargs)
+        if astrom is None or len(astrom) != len(self.times):
+            raise ValueError("CoordinateRotationERFA needs one astrom parameter dict per time (pyerfa apco output)")
+        self.astrom = list(astrom)
+        self.update_bcrs_every = float(update_bcrs_every)
+        self._time_of_last_evaluation = None
+
+    def setup(self):
+        super().setup()
+        self.eci = torch.as_tensor(np.ascontiguousarray(point_source_crd_eq(self._ra, self._dec)), device=self.device)
+        self._bcrs = torch.zeros_like(self.eci)
+
+    def enqueue_rotate(self, t: int, stream=None):
+        sh = stream_handle(stream)
+        last = self._time_of_last_evaluation
+        # cpu/coords.py:194-215: refresh when more than update_bcrs_every seconds passed
+        if last is None or self.times[t] - self.times[last] > self.update_bcrs_every:
+            a = pack_astrom(self.astrom[t])
+            check(_lib.lib.mvb_bcrs(ptr(self.eci), self.nsrc, a.ctypes.data_as(_lib.c_void_p), ptr(self._bcrs), sh))
+            self._time_of_last_evaluation = t
+        R = np.ascontiguousarray(atioq_matrix(self.astrom[t]))
+        check(_lib.lib.mvb_rotate(ptr(self._bcrs), self.nsrc, R.ctypes.data_as(_lib.c_void_p),
+                                  ptr(self.all_coords_topo), sh))
 
     def rotate(self, t: int):
         self.enqueue_rotate(t)

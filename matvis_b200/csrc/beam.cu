@@ -169,8 +169,8 @@ static int beam_interp_impl(bool azza, const void *grids, int grid_kind, int nbe
   beam_plane_kernel<ST, AZ><<<grid, kBeamThreads, SM, s>>>(g, grid_kind, nbeam, nax, nfeed, nza, naz, bp, crd, ld, n_dev, \
                                                            nsrc, out, out_c128, nout, status)
   if (plane_bytes <= kBeamSmemMax) {
-    int rc = azza ? set_smem_once(reinterpret_cast<const void *>(beam_plane_kernel<true, true>), (int)kBeamSmemMax, 4)
-                  : set_smem_once(reinterpret_cast<const void *>(beam_plane_kernel<true, false>), (int)kBeamSmemMax, 5);
+    int rc = azza ? set_smem_once(reinterpret_cast<const void *>(beam_plane_kernel<true, true>), (int)kBeamSmemMax, 10)
+                  : set_smem_once(reinterpret_cast<const void *>(beam_plane_kernel<true, false>), (int)kBeamSmemMax, 11);
     if (rc) return rc;
     if (azza)
       MVB_BEAM(true, true, plane_bytes);

@@ -68,7 +68,8 @@ struct HerkCfg {
   static constexpr int STAGE_BYTES = 2 * OPER_BYTES;
   static constexpr int STAGES = kSmemBudget / STAGE_BYTES;
   static constexpr int NPROD = P == 3 ? 6 : 3;
-  static constexpr uint32_t FMT = MODE == MVB_GEMM_TF32_3 ? 2u : 1u;
+  // UMMA operand format: 0 = F16, 1 = BF16, 2 = TF32
+  static constexpr uint32_t FMT = MODE == MVB_GEMM_TF32_3 ? 2u : (MODE == MVB_GEMM_F16_3 ? 0u : 1u);
   static constexpr uint32_t ID256 = umma_idesc(FMT, 256, 0);
   static constexpr uint32_t ID128 = umma_idesc(FMT, 128, 0);
   static constexpr uint32_t ID128N = umma_idesc(FMT, 128, 1);
@@ -139,7 +140,8 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
     umma_bf16(d, a, b, idesc, acc);
 }
 
-template <int MODE>
+// KD: k-steps accumulated in one TMEM block before it is drained (1 or 2).
+template <int MODE, int KD>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const __grid_constant__ CUtensorMap zmap, int T, int n_tiles, const int32_t *__restrict__ n_dev,
                 int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, float *__restrict__ partials,
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       }
     }
   } else if (warp == 1 && lane == 0) {
-    // ---------------- UMMA issuer: one fresh TMEM block per k-step ----------------
+    // ---------------- UMMA issuer: one fresh TMEM block per KD k-steps ----------------
     uint32_t st = 0, ph = 0, buf = 0, dph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
       const int s = u / n_tiles, t = u % n_tiles;
@@ -230,40 +232,51 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
       bool ok = true;
-      for (int ks = 0; ks < nks; ++ks) {
-        if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, kWaitLimitNs) ||
-            !mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
-          atomicOr(status, MVB_DEV_TIMEOUT);
-          abort_flag = 1;
+      for (int g0 = 0; g0 < nks && ok; g0 += KD) {
+        // one TMEM block per group of KD k-steps
+        if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, kWaitLimitNs)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t d = tbase + buf * 256;
-        const uint32_t a_base = smem_u32(smem + (size_t)st * C::STAGE_BYTES);
-        const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
+        const int gl = min(KD, nks - g0);
+        for (int kk = 0; kk < gl; ++kk) {
+          if (!mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_base = smem_u32(smem + (size_t)st * C::STAGE_BYTES);
+          const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
 #pragma unroll
-        for (int q = 0; q < C::NPROD; ++q) {
-          uint32_t pa, pb;
-          product_terms(C::NPROD, q, pa, pb);
-          const uint64_t a_re = umma_desc_sw32(a_base + (2 * pa) * kPlaneBytes);
-          const uint64_t a_im = umma_desc_sw32(a_base + (2 * pa + 1) * kPlaneBytes);
-          const uint64_t b_re = umma_desc_sw32(b_base + (2 * pb) * kPlaneBytes);
-          const uint64_t b_im = umma_desc_sw32(b_base + (2 * pb + 1) * kPlaneBytes);
-          umma<MODE>(d, a_re, b_re, C::ID256, q > 0 ? 1u : 0u);
-          umma<MODE>(d, a_im, b_im, C::ID128, 1u);
-          umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+          for (int q = 0; q < C::NPROD; ++q) {
+            uint32_t pa, pb;
+            product_terms(C::NPROD, q, pa, pb);
+            const uint64_t a_re = umma_desc_sw32(a_base + (2 * pa) * kPlaneBytes);
+            const uint64_t a_im = umma_desc_sw32(a_base + (2 * pa + 1) * kPlaneBytes);
+            const uint64_t b_re = umma_desc_sw32(b_base + (2 * pb) * kPlaneBytes);
+            const uint64_t b_im = umma_desc_sw32(b_base + (2 * pb + 1) * kPlaneBytes);
+            umma<MODE>(d, a_re, b_re, C::ID256, (kk > 0 || q > 0) ? 1u : 0u);
+            umma<MODE>(d, a_im, b_im, C::ID128, 1u);
+            umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+          }
+          tc_commit(&empty_bar[st]);
+          if (++st == C::STAGES) {
+            st = 0;
+            ph ^= 1;
+          }
         }
-        tc_commit(&empty_bar[st]);
+        if (!ok) break;
         tc_commit(&dfull_bar[buf]);
         dph ^= 1u << buf;
         buf ^= 1u;
-        if (++st == C::STAGES) {
-          st = 0;
-          ph ^= 1;
-        }
       }
-      if (!ok) break;
+      if (!ok) {
+        atomicOr(status, MVB_DEV_TIMEOUT);
+        abort_flag = 1;
+        break;
+      }
     }
   } else if (warp >= 2) {
     // ---------------- epilogue: drain every k-step block into FP32 registers ----------------
@@ -280,7 +293,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int64_t klen = min(kc, kvalid - k0);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       bool ok = true;
-      for (int ks = 0; ks < nks; ++ks) {
+      for (int g0 = 0; g0 < nks; g0 += KD) {
         // every lane waits; the vote keeps the warp converged for tcgen05.ld
         ok = __all_sync(0xffffffffu, mbar_wait(&dfull_bar[buf], (dph >> buf) & 1u, kWaitLimitNs));
         if (!ok) break;
@@ -360,7 +373,7 @@ template <typename OT>
 __global__ void __launch_bounds__(256)
     herk_reduce_all_kernel(const float *__restrict__ part, int T, int n_tiles, const int32_t *__restrict__ n_dev,
                            int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, int A, int F,
-                           void *__restrict__ out, int accumulate) {
+                           void *__restrict__ out, double vscale, int accumulate) {
   __shared__ double sre[kRedRows][kRedCols + 1], sim[kRedRows][kRedCols + 1];
   const int t = blockIdx.x / 16, sub = blockIdx.x % 16;
   int I, J;
@@ -387,8 +400,8 @@ __global__ void __launch_bounds__(256)
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    sre[lane][w * 4 + j] = are[j];
-    sim[lane][w * 4 + j] = aim[j];
+    sre[lane][w * 4 + j] = are[j] * vscale;
+    sim[lane][w * 4 + j] = aim[j] * vscale;
   }
   __syncthreads();
 
@@ -418,7 +431,7 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
                                          const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap,
                                          int k_chunk, int nsm, int F, const int32_t *__restrict__ pairs,
                                          int64_t npairs,
-                                         void *__restrict__ out, int accumulate) {
+                                         void *__restrict__ out, double vscale, int accumulate) {
   const int64_t total = npairs * F * F;
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
   int nsplit;
@@ -443,7 +456,7 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
       re += (double)p0[c * 128 + r];
       im += (double)p0[(128 + c) * 128 + r];
     }
-    store_out<OT>(out, e, re, conj ? -im : im, accumulate);
+    store_out<OT>(out, e, re * vscale, (conj ? -im : im) * vscale, accumulate);
   }
 }
 
@@ -453,9 +466,9 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
 // Raises a kernel's dynamic shared-memory limit once per (device, slot); the
 // attribute is not touched again, in particular not during graph capture.
 int set_smem_once(const void *fn, int bytes, int slot) {
-  static bool done[64][8] = {};
+  static bool done[64][16] = {};
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 8)
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 16)
     return fail(MVB_ERR_CUDA, "set_smem_once: bad device");
   if (done[dev][slot]) return MVB_OK;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -477,7 +490,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-template <int MODE>
+template <int MODE, int KD>
 static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
                        int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
   using C = HerkCfg<MODE>;
@@ -488,7 +501,10 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   cuuint64_t strides[2] = {(cuuint64_t)Kcap * C::ES, (cuuint64_t)Mpad * Kcap * C::ES};
   cuuint32_t box[3] = {(cuuint32_t)C::KSTEP, 128u, (cuuint32_t)(2 * C::P)};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = enc(&map, MODE == MVB_GEMM_TF32_3 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+  const CUtensorMapDataType dt = MODE == MVB_GEMM_TF32_3  ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                 : MODE == MVB_GEMM_F16_3 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                          : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  CUresult r = enc(&map, dt, 3,
                    const_cast<void *>(z), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(MVB_ERR_CUDA, "mvb_herk: cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -498,10 +514,10 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   const int64_t max_units = (int64_t)n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
   const int grid = (int)std::min<int64_t>(max_units, nsm);
   const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
-  int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE>), (int)smem, MODE);
+  int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE, KD>), (int)smem, 2 * MODE + (KD - 1));
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
-  herk_kernel<MODE><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials,
+  herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials,
                                                      status);
   return check_launch("herk_kernel");
 }
@@ -517,7 +533,8 @@ extern "C" size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk) {
 }
 
 extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
-                        int kmul, int k_chunk, void *ws, size_t ws_bytes, int32_t *status, void *stream) {
+                        int kmul, int k_chunk, int drain_ksteps, void *ws, size_t ws_bytes, int32_t *status,
+                        void *stream) {
   if (!z || !ws || !status || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || Kcap % kKAlign || k_chunk <= 0 ||
       k_chunk % kKAlign || n_host < 0 || kmul <= 0)
     return fail(MVB_ERR_ARG, "mvb_herk: bad arguments");
@@ -525,22 +542,27 @@ extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, con
   if (reinterpret_cast<uintptr_t>(z) % 16) return fail(MVB_ERR_ARG, "mvb_herk: panel not 16-byte aligned");
   if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk)) return fail(MVB_ERR_ARG, "mvb_herk: workspace too small");
   if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk: panel too large");
+  if (drain_ksteps < 0 || drain_ksteps > 2) return fail(MVB_ERR_ARG, "mvb_herk: drain_ksteps must be 0, 1 or 2");
+  // default: 6-product mode drains every k-step, 3-product modes every 2
+  const int kd = drain_ksteps ? drain_ksteps : (mode == MVB_GEMM_BF16_6 ? 1 : 2);
   cudaStream_t s = as_stream(stream);
   float *part = static_cast<float *>(ws);
+#define MVB_HERK(M)                                                                           \
+  return kd == 1 ? launch_herk<M, 1>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
+                 : launch_herk<M, 2>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s)
   switch (mode) {
-    case MVB_GEMM_BF16_3:
-      return launch_herk<MVB_GEMM_BF16_3>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s);
-    case MVB_GEMM_BF16_6:
-      return launch_herk<MVB_GEMM_BF16_6>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s);
-    case MVB_GEMM_TF32_3:
-      return launch_herk<MVB_GEMM_TF32_3>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s);
+    case MVB_GEMM_BF16_3: MVB_HERK(MVB_GEMM_BF16_3);
+    case MVB_GEMM_BF16_6: MVB_HERK(MVB_GEMM_BF16_6);
+    case MVB_GEMM_TF32_3: MVB_HERK(MVB_GEMM_TF32_3);
+    case MVB_GEMM_F16_3: MVB_HERK(MVB_GEMM_F16_3);
     default: return fail(MVB_ERR_ARG, "mvb_herk: unknown mode %d", mode);
   }
+#undef MVB_HERK
 }
 
 extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
                                int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs,
-                               void *out, int out_c128, int accumulate, void *stream) {
+                               void *out, int out_c128, double vscale, int accumulate, void *stream) {
   if (!ws || !out || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || nant <= 0 || (nfeed != 1 && nfeed != 2) ||
       k_chunk <= 0 || kmul <= 0 || (int64_t)nant * nfeed > Mpad || (pairs && npairs < 0))
     return fail(MVB_ERR_ARG, "mvb_herk_reduce: bad arguments");
@@ -553,10 +575,10 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
     const int grid = n_tiles * 16;
     if (out_c128)
       herk_reduce_all_kernel<double2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, nant,
-                                                           nfeed, out, accumulate);
+                                                           nfeed, out, vscale, accumulate);
     else
       herk_reduce_all_kernel<float2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, nant,
-                                                          nfeed, out, accumulate);
+                                                          nfeed, out, vscale, accumulate);
   } else {
     if (npairs == 0) return MVB_OK;
     const int64_t total = npairs * nfeed * nfeed;
@@ -564,11 +586,11 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
     if (out_c128)
       herk_reduce_pairs_kernel<double2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
                                                                          k_chunk, nsm, nfeed, pairs, npairs, out,
-                                                                         accumulate);
+                                                                         vscale, accumulate);
     else
       herk_reduce_pairs_kernel<float2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
                                                                         k_chunk, nsm, nfeed, pairs, npairs, out,
-                                                                        accumulate);
+                                                                        vscale, accumulate);
   }
   return check_launch("herk_reduce");
 }

@@ -139,6 +139,50 @@ __global__ void __launch_bounds__(kCompactThreads)
   }
 }
 
+// ERFA-style apparent place of each source (cpu/coords.py:118-181): light
+// deflection by the Sun (_ld), aberration (_ab), bias-precession-nutation
+// (_bpn), in FP64.  The aberration follows the reference expression, whose w2
+// term uses the direction already scaled by bm1.
+constexpr double kErfaSrs = 1.97412574336e-8;  // Schwarzschild radius of the Sun (au)
+
+struct Astrom {
+  double eh[3], em, dlim, v[3], bm1, bpn[9];
+};
+
+__global__ void bcrs_kernel(const double *__restrict__ eci, int64_t n, Astrom a, double *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double p0 = eci[i], p1 = eci[n + i], p2 = eci[2 * n + i];
+    const double e0 = a.eh[0], e1 = a.eh[1], e2 = a.eh[2];
+    // light deflection: p += w p x (e x p), w = SRS / em / max(p.(p + e), dlim)
+    double qdqpe = p0 * (p0 + e0) + p1 * (p1 + e1) + p2 * (p2 + e2);
+    qdqpe = qdqpe < a.dlim ? a.dlim : qdqpe;
+    const double w = kErfaSrs / a.em / qdqpe;
+    const double q0 = e1 * p2 - e2 * p1, q1 = e2 * p0 - e0 * p2, q2 = e0 * p1 - e1 * p0;  // e x p
+    const double r0 = p1 * q2 - p2 * q1, r1 = p2 * q0 - p0 * q2, r2 = p0 * q1 - p1 * q0;  // p x (e x p)
+    p0 += w * r0;
+    p1 += w * r1;
+    p2 += w * r2;
+    // aberration
+    const double pdv = a.v[0] * p0 + a.v[1] * p1 + a.v[2] * p2;
+    const double w1 = 1.0 + pdv / (1.0 + a.bm1);
+    const double w2 = kErfaSrs / a.em;
+    p0 *= a.bm1;
+    p1 *= a.bm1;
+    p2 *= a.bm1;
+    p0 += a.v[0] * w1 + w2 * (a.v[0] - pdv * p0);
+    p1 += a.v[1] * w1 + w2 * (a.v[1] - pdv * p1);
+    p2 += a.v[2] * w1 + w2 * (a.v[2] - pdv * p2);
+    const double rinv = 1.0 / sqrt(p0 * p0 + p1 * p1 + p2 * p2);
+    p0 *= rinv;
+    p1 *= rinv;
+    p2 *= rinv;
+    // bias-precession-nutation
+    out[i] = a.bpn[0] * p0 + a.bpn[1] * p1 + a.bpn[2] * p2;
+    out[n + i] = a.bpn[3] * p0 + a.bpn[4] * p1 + a.bpn[5] * p2;
+    out[2 * n + i] = a.bpn[6] * p0 + a.bpn[7] * p1 + a.bpn[8] * p2;
+  }
+}
+
 }  // namespace mvb
 
 using namespace mvb;
@@ -152,6 +196,23 @@ extern "C" int mvb_rotate(const double *eci, int64_t N, const double *R, double 
   const int64_t blocks = std::min<int64_t>(ceil_div(N, threads), (int64_t)num_sms() * 16);
   rotate_kernel<<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(eci, N, r, topo);
   return check_launch("rotate_kernel");
+}
+
+extern "C" int mvb_bcrs(const double *eci, int64_t N, const double *astrom, double *bcrs, void *stream) {
+  if (N < 0 || !astrom || (N > 0 && (!eci || !bcrs))) return fail(MVB_ERR_ARG, "mvb_bcrs: bad arguments");
+  if (N == 0) return MVB_OK;
+  Astrom a;
+  for (int k = 0; k < 3; ++k) a.eh[k] = astrom[k];
+  a.em = astrom[3];
+  a.dlim = astrom[4];
+  for (int k = 0; k < 3; ++k) a.v[k] = astrom[5 + k];
+  a.bm1 = astrom[8];
+  for (int k = 0; k < 9; ++k) a.bpn[k] = astrom[9 + k];
+  if (!(a.em > 0.0) || !(a.bm1 > 0.0)) return fail(MVB_ERR_ARG, "mvb_bcrs: em and bm1 must be positive");
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>(ceil_div(N, threads), (int64_t)num_sms() * 16);
+  bcrs_kernel<<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(eci, N, a, bcrs);
+  return check_launch("bcrs_kernel");
 }
 
 extern "C" size_t mvb_horizon_ws_bytes(int64_t count) {

@@ -13,8 +13,10 @@
 // Split formats (the operand of the tensor-core Hermitian product):
 //   bf16, P terms: t0 = bf16_rn(v), t1 = bf16_rn(v - t0), t2 = bf16_rn(v - t0 - t1)
 //   tf32, 2 terms: t0 = tf32_rna(v), t1 = tf32_rna(v - t0)
+//   fp16, 2 terms of s*v: t0 = fp16_rn(s v), t1 = fp16_rn(s v - t0), s = zscale
 // each residual being exact in FP32.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 
@@ -32,8 +34,27 @@ __device__ __forceinline__ float tf32_rna(float v) {
 // as the P split terms into planes [2p + c] of a panel row, with vector stores:
 // NV = 8 bf16 (16 bytes) or NV = 4 bf16 (8 bytes), NV float32 (16-byte stores).
 template <int MODE, int NV>
-__device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t off, int comp, const float *v) {
-  if constexpr (MODE == MVB_GEMM_TF32_3) {
+__device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t off, int comp, const float *v,
+                                          float zscale) {
+  if constexpr (MODE == MVB_GEMM_F16_3) {
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      uint32_t w[NV / 2];
+#pragma unroll
+      for (int i = 0; i < NV; i += 2) {
+        const float r0 = v[i] * zscale, r1 = v[i + 1] * zscale;
+        const __half h0 = __float2half_rn(r0), h1 = __float2half_rn(r1);
+        const __half q0 = p == 0 ? h0 : __float2half_rn(r0 - __half2float(h0));
+        const __half q1 = p == 0 ? h1 : __float2half_rn(r1 - __half2float(h1));
+        w[i / 2] = (uint32_t)__half_as_ushort(q0) | ((uint32_t)__half_as_ushort(q1) << 16);
+      }
+      __half *pp = static_cast<__half *>(z) + off + (int64_t)(2 * p + comp) * plane_stride;
+      if constexpr (NV == 8)
+        *reinterpret_cast<uint4 *>(pp) = make_uint4(w[0], w[1], w[2], w[3]);
+      else
+        *reinterpret_cast<uint2 *>(pp) = make_uint2(w[0], w[1]);
+    }
+  } else if constexpr (MODE == MVB_GEMM_TF32_3) {
     float hi[NV], lo[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
@@ -77,8 +98,16 @@ template <int MODE>
 struct PanelWriter {
   static constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
   static __device__ __forceinline__ void put(void *z, int64_t plane_stride, int64_t off, int comp, const float *v,
-                                             int X) {
-    if constexpr (MODE == MVB_GEMM_TF32_3) {
+                                             int X, float zscale) {
+    if constexpr (MODE == MVB_GEMM_F16_3) {
+      __half *zp = static_cast<__half *>(z) + off;
+      for (int x = 0; x < X; ++x) {
+        const float r = v[x] * zscale;
+        const __half hi = __float2half_rn(r);
+        zp[(2 * 0 + comp) * plane_stride + x] = hi;
+        zp[(2 * 1 + comp) * plane_stride + x] = __float2half_rn(r - __half2float(hi));
+      }
+    } else if constexpr (MODE == MVB_GEMM_TF32_3) {
       float *zp = static_cast<float *>(z) + off;
       float hi[2], lo[2];
       for (int x = 0; x < X; ++x) {
@@ -135,8 +164,8 @@ __global__ void __launch_bounds__(kTauZThreads)
     tau_z_kernel(const double *__restrict__ antpos, int A, double f_over_c, const double *__restrict__ crd, int64_t ld,
                  const int32_t *__restrict__ n_dev, int64_t nsrc, const float *__restrict__ sflux,
                  const int32_t *__restrict__ sidx, const float2 *__restrict__ beam, int64_t beam_ld, int nbeam,
-                 const int32_t *__restrict__ beam_idx, int F, void *__restrict__ z, int64_t Mpad, int64_t Kcap,
-                 const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
+                 const int32_t *__restrict__ beam_idx, int F, float zscale, void *__restrict__ z, int64_t Mpad,
+                 int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
   __shared__ float2 bsm[kTauZMaxBFX][kTauZThreads][kTauZSrc];
   const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
   const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
@@ -220,8 +249,8 @@ __global__ void __launch_bounds__(kTauZThreads)
         for (int i = 0; i < kTauZSrc * X; i += 2)
           *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
       } else {
-        put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr);
-        put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi);
+        put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr, zscale);
+        put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi, zscale);
       }
     }
   }
@@ -249,8 +278,8 @@ __global__ void exptau_kernel(const double *__restrict__ antpos, int A, double f
 
 // Packs a caller complex matrix (M, K) into a panel; one thread per (m, k-pair).
 template <int MODE, typename CT>
-__global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, int64_t ldz, void *__restrict__ z,
-                              int64_t Mpad, int64_t Kcap) {
+__global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, int64_t ldz, float zscale,
+                              void *__restrict__ z, int64_t Mpad, int64_t Kcap) {
   const int64_t kend = round_up(K, kKAlign);
   const int64_t half = kend / 2;
   const int64_t total = M * half;
@@ -271,15 +300,39 @@ __global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, i
     if constexpr (MODE == MVB_Z_C64) {
       *reinterpret_cast<float4 *>(static_cast<float2 *>(z) + off) = make_float4(vr[0], vi[0], vr[1], vi[1]);
     } else {
-      PanelWriter<MODE>::put(z, plane, off, 0, vr, 2);
-      PanelWriter<MODE>::put(z, plane, off, 1, vi, 2);
+      PanelWriter<MODE>::put(z, plane, off, 0, vr, 2, zscale);
+      PanelWriter<MODE>::put(z, plane, off, 1, vi, 2, zscale);
     }
   }
+}
+
+template <typename CT>
+__global__ void absmax_kernel(const CT *__restrict__ z, int64_t n, float *__restrict__ out) {
+  float m = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const CT v = z[i];
+    m = fmaxf(m, (float)sqrt((double)v.x * v.x + (double)v.y * v.y));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  // non-negative floats order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
 }
 
 }  // namespace mvb
 
 using namespace mvb;
+
+extern "C" int mvb_absmax(const void *z, int z_c128, int64_t n, float *out, void *stream) {
+  if (!out || n < 0 || (n > 0 && !z)) return fail(MVB_ERR_ARG, "mvb_absmax: bad arguments");
+  if (n == 0) return MVB_OK;
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>(ceil_div(n, threads), (int64_t)num_sms() * 8);
+  if (z_c128)
+    absmax_kernel<double2><<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(static_cast<const double2 *>(z), n, out);
+  else
+    absmax_kernel<float2><<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(static_cast<const float2 *>(z), n, out);
+  return check_launch("absmax_kernel");
+}
 
 extern "C" size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap) {
   if (mode == MVB_Z_C64) return (size_t)Mpad * Kcap * 8;
@@ -287,7 +340,7 @@ extern "C" size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap) {
 }
 
 static int check_panel(int mode, int64_t M, int64_t Mpad, int64_t Kcap, const char *who) {
-  if (mode < MVB_GEMM_BF16_3 || mode > MVB_Z_C64) return fail(MVB_ERR_ARG, "%s: unknown mode %d", who, mode);
+  if (mode < MVB_GEMM_BF16_3 || mode > MVB_GEMM_F16_3) return fail(MVB_ERR_ARG, "%s: unknown mode %d", who, mode);
   if (Kcap % kKAlign) return fail(MVB_ERR_ARG, "%s: Kcap must be a multiple of %d", who, kKAlign);
   if (Mpad < M) return fail(MVB_ERR_ARG, "%s: Mpad < M", who);
   if (mode != MVB_Z_C64 && Mpad % kTile) return fail(MVB_ERR_ARG, "%s: Mpad must be a multiple of %d", who, kTile);
@@ -309,8 +362,8 @@ extern "C" int mvb_exptau(const double *antpos, int A, double freq, const double
 
 extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
                          int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld,
-                         int nbeam, const int32_t *beam_idx, int F, int X, int mode, void *z, int64_t Mpad,
-                         int64_t Kcap, void *stream) {
+                         int nbeam, const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z,
+                         int64_t Mpad, int64_t Kcap, void *stream) {
   if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !sflux || (nsrc > 0 && !crd) || (F != 1 && F != 2) ||
       (X != 1 && X != 2) || nbeam <= 0 || nbeam * F * X > kTauZMaxBFX || beam_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_tau_z: bad arguments");
@@ -325,7 +378,7 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
   cudaStream_t s = as_stream(stream);
 #define MVB_TAUZ(M, XX)                                                                                              \
   tau_z_kernel<M, XX><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld,   \
-                                                    nbeam, beam_idx, F, z, Mpad, Kcap)
+                                                    nbeam, beam_idx, F, zscale, z, Mpad, Kcap)
 #define MVB_TAUZ2(M) \
   if (X == 2)        \
     MVB_TAUZ(M, 2);  \
@@ -335,6 +388,7 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
     case MVB_GEMM_BF16_3: MVB_TAUZ2(MVB_GEMM_BF16_3); break;
     case MVB_GEMM_BF16_6: MVB_TAUZ2(MVB_GEMM_BF16_6); break;
     case MVB_GEMM_TF32_3: MVB_TAUZ2(MVB_GEMM_TF32_3); break;
+    case MVB_GEMM_F16_3: MVB_TAUZ2(MVB_GEMM_F16_3); break;
     default: MVB_TAUZ2(MVB_Z_C64); break;
   }
 #undef MVB_TAUZ2
@@ -342,8 +396,8 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
   return check_launch("tau_z_kernel");
 }
 
-extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, void *z,
-                          int64_t Mpad, int64_t Kcap, void *stream) {
+extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, float zscale,
+                          void *z, int64_t Mpad, int64_t Kcap, void *stream) {
   if (M < 0 || K < 0 || ldz < K || !z || (M * K > 0 && !zsrc)) return fail(MVB_ERR_ARG, "mvb_z_pack: bad arguments");
   int rc = check_panel(mode, M, Mpad, Kcap, "mvb_z_pack");
   if (rc) return rc;
@@ -354,7 +408,8 @@ extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, in
   const int64_t blocks = std::min<int64_t>(ceil_div(total, threads), (int64_t)num_sms() * 16);
   cudaStream_t s = as_stream(stream);
 #define MVB_PACK(M_, CT)                                                                                             \
-  z_pack_kernel<M_, CT><<<(unsigned)blocks, threads, 0, s>>>(static_cast<const CT *>(zsrc), M, K, ldz, z, Mpad, Kcap)
+  z_pack_kernel<M_, CT><<<(unsigned)blocks, threads, 0, s>>>(static_cast<const CT *>(zsrc), M, K, ldz, zscale, z, Mpad, \
+                                                             Kcap)
 #define MVB_PACK2(M_) \
   if (z_c128)         \
     MVB_PACK(M_, double2); \
@@ -364,6 +419,7 @@ extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, in
     case MVB_GEMM_BF16_3: MVB_PACK2(MVB_GEMM_BF16_3); break;
     case MVB_GEMM_BF16_6: MVB_PACK2(MVB_GEMM_BF16_6); break;
     case MVB_GEMM_TF32_3: MVB_PACK2(MVB_GEMM_TF32_3); break;
+    case MVB_GEMM_F16_3: MVB_PACK2(MVB_GEMM_F16_3); break;
     default: MVB_PACK2(MVB_Z_C64); break;
   }
 #undef MVB_PACK2
@@ -373,7 +429,7 @@ extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, in
 
 extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, int A, int64_t nsrc, const float *sflux,
                                  const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X,
-                                 int mode, void *z, int64_t Mpad, int64_t Kcap, void *stream) {
+                                 int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap, void *stream) {
   if (A <= 0 || nsrc < 0 || !exptau || !z || !beam || !sflux || (F != 1 && F != 2) || (X != 1 && X != 2) ||
       nbeam <= 0 || nbeam * F * X > kTauZMaxBFX || beam_ld < nsrc || e_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_z_from_exptau: bad arguments");
@@ -387,7 +443,7 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
   cudaStream_t s = as_stream(stream);
 #define MVB_ZX(M, XX, E)                                                                                              \
   tau_z_kernel<M, XX, E><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, nullptr, bm, \
-                                                       beam_ld, nbeam, beam_idx, F, z, Mpad, Kcap, exptau, e_ld)
+                                                       beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, exptau, e_ld)
 #define MVB_ZX3(M, E) \
   if (X == 2)         \
     MVB_ZX(M, 2, E);  \
@@ -402,6 +458,7 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
     case MVB_GEMM_BF16_3: MVB_ZX2(MVB_GEMM_BF16_3); break;
     case MVB_GEMM_BF16_6: MVB_ZX2(MVB_GEMM_BF16_6); break;
     case MVB_GEMM_TF32_3: MVB_ZX2(MVB_GEMM_TF32_3); break;
+    case MVB_GEMM_F16_3: MVB_ZX2(MVB_GEMM_F16_3); break;
     default: MVB_ZX2(MVB_Z_C64); break;
   }
 #undef MVB_ZX2

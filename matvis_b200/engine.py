@@ -23,7 +23,7 @@ import torch
 
 from . import _lib
 from .beams import B200BeamInterpolator, GaussianBeam, GridBeam
-from .coordinates import eci_to_enu_matrix, point_source_crd_eq
+from .coordinates import atioq_matrix, bcrs_refresh_plan, eci_to_enu_matrix, pack_astrom, point_source_crd_eq
 from .getz import ZMatrixCalc
 from .autotune import tune_k_chunk
 from .matprod import B200MatMul, B200VectorDot, choose_k_chunk
@@ -51,6 +51,10 @@ class JobSpec:
     k_chunk: int | None = None
     source_buffer: float = 1.0
     nchunks: int = 1
+    #: ERFA-style apparent place: one astrom dict per time (else the LST rotation)
+    astrom: list | None = None
+    update_bcrs_every: float = 0.0
+    time_s: np.ndarray | None = None
 
 
 def _norm_matprod(name: str) -> str:
@@ -92,7 +96,24 @@ class VisEngine:
         self.cap = int(self.chunk_size * s.source_buffer) if self.chunk_size > 1000 else self.chunk_size
         self.cap = max(self.cap, 1)
         self.ctype = torch.complex64 if s.precision == 1 else torch.complex128
-        self.rot = np.stack([eci_to_enu_matrix(l, s.latitude) for l in self.lsts]) if len(self.lsts) else np.zeros((0, 3, 3))
+        if s.astrom is not None:
+            if len(s.astrom) != len(self.lsts):
+                raise ValueError("astrom must hold one parameter dict per time")
+            self.rot = np.stack([atioq_matrix(a) for a in s.astrom])
+            if s.time_s is None and s.update_bcrs_every > 0:
+                raise ValueError("update_bcrs_every needs time_s (the times in seconds)")
+            # without time_s every time step refreshes the apparent-place directions
+            self.bcrs_plan = ([True] * len(self.lsts) if s.time_s is None
+                              else bcrs_refresh_plan(s.time_s, s.update_bcrs_every))
+            self.astrom_packed = [pack_astrom(a) for a in s.astrom]
+        else:
+            self.rot = (np.stack([eci_to_enu_matrix(l, s.latitude) for l in self.lsts]) if len(self.lsts)
+                        else np.zeros((0, 3, 3)))
+            self.bcrs_plan = None
+        self.zscale = 1.0
+        if self.method == "MatMul" and _lib.GEMM_MODES.get(s.gemm_mode, s.gemm_mode) == _lib.GEMM_F16_3:
+            # |Z| <= max sqrt(0.5 I) * max |beam| (bilinear weights are convex, |exptau| = 1)
+            self.zscale = _lib.f16_scale(float(self.sflux_host.max(initial=0.0)) * beam_bound(s.beams) * (1 + 2**-10))
         self._graph = None
         self._allocated = False
 
@@ -105,6 +126,7 @@ class VisEngine:
         self.antpos = torch.empty((A, 3), dtype=torch.float64, device=dev)
         self.sflux = torch.empty((len(self.freqs), N), dtype=torch.float32, device=dev)
         self.topo = torch.zeros((3, N), dtype=torch.float64, device=dev)
+        self.bcrs = torch.zeros((3, N), dtype=torch.float64, device=dev) if self.bcrs_plan is not None else None
         self.crd = torch.zeros((3, self.cap), dtype=torch.float64, device=dev)
         self.kept = torch.zeros((self.cap,), dtype=torch.int32, device=dev)
         self.n_above = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -163,7 +185,13 @@ class VisEngine:
         F, X = self.nfeed, self.nax
         panel = self.zcalc.z
         R = np.ascontiguousarray(self.rot[t])
-        chk(L.mvb_rotate(_lib.ptr(self.eci), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
+        src = self.eci
+        if self.bcrs_plan is not None:
+            if self.bcrs_plan[t]:
+                a = self.astrom_packed[t]
+                chk(L.mvb_bcrs(_lib.ptr(self.eci), self.nsrc, a.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.bcrs), sh))
+            src = self.bcrs
+        chk(L.mvb_rotate(_lib.ptr(src), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
         for c in range(self.nchunks):
             c0 = min(c * self.chunk_size, self.nsrc)
             c1 = min((c + 1) * self.chunk_size, self.nsrc)
@@ -179,9 +207,10 @@ class VisEngine:
                     _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
                     _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f]), _lib.ptr(self.kept), _lib.ptr(beam),
                     beam.shape[-1], beam.shape[0], _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode,
-                    _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
+                    self.zscale, _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
                 panel.n_dev = self.n_above
                 panel.n_host = self.cap
+                panel.scale = self.zscale
                 out = self.vis[f, t]
                 if self.method == "MatMul":
                     self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream, k_chunk=self.k_chunk)
@@ -201,7 +230,8 @@ class VisEngine:
     def launches_per_run(self) -> int:
         per_f = 3 if self.method == "MatMul" else 2
         per_chunk = 3 + per_f * len(self.freqs)  # count + scatter + beam, then per frequency
-        return len(self.lsts) * (1 + self.nchunks * per_chunk)
+        n = len(self.lsts) * (1 + self.nchunks * per_chunk)
+        return n + (sum(self.bcrs_plan) if self.bcrs_plan is not None else 0)
 
     def run(self, check: bool = True) -> torch.Tensor:
         """Run the job on the current stream; returns the device visibilities."""
@@ -281,3 +311,15 @@ def estimate_device_bytes(spec: JobSpec) -> int:
     nbeam = len(spec.beams)
     return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + 8 * nbeam * F * X * cap + panel + ws
                + Nf * Nt * npairs * F * F * csize)
+
+
+def beam_bound(beams) -> float:
+    """Upper bound of |interpolated beam| over all beams (grid maximum; 1 for Gaussians)."""
+    b = 0.0
+    for bm in beams:
+        if isinstance(bm, GridBeam):
+            d = bm.data if bm.beam_type == "efield" else np.sqrt(np.abs(bm.data))
+            b = max(b, float(np.abs(d).max()))
+        else:
+            b = max(b, 1.0)
+    return b

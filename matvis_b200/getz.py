@@ -37,6 +37,8 @@ class ZPanel:
             self.data = torch.zeros((planes, self.Mpad, self.Kcap), dtype=dt, device=device)
         self.n_dev = None
         self.n_host = 0
+        #: power-of-two factor the panel holds Z multiplied by (fp16x3 mode)
+        self.scale = 1.0
 
     @property
     def shape(self):
@@ -49,19 +51,20 @@ class ZPanel:
         if self.mode == _lib.Z_C64:
             return self.data[:, :k].to(torch.complex128)
         d = self.data[:, : self.M, :k].to(torch.float64)
-        re = d[0::2].sum(0)
-        im = d[1::2].sum(0)
+        re = d[0::2].sum(0) / self.scale
+        im = d[1::2].sum(0) / self.scale
         return torch.complex(re, im)
 
 
 class ZMatrixCalc:
     """Builds Z = A * sqrt(I) * exp(tau) on the device."""
 
-    def __init__(self, nant, nfeed, nax, nsrc, ctype=None, gpu: bool = True, mode: int = _lib.GEMM_BF16_6, device=None):
+    def __init__(self, nant, nfeed, nax, nsrc, ctype=None, gpu: bool = True, mode: int | str = _lib.GEMM_BF16_6,
+                 device=None):
         self.device = _lib.require_cuda(device)
         self.nant, self.nfeed, self.nax, self.nsrc = nant, nfeed, nax, nsrc
         self.ctype = ctype
-        self.mode = mode
+        self.mode = _lib.GEMM_MODES[mode] if isinstance(mode, str) else int(mode)
         self.gpu = True
 
     def setup(self):
@@ -84,11 +87,15 @@ class ZMatrixCalc:
         b64 = beam.to(torch.complex64).contiguous()
         e_c128 = 1 if exptau.dtype == torch.complex128 else 0
         exptau = exptau.contiguous()
+        if self.mode == _lib.GEMM_F16_3:
+            # |Z| <= max |exptau| * max sqrt_flux * max |beam|, |exptau| = 1
+            bound = float(sf.abs().max().item()) * float(b64.abs().max().item()) if n else 0.0
+            self.z.scale = _lib.f16_scale(bound)
         check(
             _lib.lib.mvb_z_from_exptau(
                 ptr(exptau), e_c128, exptau.shape[1], self.nant, n, ptr(self._sflux), ptr(b64), b64.shape[-1],
-                b64.shape[0], ptr(bidx), self.nfeed, self.nax, self.mode, ptr(self.z.data), self.z.Mpad, self.z.Kcap,
-                stream_handle(),
+                b64.shape[0], ptr(bidx), self.nfeed, self.nax, self.mode, self.z.scale, ptr(self.z.data), self.z.Mpad,
+                self.z.Kcap, stream_handle(),
             )
         )
         self.z.n_dev = None
@@ -96,12 +103,14 @@ class ZMatrixCalc:
         return self.z
 
     def fused(self, antpos: torch.Tensor, freq: float, crd: torch.Tensor, ld: int, n_dev, nsrc: int,
-              sflux: torch.Tensor, sidx, beam: torch.Tensor, beam_idx: torch.Tensor, stream=None) -> ZPanel:
+              sflux: torch.Tensor, sidx, beam: torch.Tensor, beam_idx: torch.Tensor, stream=None,
+              scale: float = 1.0) -> ZPanel:
         """Fused tau + Z (``mvb_tau_z``): no exptau round trip, count read on the device."""
+        self.z.scale = scale
         check(
             _lib.lib.mvb_tau_z(
                 ptr(antpos), self.nant, float(freq), ptr(crd), ld, ptr(n_dev), nsrc, ptr(sflux), ptr(sidx),
-                ptr(beam), beam.shape[-1], beam.shape[0], ptr(beam_idx), self.nfeed, self.nax, self.mode,
+                ptr(beam), beam.shape[-1], beam.shape[0], ptr(beam_idx), self.nfeed, self.nax, self.mode, scale,
                 ptr(self.z.data), self.z.Mpad, self.z.Kcap, stream_handle(stream),
             )
         )

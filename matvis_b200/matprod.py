@@ -112,10 +112,16 @@ class MatProd(ABC):
         if panel is None:
             panel = ZPanel(mode, self.nant, self.nfeed, 1, K, self.device)
             self._packed = {key: panel}
+        c128 = 1 if zt.dtype == torch.complex128 else 0
+        scale = 1.0
+        if mode == _lib.GEMM_F16_3:
+            mx = torch.zeros(1, dtype=torch.float32, device=self.device)
+            check(_lib.lib.mvb_absmax(ptr(zt), c128, M * K, ptr(mx), stream_handle()))
+            scale = _lib.f16_scale(float(mx.item()) * (1 + 2**-10))
+        panel.scale = scale
         check(
             _lib.lib.mvb_z_pack(
-                ptr(zt), 1 if zt.dtype == torch.complex128 else 0, M, K, K, mode, ptr(panel.data), panel.Mpad,
-                panel.Kcap, stream_handle(),
+                ptr(zt), c128, M, K, K, mode, scale, ptr(panel.data), panel.Mpad, panel.Kcap, stream_handle(),
             )
         )
         panel.n_dev = None
@@ -127,10 +133,12 @@ class B200MatMul(MatProd):
     """Hermitian product V = conj(Z) Z^T, upper-triangle tiles on the tensor cores."""
 
     def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, gemm_mode: str | int = "bf16x6",
-                 k_chunk: int | None = None, device=None):
+                 k_chunk: int | None = None, device=None, drain_ksteps: int = 0):
         super().__init__(nchunks, nfeed, nant, antpairs, precision=precision, device=device)
+        #: k-steps per TMEM block before the drain to FP32 registers (0: the mode's default)
+        self.drain_ksteps = int(drain_ksteps)
         self.mode = _lib.GEMM_MODES[gemm_mode] if isinstance(gemm_mode, str) else int(gemm_mode)
-        if self.mode not in (_lib.GEMM_BF16_3, _lib.GEMM_BF16_6, _lib.GEMM_TF32_3):
+        if self.mode not in (_lib.GEMM_BF16_3, _lib.GEMM_BF16_6, _lib.GEMM_TF32_3, _lib.GEMM_F16_3):
             raise ValueError(f"unknown gemm_mode {gemm_mode!r}")
         self.k_chunk = k_chunk
         self._ws = None
@@ -156,15 +164,16 @@ class B200MatMul(MatProd):
         kmul = panel.nax
         check(
             _lib.lib.mvb_herk(
-                ptr(panel.data), self.mode, panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc, ptr(ws),
-                ws.numel(), ptr(self.status), sh,
+                ptr(panel.data), self.mode, panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc,
+                self.drain_ksteps, ptr(ws), ws.numel(), ptr(self.status), sh,
             )
         )
         pairs = None if self.all_pairs else self._pairs_dev
         check(
             _lib.lib.mvb_herk_reduce(
                 ptr(ws), panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc, self.nant, self.nfeed,
-                ptr(pairs), self.npairs, ptr(out), 1 if out.dtype == torch.complex128 else 0, int(accumulate), sh,
+                ptr(pairs), self.npairs, ptr(out), 1 if out.dtype == torch.complex128 else 0, 1.0 / panel.scale**2,
+                int(accumulate), sh,
             )
         )
 

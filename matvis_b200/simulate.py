@@ -29,7 +29,8 @@ from .engine import JobSpec, VisEngine, _norm_matprod
 
 logger = logging.getLogger(__name__)
 
-_UNAVAILABLE_COORD = ("CoordinateRotationAstropy", "CoordinateRotationERFA", "GPUCoordinateRotationERFA")
+_UNAVAILABLE_COORD = ("CoordinateRotationAstropy",)
+_ERFA_COORD = ("CoordinateRotationERFA", "GPUCoordinateRotationERFA")
 
 
 def _validate_inputs(precision, polarized, antpos, times, I_sky):
@@ -43,14 +44,24 @@ def _validate_inputs(precision, polarized, antpos, times, I_sky):
     return nax, nfeed, nant, ntimes
 
 
-def _check_coord_method(coord_method):
+def _check_coord_method(coord_method, params=None):
+    """Rotation keywords for the JobSpec: {} for the LST rotation, the astrom
+    parameters for the ERFA-style one."""
     if coord_method in _UNAVAILABLE_COORD:
         raise NotImplementedError(
-            f"{coord_method} needs astropy/ERFA time-dependent astrometry, which this build does not ship; "
-            "use coord_method='CoordinateRotationLST' with times given as LSTs (radians)"
+            f"{coord_method} needs astropy's transform machinery, which this build does not ship; use "
+            "coord_method='CoordinateRotationLST' (times = LSTs in radians) or 'CoordinateRotationERFA' with "
+            "coord_method_params={'astrom': [...], 'time_s': [...], 'update_bcrs_every': seconds}"
         )
+    if coord_method in _ERFA_COORD:
+        params = dict(params or {})
+        if "astrom" not in params:
+            raise ValueError("CoordinateRotationERFA needs coord_method_params['astrom'] (one pyerfa apco dict per time)")
+        return {"astrom": list(params["astrom"]), "time_s": params.get("time_s"),
+                "update_bcrs_every": float(params.get("update_bcrs_every", 0.0))}
     if coord_method != "CoordinateRotationLST":
         raise ValueError(f"unknown coord_method {coord_method!r}")
+    return {}
 
 
 def simulate(
@@ -84,7 +95,7 @@ def simulate(
         raise ValueError("source_buffer must satisfy 0 < source_buffer <= 1")
     if not 0 < memory_buffer <= 1:
         raise ValueError("memory_buffer must satisfy 0 < memory_buffer <= 1")
-    _check_coord_method(coord_method)
+    rot_kw = _check_coord_method(coord_method, coord_method_params)
     dev = _lib.require_cuda(device)
     antpos = np.asarray(antpos, dtype=np.float64)
     I_sky = np.asarray(I_sky)
@@ -98,7 +109,7 @@ def simulate(
         antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=I_sky[:, None], freqs=np.array([float(freq)]),
         lsts=lsts, latitude=latitude_of(telescope_loc), beams=list(beam_list), beam_idx=beam_idx, polarized=polarized,
         antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
-        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks,
+        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks, **rot_kw,
     )
     eng = VisEngine(spec, device=dev)
     vis = eng.run()[0]
@@ -139,7 +150,7 @@ def simulate_vis(
     """
     if not use_gpu:
         raise ValueError("matvis_b200 runs on the GPU only (use_gpu=False has no CPU path here)")
-    _check_coord_method(coord_method)
+    rot_kw = _check_coord_method(coord_method, coord_method_params)
     fluxes = np.asarray(fluxes)
     ra = np.asarray(ra, dtype=np.float64)
     dec = np.asarray(dec, dtype=np.float64)
@@ -152,7 +163,7 @@ def simulate_vis(
         antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=fluxes, freqs=freqs, lsts=lsts_of(times),
         latitude=latitude_of(telescope_loc), beams=list(beams), beam_idx=beam_idx, polarized=polarized,
         antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
-        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=max(1, int(min_chunks)),
+        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=max(1, int(min_chunks)), **rot_kw,
     )
     eng = VisEngine(spec, device=device)
     vis = eng.run().cpu().numpy()

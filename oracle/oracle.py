@@ -296,8 +296,17 @@ def simulate(
     source_buffer=1.0,
     matprod="MatMul",
     eci=None,
+    astrom=None,
+    time_s=None,
+    update_bcrs_every=0.0,
 ):
     """One frequency, all times; ``cpu/cpu.py:163-277`` at precision=2.
+
+    With ``astrom`` (one apco parameter dict per time) the rotation is the
+    ERFA-style apparent place of ``CoordinateRotationERFA`` (cpu/coords.py:186-230),
+    refreshing the deflected/aberrated directions when more than
+    ``update_bcrs_every`` seconds of ``time_s`` have passed (every step when
+    ``time_s`` is None); otherwise the LST rotation.
 
     Returns (ntimes, npairs, nfeed, nfeed) complex128 when polarized, else
     (ntimes, npairs).
@@ -320,8 +329,14 @@ def simulate(
     alloc = nsrc_alloc(chunk_size, source_buffer)
     pairs = all_pairs(nant) if antpairs is None else np.asarray(antpairs)
     vis = np.zeros((len(lsts), len(pairs), nfeed, nfeed), dtype=np.complex128)
+    last, bcrs = None, None
     for t, lst in enumerate(lsts):
-        topo = rotate_fixed_order(eci_to_enu_matrix(lst, latitude), eci)
+        if astrom is None:
+            topo = rotate_fixed_order(eci_to_enu_matrix(lst, latitude), eci)
+        else:
+            if last is None or time_s is None or time_s[t] - time_s[last] > update_bcrs_every:
+                bcrs, last = erfa_bcrs(eci, astrom[t]), t
+            topo = rotate_fixed_order(erfa_atioq_matrix(astrom[t]), bcrs)
         for c in range(nchunks):
             crd, fl, n, _ = select_chunk(topo, flux, c, chunk_size, alloc)
             if n == 0:
@@ -354,8 +369,11 @@ def simulate_vis(
     matprod="MatMul",
     nchunks=1,
     source_buffer=1.0,
+    **rotation,
 ):
-    """Frequency loop of ``wrapper.simulate_vis``; ``wrapper.py:150-199``."""
+    """Frequency loop of ``wrapper.simulate_vis``; ``wrapper.py:150-199``.
+    ``rotation`` holds the ERFA keywords of :func:`simulate` (astrom, time_s,
+    update_bcrs_every)."""
     antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
     fluxes = np.asarray(fluxes)
     assert fluxes.shape == (len(ra), len(freqs)), "The `fluxes` array must have shape (NSRCS, NFREQS)."
@@ -379,6 +397,7 @@ def simulate_vis(
                 source_buffer=source_buffer,
                 matprod=matprod,
                 eci=eci,
+                **rotation,
             )
         )
     return np.asarray(out)
@@ -431,3 +450,54 @@ def cosine_error_metric(v, ref, nfeed):
     den = np.sqrt(auto[..., :, None, None, :] * auto[..., None, :, :, None])
     den = np.where(den > 0, den, np.inf)
     return float(np.max(np.abs(d) / den)) if d.size else 0.0
+
+
+# ---------------------------------------------------------------------------
+# ERFA-style apparent place (src/matvis/cpu/coords.py:89-215)
+# ---------------------------------------------------------------------------
+#: Schwarzschild radius of the Sun in au (cpu/coords.py:11).
+ERFA_SRS = 1.97412574336e-8
+
+
+def erfa_ld(p, e, em, dlim):
+    """Light deflection by the Sun; ``CoordinateRotationERFA._ld`` (cpu/coords.py:118-148)."""
+    p = np.array(p, dtype=np.float64)
+    e = np.asarray(e, dtype=np.float64)
+    qpe = (p.T + e).T
+    qdqpe = np.sum(p * qpe, axis=0)
+    qdqpe = np.clip(qdqpe, dlim, None)
+    w = ERFA_SRS / em / qdqpe
+    eq = np.cross(e.T, p.T)
+    peq = np.cross(p.T, eq).T
+    return p + w[None] * peq
+
+
+def erfa_ab(pnat, v, s, bm1):
+    """Aberration; ``CoordinateRotationERFA._ab`` (cpu/coords.py:150-174), including its
+    use of the already-scaled direction in the w2 term."""
+    pnat = np.array(pnat, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
+    pdv = np.dot(v, pnat)
+    w1 = 1.0 + pdv / (1.0 + bm1)
+    w2 = ERFA_SRS / s
+    pnat = pnat * bm1
+    pnat = pnat + np.outer(v, w1) + w2 * (v - (pdv * pnat).T).T
+    return pnat / np.linalg.norm(pnat, axis=0)
+
+
+def erfa_atioq_matrix(astrom):
+    """CIRS -> ENU 3x3 of ``CoordinateRotationERFA._atioq`` (cpu/coords.py:89-116)."""
+    ce, se = np.cos(astrom["eral"]), np.sin(astrom["eral"])
+    c2h = np.array([[ce, se, 0], [-se, ce, 0], [0, 0, 1]])
+    sx, cx = np.sin(astrom["xpl"]), np.cos(astrom["xpl"])
+    sy, cy = np.sin(astrom["ypl"]), np.cos(astrom["ypl"])
+    pm = np.array([[cx, 0, sx], [sx * sy, cy, -cx * sy], [-sx * cy, sy, cx * cy]])
+    enu = np.array([[0, 1, 0], [-astrom["sphi"], 0, astrom["cphi"]], [astrom["cphi"], 0, astrom["sphi"]]])
+    return enu.dot(pm.dot(c2h))
+
+
+def erfa_bcrs(eci, astrom, dlim=1e-6):
+    """_set_bcrs (cpu/coords.py:186-215): deflection, aberration, bias-precession-nutation."""
+    p = erfa_ld(eci, astrom["eh"], astrom["em"], dlim)
+    p = erfa_ab(p, astrom["v"], astrom["em"], astrom["bm1"])
+    return np.asarray(astrom["bpn"], dtype=np.float64) @ p

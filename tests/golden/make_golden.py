@@ -17,7 +17,9 @@ reference functions return:
 * ``tauz.npz``      -- ``TauCalculator`` and ``ZMatrixCalc``;
 * ``chunks.npz``    -- ``get_required_chunks`` over a parameter grid;
 * ``pipeline.npz``  -- end-to-end visibilities from the reference plugin classes
-  driven in the loop order of ``cpu/cpu.py:247-272``.
+  driven in the loop order of ``cpu/cpu.py:247-272``;
+* ``erfa.npz``      -- ``CoordinateRotationERFA._ld / _ab / _bpn / _atioq``
+  (``cpu/coords.py:89-181``) on seeded unit vectors and astrom parameters.
 
 The fixtures are small (< 1 MB) and committed; the tests never read the
 reference tree.
@@ -373,6 +375,53 @@ def make_pipeline():
     _save("pipeline.npz", **out)
 
 
+def seeded_astrom(rng, lat):
+    """Astrom-like parameters of realistic size (the pyerfa apco output is not available)."""
+    eh = rng.normal(size=3)
+    eh /= np.linalg.norm(eh)
+    v = rng.normal(size=3)
+    v *= 1.0e-4 / np.linalg.norm(v)  # ~30 km/s in units of c
+    a, b, c = rng.normal(size=3) * 1e-3
+    ca, sa, cb, sb, cc, sc = np.cos(a), np.sin(a), np.cos(b), np.sin(b), np.cos(c), np.sin(c)
+    rz = np.array([[ca, -sa, 0], [sa, ca, 0], [0, 0, 1]])
+    ry = np.array([[cb, 0, sb], [0, 1, 0], [-sb, 0, cb]])
+    rx = np.array([[1, 0, 0], [0, cc, -sc], [0, sc, cc]])
+    return {
+        "eh": eh, "em": 1.0 + 0.0167 * rng.uniform(-1, 1), "v": v, "bm1": float(np.sqrt(1 - v @ v)),
+        "bpn": rz @ ry @ rx, "eral": rng.uniform(0, 2 * np.pi), "xpl": 1e-6 * rng.normal(), "ypl": 1e-6 * rng.normal(),
+        "sphi": np.sin(lat), "cphi": np.cos(lat),
+    }
+
+
+def make_erfa():
+    rot_cls = ref.cpu_coords.CoordinateRotationERFA
+
+    class _Self:
+        xp = np
+
+    rng = np.random.default_rng(31)
+    nsrc = 500
+    ra = rng.uniform(0, 2 * np.pi, nsrc)
+    dec = np.arcsin(rng.uniform(-1, 1, nsrc))
+    eci = np.asarray(ref.coordinates.point_source_crd_eq(ra, dec))
+    out = {"eci": eci}
+    for t in range(3):
+        astrom = seeded_astrom(rng, np.deg2rad(-30.72))
+        for k, val in astrom.items():
+            out[f"t{t}_{k}"] = np.asarray(val)
+        p = eci.copy()
+        rot_cls._ld(_Self(), p, astrom["eh"], astrom["em"], 1e-6)
+        out[f"t{t}_after_ld"] = p.copy()
+        rot_cls._ab(_Self(), p, astrom["v"], astrom["em"], astrom["bm1"])
+        out[f"t{t}_after_ab"] = p.copy()
+        rot_cls._bpn(_Self(), p, astrom)
+        out[f"t{t}_bcrs"] = p.copy()
+        top = p.copy()
+        rot_cls._atioq(_Self(), top, astrom)
+        out[f"t{t}_topo"] = top
+    _save("erfa.npz", **out)
+
+
 if __name__ == "__main__":
     make_matprod()
     make_bilinear()
@@ -380,3 +429,4 @@ if __name__ == "__main__":
     make_tauz()
     make_chunks()
     make_pipeline()
+    make_erfa()

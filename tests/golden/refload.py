@@ -122,4 +122,5 @@ def load_reference():
     ns.core_matprod = importlib.import_module("matvis.core.matprod")
     ns.cpu_matprod = importlib.import_module("matvis.cpu.matprod")
     ns.gpu_beams = importlib.import_module("matvis.gpu.beams")
+    ns.cpu_coords = importlib.import_module("matvis.cpu.coords")
     return ns

@@ -54,7 +54,7 @@ def test_argument_errors_are_reported_without_gpu():
     """Argument validation happens on the host, before any CUDA call."""
     from matvis_b200 import _lib
 
-    rc = _lib.lib.mvb_herk(None, 0, 768, 100, None, 0, 1, 64, None, 0, None, None)
+    rc = _lib.lib.mvb_herk(None, 0, 768, 100, None, 0, 1, 64, 0, None, 0, None, None)
     assert rc == _lib.MVB_ERR_ARG
     assert b"mvb_herk" in _lib.lib.mvb_last_error()
     with pytest.raises(ValueError):

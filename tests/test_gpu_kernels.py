@@ -151,7 +151,7 @@ def test_exptau_long_baseline_phase():
     np.testing.assert_allclose(out, orc.exptau(antpos, 200e6, crd), rtol=0, atol=5e-7)
 
 
-@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32x3"])
+@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32x3", "fp16x3"])
 def test_z_from_exptau_matches_reference(device, mode):
     g = golden("tauz")
     zc = mv.ZMatrixCalc(nant=6, nfeed=2, nax=2, nsrc=g["exptau"].shape[1], mode=_lib.GEMM_MODES[mode])
@@ -160,12 +160,12 @@ def test_z_from_exptau_matches_reference(device, mode):
     zz = z.to_complex().cpu().numpy()
     # panel column order is (src, ax); reference order is (ax, src)
     ref = g["z"].reshape(12, 2, -1).transpose(0, 2, 1).reshape(12, -1)
-    tol = {"bf16x3": 2e-5, "bf16x6": 5e-7, "tf32x3": 5e-7}[mode]
+    tol = {"bf16x3": 2e-5, "bf16x6": 5e-7, "tf32x3": 5e-7, "fp16x3": 5e-7}[mode]
     np.testing.assert_allclose(zz, ref, rtol=0, atol=tol * np.abs(ref).max())
 
 
 # ---------------------------------------------------------------- Hermitian product
-@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32x3"])
+@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32x3", "fp16x3"])
 @pytest.mark.parametrize("nfeed", [1, 2])
 @pytest.mark.parametrize("explicit", [False, True])
 def test_matmul_arange_known_answer(device, mode, nfeed, explicit):
@@ -196,7 +196,7 @@ def test_vectordot_arange_known_answer(device):
         np.testing.assert_allclose(out, g[f"arange_CPUVectorDot_f{nfeed}_p2_e0_c1"], rtol=1e-7)
 
 
-@pytest.mark.parametrize("mode,tol", [("bf16x6", 1e-6), ("tf32x3", 1e-6), ("bf16x3", 3e-5)])
+@pytest.mark.parametrize("mode,tol", [("bf16x6", 1e-6), ("tf32x3", 1e-6), ("fp16x3", 1e-6), ("bf16x3", 3e-5)])
 @pytest.mark.parametrize("nant,nfeed,K,k_chunk", [(350, 2, 20000, 2048), (64, 1, 777, 64), (129, 2, 4096, 1024)])
 def test_matmul_random_vs_oracle(device, mode, tol, nant, nfeed, K, k_chunk):
     rng = np.random.default_rng(nant + K)
@@ -215,7 +215,7 @@ def test_matmul_random_vs_oracle(device, mode, tol, nant, nfeed, K, k_chunk):
 def test_matmul_sparse_pairs_vs_reference(device):
     g = golden("matprod")
     z, pairs = g["random_z"], g["random_pairs"]
-    for mode in ("bf16x6", "tf32x3"):
+    for mode in ("bf16x6", "tf32x3", "fp16x3"):
         mp = mv.B200MatMul(nchunks=1, nfeed=2, nant=7, antpairs=pairs, precision=2, gemm_mode=mode)
         mp.setup()
         out = np.zeros((len(pairs), 2, 2), dtype=complex)
@@ -237,19 +237,20 @@ def test_vectordot_random_vs_reference(device):
     np.testing.assert_allclose(out, ref, rtol=0, atol=1e-6 * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("mode", ["bf16x6", "fp16x3"])
 @pytest.mark.parametrize("k_chunk", [512, 2048, 8192])
-def test_herk_accumulation_positive_sums(device, k_chunk):
+def test_herk_accumulation_positive_sums(device, k_chunk, mode):
     """All-positive terms (autocorrelation-like) over a long K: FP32 TMEM
     accumulation per k-slice, FP64 across slices."""
     rng = np.random.default_rng(1)
     M, K = 128, 65536
     z = rng.uniform(0.5, 1.5, size=(M, K)) * np.exp(1j * 0.01 * rng.normal(size=(M, K)))
-    mp = mv.B200MatMul(nchunks=1, nfeed=1, nant=M, antpairs=None, precision=2, gemm_mode="bf16x6", k_chunk=k_chunk)
+    mp = mv.B200MatMul(nchunks=1, nfeed=1, nant=M, antpairs=None, precision=2, gemm_mode=mode, k_chunk=k_chunk)
     mp.setup()
     out = torch.zeros((M * M, 1, 1), dtype=torch.complex128, device=DEV)
     mp(z, 0)
     mp.sum_chunks(out)
     ref = orc.matmul_vis(z.astype(np.complex64).astype(np.complex128), M, 1)
     rel = np.abs(out.cpu().numpy() - ref) / np.abs(ref)
-    print(f"k_chunk={k_chunk}: max rel {rel.max():.3e}, mean rel {rel.mean():.3e}")
+    print(f"{mode} k_chunk={k_chunk}: max rel {rel.max():.3e}, mean rel {rel.mean():.3e}")
     assert rel.max() < 2e-6

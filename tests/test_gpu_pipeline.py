@@ -49,7 +49,7 @@ def _cos(v, ref, nfeed):
                                    nfeed)
 
 
-@pytest.mark.parametrize("mode", ["bf16x6", "tf32x3"])
+@pytest.mark.parametrize("mode", ["bf16x6", "tf32x3", "fp16x3"])
 def test_config1_full_vs_oracle(device, mode):
     cfg = wl.config1()
     ref = _oracle_job(cfg)  # (Nf, Nt, Npairs)
@@ -69,7 +69,7 @@ def test_config1_graph_replay_identical(device):
     assert torch.equal(v1, v2) and torch.equal(v2, v3)
 
 
-@pytest.mark.parametrize("mode", ["bf16x6", "tf32x3"])
+@pytest.mark.parametrize("mode", ["bf16x6", "tf32x3", "fp16x3"])
 def test_config2_subset_vs_oracle(device, mode):
     """HERA-350-like array and beams, 20k sources, 2 frequencies x 2 times."""
     cfg = wl.subset(wl.config2(nfreq=64, ntimes=16), nsrc=20000, nfreq=2, ntimes=2, seed=1)

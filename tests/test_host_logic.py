@@ -148,3 +148,67 @@ def test_shard_spec_slices_fluxes():
     assert (f0, f1) == (3, 5)
     np.testing.assert_array_equal(s1.fluxes, spec.fluxes[:, 3:5])
     np.testing.assert_array_equal(s1.freqs, [3.0, 4.0])
+
+
+def _golden_astrom(t):
+    g = golden("erfa")
+    return {k: (g[f"t{t}_{k}"] if g[f"t{t}_{k}"].ndim else float(g[f"t{t}_{k}"]))
+            for k in ("eh", "em", "v", "bm1", "bpn", "eral", "xpl", "ypl", "sphi", "cphi")}
+
+
+def test_atioq_matrix_reproduces_reference_topocentric():
+    """The host 3x3 of the ERFA-style rotation against the reference's _atioq output."""
+    from matvis_b200.coordinates import atioq_matrix
+
+    g = golden("erfa")
+    for t in range(3):
+        a = _golden_astrom(t)
+        np.testing.assert_allclose(atioq_matrix(a) @ g[f"t{t}_bcrs"], g[f"t{t}_topo"], rtol=0, atol=2e-15)
+
+
+def test_pack_astrom_layout():
+    from matvis_b200.coordinates import pack_astrom
+
+    a = _golden_astrom(1)
+    p = pack_astrom(a)
+    assert p.shape == (18,) and p.dtype == np.float64 and p.flags["C_CONTIGUOUS"]
+    np.testing.assert_array_equal(p[0:3], a["eh"])
+    assert p[3] == a["em"] and p[4] == 1e-6 and p[8] == a["bm1"]
+    np.testing.assert_array_equal(p[5:8], a["v"])
+    np.testing.assert_array_equal(p[9:18], np.asarray(a["bpn"]).reshape(9))
+
+
+def test_bcrs_refresh_plan_follows_update_interval():
+    from matvis_b200.coordinates import bcrs_refresh_plan
+
+    ts = np.array([0.0, 60.0, 120.0, 181.0, 240.0, 400.0])
+    assert bcrs_refresh_plan(ts, 0.0) == [True] * 6
+    # refresh strictly after 180 s since the last refresh
+    assert bcrs_refresh_plan(ts, 180.0) == [True, False, False, True, False, True]
+    assert bcrs_refresh_plan(ts, 1e9) == [True] + [False] * 5
+
+
+def test_coord_method_keywords():
+    from matvis_b200.simulate import _check_coord_method
+
+    assert _check_coord_method("CoordinateRotationLST") == {}
+    with pytest.raises(NotImplementedError):
+        _check_coord_method("CoordinateRotationAstropy")
+    with pytest.raises(ValueError):
+        _check_coord_method("CoordinateRotationERFA", {})
+    with pytest.raises(ValueError):
+        _check_coord_method("Nope")
+    kw = _check_coord_method("GPUCoordinateRotationERFA", {"astrom": [{}], "time_s": [0.0], "update_bcrs_every": 5})
+    assert kw["update_bcrs_every"] == 5.0 and kw["time_s"] == [0.0] and len(kw["astrom"]) == 1
+
+
+def test_oracle_erfa_refresh_reuses_directions():
+    """With a long update interval the oracle's ERFA path rotates the first
+    time's apparent directions at every later time (cpu/coords.py:194-199)."""
+    g = golden("erfa")
+    eci = g["eci"]
+    astrom = [_golden_astrom(t) for t in range(3)]
+    b0 = orc.erfa_bcrs(eci, astrom[0])
+    for t in range(3):
+        topo = orc.rotate_fixed_order(orc.erfa_atioq_matrix(astrom[t]), b0)
+        np.testing.assert_allclose(topo, orc.erfa_atioq_matrix(astrom[t]) @ b0, rtol=0, atol=4e-16)

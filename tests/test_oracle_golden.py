@@ -163,3 +163,22 @@ def test_pipeline_polarized_matches_reference(method, name):
         nchunks=2,
     )
     np.testing.assert_allclose(vis, g[f"b_vis_{method}_{name}"], rtol=1e-9, atol=1e-11)
+
+
+def _astrom(g, t):
+    keys = ("eh", "em", "v", "bm1", "bpn", "eral", "xpl", "ypl", "sphi", "cphi")
+    return {k: (g[f"t{t}_{k}"] if g[f"t{t}_{k}"].ndim else float(g[f"t{t}_{k}"])) for k in keys}
+
+
+def test_erfa_steps_match_reference():
+    """cpu/coords.py:89-181 (_ld, _ab, _bpn, _atioq) through the reference's own methods."""
+    g = golden("erfa")
+    for t in range(3):
+        a = _astrom(g, t)
+        p1 = orc.erfa_ld(g["eci"], a["eh"], a["em"], 1e-6)
+        np.testing.assert_allclose(p1, g[f"t{t}_after_ld"], rtol=0, atol=1e-15)
+        p2 = orc.erfa_ab(g[f"t{t}_after_ld"], a["v"], a["em"], a["bm1"])
+        np.testing.assert_allclose(p2, g[f"t{t}_after_ab"], rtol=0, atol=1e-15)
+        np.testing.assert_allclose(orc.erfa_bcrs(g["eci"], a), g[f"t{t}_bcrs"], rtol=0, atol=2e-15)
+        top = orc.erfa_atioq_matrix(a) @ g[f"t{t}_bcrs"]
+        np.testing.assert_allclose(top, g[f"t{t}_topo"], rtol=0, atol=2e-15)
