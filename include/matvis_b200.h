@@ -220,6 +220,16 @@ int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host
                const int32_t *pairs, int64_t npairs, int k_chunk, void *ws, size_t ws_bytes, void *out, int out_c128,
                int accumulate, void *stream);
 
+/* ---- Redundant-baseline pair selection (host memory, no device work) ------- */
+/* bls: (nant, nant, 2) float64 baselines, bls[i, j] = pos[j, :2] - pos[i, :2].
+ * Writes the pairs (i, j), i < j, that get_redundancies (cli.py:273-290) keeps:
+ * baselines rounded to ndecimals decimals as numpy's round does, visited with i
+ * slow, kept when neither (u, v) nor (-u, -v) was kept before.  pairs_out is
+ * int32 [cap][2]; *n_out receives the count (MVB_ERR_OVERFLOW when it exceeds
+ * cap, after counting all of them).  Feeds mvb_vecdot's pair list. */
+int mvb_redundant_pairs(const double *bls, int64_t nant, int ndecimals, int32_t *pairs_out, int64_t cap,
+                        int64_t *n_out);
+
 #ifdef __cplusplus
 }
 #endif

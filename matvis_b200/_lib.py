@@ -47,6 +47,7 @@ _SIGNATURES = {
     "mvb_device_info": (c_int, [_p, _p, _p]),
     "mvb_rotate": (c_int, [_p, c_int64, _p, _p, _p]),
     "mvb_bcrs": (c_int, [_p, c_int64, _p, _p, _p]),
+    "mvb_redundant_pairs": (c_int, [_p, c_int64, c_int, _p, c_int64, _p]),
     "mvb_horizon_ws_bytes": (c_size_t, [c_int64]),
     "mvb_horizon_compact": (
         c_int,

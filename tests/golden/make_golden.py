@@ -19,7 +19,11 @@ reference functions return:
 * ``pipeline.npz``  -- end-to-end visibilities from the reference plugin classes
   driven in the loop order of ``cpu/cpu.py:247-272``;
 * ``erfa.npz``      -- ``CoordinateRotationERFA._ld / _ab / _bpn / _atioq``
-  (``cpu/coords.py:89-181``) on seeded unit vectors and astrom parameters.
+  (``cpu/coords.py:89-181``) on seeded unit vectors and astrom parameters;
+* ``redundancies.npz`` -- ``get_redundancies`` (``cli.py:273-290``) on hexagonal,
+  jittered, random and co-located antenna layouts.  ``cli.py`` imports click,
+  astropy, line_profiler and pyuvdata at module level, so only that function's
+  source is compiled (it needs numpy alone).
 
 The fixtures are small (< 1 MB) and committed; the tests never read the
 reference tree.
@@ -422,6 +426,44 @@ def make_erfa():
     _save("erfa.npz", **out)
 
 
+def reference_get_redundancies():
+    import ast
+
+    src = (refload.REF_ROOT / "src" / "matvis" / "cli.py").read_text()
+    tree = ast.parse(src)
+    fn = next(n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == "get_redundancies")
+    mod = ast.Module(body=[fn], type_ignores=[])
+    ns = {"np": np}
+    exec(compile(mod, "cli.py", "exec"), ns)
+    return ns["get_redundancies"]
+
+
+def make_redundancies():
+    sys.path.insert(0, str(HERE.parents[1]))
+    from matvis_b200 import workloads as wl
+
+    get_red = reference_get_redundancies()
+    rng = np.random.default_rng(41)
+    layouts = {
+        "hex37": wl.hex_array(37, 14.6),
+        "hex127_jitter": wl.hex_array(127, 14.6) + np.column_stack([rng.normal(0, 2e-3, (127, 2)), np.zeros(127)]),
+        "hera350": wl.hera350(np.random.default_rng(20261205)),
+        "random40": np.column_stack([rng.uniform(-100, 100, (40, 2)), np.zeros(40)]),
+        "colocated": np.array([[0, 0, 0], [0, 0, 0], [14.6, 0, 0], [14.6, 0, 0], [0, 14.6, 0], [-14.6, 0, 0.0]]),
+        "line_half": np.column_stack([np.arange(12) * 0.005, np.zeros(12), np.zeros(12)]),
+        "two": np.array([[0.0, 0, 0], [1.0, 2.0, 0]]),
+        "one": np.zeros((1, 3)),
+    }
+    out = {}
+    for name, pos in layouts.items():
+        bls = pos[np.newaxis, :, :2] - pos[:, np.newaxis, :2]
+        for nd in (2, 0, -1):
+            pairs = np.asarray(get_red(bls, ndecimals=nd), dtype=np.int64).reshape(-1, 2)
+            out[f"{name}_pos"] = pos
+            out[f"{name}_nd{nd}"] = pairs
+    _save("redundancies.npz", **out)
+
+
 if __name__ == "__main__":
     make_matprod()
     make_bilinear()
@@ -430,3 +472,4 @@ if __name__ == "__main__":
     make_chunks()
     make_pipeline()
     make_erfa()
+    make_redundancies()

@@ -198,3 +198,21 @@ def test_plugin_chain_matches_engine(device):
         mp.sum_chunks(vis[t])
     ref = _oracle_job(dict(cfg, freqs=cfg["freqs"][:1], fluxes=cfg["fluxes"][:, :1]))[0]
     assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6
+
+
+@pytest.mark.parametrize("matprod", ["VectorDot", "MatMul"])
+def test_redundant_pairs_through_products(device, matprod):
+    """Redundant-baseline representatives of a 37-element hexagon (the
+    hera_profile pair list, cli.py:316-319) through both products."""
+    from matvis_b200.pairs import redundant_antpairs
+
+    cfg = wl.config1()
+    cfg["antpos"] = wl.hex_array(37, 14.6)
+    cfg["antpairs"] = redundant_antpairs(cfg["antpos"])
+    assert len(cfg["antpairs"]) == 63
+    ref = _oracle_job(cfg, matprod="VectorDot")
+    vis = _engine(cfg, precision=2, matprod=matprod).run().cpu().numpy()[..., 0, 0]
+    assert vis.shape == ref.shape
+    full = _oracle_job(dict(cfg, antpairs=None))
+    scale = np.abs(full).max()
+    np.testing.assert_allclose(vis, ref, rtol=0, atol=1e-6 * scale)

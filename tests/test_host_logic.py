@@ -212,3 +212,39 @@ def test_oracle_erfa_refresh_reuses_directions():
     for t in range(3):
         topo = orc.rotate_fixed_order(orc.erfa_atioq_matrix(astrom[t]), b0)
         np.testing.assert_allclose(topo, orc.erfa_atioq_matrix(astrom[t]) @ b0, rtol=0, atol=4e-16)
+
+
+@pytest.mark.parametrize("layout", ["hex37", "hex127_jitter", "hera350", "random40", "colocated", "line_half", "two",
+                                    "one"])
+@pytest.mark.parametrize("nd", [2, 0, -1])
+def test_redundant_pairs_match_reference(layout, nd):
+    """mvb_redundant_pairs against the reference's get_redundancies (cli.py:273-290)."""
+    from matvis_b200.pairs import baselines, get_redundancies
+
+    g = golden("redundancies")
+    got = np.asarray(get_redundancies(baselines(g[f"{layout}_pos"]), ndecimals=nd), dtype=np.int64).reshape(-1, 2)
+    np.testing.assert_array_equal(got, g[f"{layout}_nd{nd}"])
+
+
+def test_redundant_pairs_errors_and_capacity():
+    import ctypes
+
+    from matvis_b200 import _lib
+    from matvis_b200.pairs import get_redundancies
+
+    with pytest.raises(ValueError):
+        get_redundancies(np.zeros((3, 2, 2)))
+    bls = np.zeros((3, 3, 2))
+    bls[0, 1] = (1.0, 0.0)
+    bls[0, 2] = (0.0, 1.0)
+    bls[1, 2] = (np.nan, 0.0)
+    with pytest.raises(ValueError):
+        get_redundancies(bls)
+    bls[1, 2] = (-1.0, 1.0)
+    assert get_redundancies(bls) == [[0, 1], [0, 2], [1, 2]]
+    out = np.zeros((1, 2), dtype=np.int32)
+    n = ctypes.c_int64(0)
+    rc = _lib.lib.mvb_redundant_pairs(bls.ctypes.data_as(ctypes.c_void_p), 3, 2, out.ctypes.data_as(ctypes.c_void_p),
+                                      1, ctypes.byref(n))
+    assert rc == _lib.MVB_ERR_OVERFLOW and n.value == 3 and out.tolist() == [[0, 1]]
+    assert get_redundancies(np.zeros((0, 0, 2))) == []
