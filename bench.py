@@ -45,13 +45,21 @@ UNIT = "antenna-pair×source terms/s"
 SPEED_OF_LIGHT = 299792458.0
 
 
+GEMM_PRECISION = {
+    "fp16x3": "2-term fp16 split of the power-of-two-scaled Z (3 products)",
+    "bf16x6": "3-term bf16 split (6 products)",
+    "bf16x3": "2-term bf16 split (3 products)",
+    "tf32x3": "2-term tf32 split (3 products)",
+}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--gemm-mode", default="bf16x6")
+    ap.add_argument("--gemm-mode", default="fp16x3", choices=sorted(GEMM_PRECISION))
     ap.add_argument("--k-chunk", type=int, default=None)
     ap.add_argument("--nfreq", type=int, default=64)
     ap.add_argument("--ntimes", type=int, default=16)
@@ -340,7 +348,7 @@ def run_b200(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": args.gemm_mode[:4],
+        "dtype": {"fp16x3": "fp16", "bf16x6": "bf16", "bf16x3": "bf16", "tf32x3": "tf32"}[args.gemm_mode],
         "data": "synthetic (seeded; HEALPix nside=128 centres, HERA-350-like array, dipole-like beams)",
         "config": {
             "workload": f"config2 HERA-350-like: 350 ant x {len(cfg['ra'])} src x {len(cfg['freqs'])} freq x "
@@ -351,9 +359,9 @@ def run_b200(args, rank, world, local_rank):
                                                                           panel.data.element_size() / 1e9 * kvalid /
                                                                           panel.Kcap),
             "parallelism": "replicas (one job per GPU)" if world > 1 else "1 GPU",
-            "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, split-bf16 6-product "
-                         "tcgen05 Hermitian product with FP32 TMEM accumulation per k-slice, FP64 slice sums"
-                         if args.gemm_mode == "bf16x6" else args.gemm_mode,
+            "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, "
+                         + GEMM_PRECISION[args.gemm_mode]
+                         + " tcgen05 Hermitian product, FP32 register sums per drained TMEM block, FP64 slice sums",
         },
         "roofline": roofline,
         "gpu_launches": eng.launches_per_run() * args.steps,

@@ -144,7 +144,11 @@ int mvb_beam_gaussian(const double *sigmas, int nbeam, const double *crd, int64_
  * Replaces TauCalculator.__call__ (core/tau.py:48-71). */
 int mvb_exptau(const double *antpos, int A, double freq, const double *crd, int64_t ld, int64_t nsrc,
                void *exptau, int out_c128, void *stream);
-/* Bytes of a Z panel for the given mode (2P planes of Mpad x Kcap). */
+/* Z panel layout (modes MVB_GEMM_*): 2P planes (plane 2p + c holds split term
+ * p of component c, c = 0 real, 1 imaginary), each k-blocked as
+ * [Kcap / KB][Mpad][KB] with KB = 32 bytes of elements (16 for bf16 / fp16, 8
+ * for tf32): element (m, k) of a plane is at (k / KB) * Mpad * KB + m * KB + k % KB.
+ * Mpad is a multiple of 128, Kcap of 64.  Bytes: 2P x Mpad x Kcap x element size. */
 size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap);
 /* Fused tau + Z: Z[a*F+f, s*X+x] = exptau(a, s) * sflux[j] * beam[bidx[a], f, x, s]
  * with j = sidx[s] (sidx != NULL: sflux is the full per-source sqrt(0.5 I) at

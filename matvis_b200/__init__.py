@@ -10,6 +10,7 @@ without the built library raises ImportError.
 from . import _lib  # noqa: F401  (loads libmatvis_b200.so, fails loudly if absent)
 from ._lib import GEMM_MODES, MatvisB200Error
 from ._utils import get_desired_chunks, get_dtypes, get_required_chunks
+from .beamfits import BeamFits, read_beamfits, write_beamfits
 from .beams import B200BeamInterpolator, BeamInterpolator, GaussianBeam, GridBeam
 from .coordinates import SkyCoords, eci_to_enu_matrix, enu_to_az_za, enu_to_eci_matrix, point_source_crd_eq
 from .coords import CoordinateRotation, CoordinateRotationERFA, CoordinateRotationLST
@@ -23,6 +24,7 @@ HAVE_GPU = True
 
 __all__ = [
     "B200BeamInterpolator",
+    "BeamFits",
     "B200MatMul",
     "B200VectorDot",
     "BeamInterpolator",
@@ -47,6 +49,8 @@ __all__ = [
     "get_dtypes",
     "get_required_chunks",
     "point_source_crd_eq",
+    "read_beamfits",
     "simulate",
     "simulate_vis",
+    "write_beamfits",
 ]

@@ -174,6 +174,12 @@ def zpanel_dtype(mode: int) -> torch.dtype:
             GEMM_F16_3: torch.float16, Z_C64: torch.complex64}[mode]
 
 
+def zpanel_kblock(mode: int) -> int:
+    """Elements per 32-byte k-block of a split-plane panel (planes are stored
+    [Kcap / KB][Mpad][KB])."""
+    return 32 // torch.empty((), dtype=zpanel_dtype(mode)).element_size()
+
+
 def zpanel_planes(mode: int) -> int:
     return {GEMM_BF16_3: 4, GEMM_BF16_6: 6, GEMM_TF32_3: 4, GEMM_F16_3: 4, Z_C64: 1}[mode]
 

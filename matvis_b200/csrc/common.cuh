@@ -54,6 +54,15 @@ constexpr int kTile = 128;
 __host__ __device__ inline int mode_terms(int mode) { return mode == MVB_GEMM_BF16_6 ? 3 : 2; }
 __host__ __device__ inline int mode_elem_bytes(int mode) { return mode == MVB_GEMM_TF32_3 ? 4 : 2; }
 
+// Split-plane panel layout: each plane is stored k-blocked, [Kcap / KB][Mpad][KB]
+// with KB = 32 bytes of elements (16 bf16 / fp16, 8 tf32), so the 128-row x
+// 32-byte box one k-step of the Hermitian product loads is one contiguous 4 KB
+// run of HBM (a row-major plane would scatter it over 128 DRAM pages).
+constexpr int kKBlockBytes = 32;
+__host__ __device__ inline int64_t panel_off(int64_t m, int64_t k, int64_t Mpad, int kb) {
+  return (k / kb) * (Mpad * kb) + m * kb + (k % kb);
+}
+
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
@@ -117,6 +126,16 @@ __device__ __forceinline__ void tma_load_3d(void *smem_dst, const void *map, uin
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(smem_dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// 4-D tiled load, no multicast, into this CTA's shared memory.
+__device__ __forceinline__ void tma_load_4d(void *smem_dst, const void *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
 }
 

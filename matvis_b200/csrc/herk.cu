@@ -64,6 +64,7 @@ struct HerkCfg {
   static constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
   static constexpr int ES = MODE == MVB_GEMM_TF32_3 ? 4 : 2;
   static constexpr int KSTEP = 32 / ES;  // elements per 32-byte k-step (= UMMA K)
+  static_assert(KSTEP * ES == kKBlockBytes, "one k-step is one k-block of the panel");
   static constexpr int OPER_BYTES = 2 * P * kPlaneBytes;
   static constexpr int STAGE_BYTES = 2 * OPER_BYTES;
   static constexpr int STAGES = kSmemBudget / STAGE_BYTES;
@@ -210,9 +211,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         }
         mbar_arrive_expect_tx(&full_bar[st], bytes);
         uint8_t *a = smem + (size_t)st * C::STAGE_BYTES;
-        const int kc = (int)(k0 + (int64_t)ks * C::KSTEP);
-        tma_load_3d(a, &zmap, &full_bar[st], kc, I * 128, 0);
-        if (!diag) tma_load_3d(a + C::OPER_BYTES, &zmap, &full_bar[st], kc, J * 128, 0);
+        // k-block index: k0 is a multiple of 64 and each k-step is one 32-byte block
+        const int kb = (int)((k0 + (int64_t)ks * C::KSTEP) / C::KSTEP);
+        tma_load_4d(a, &zmap, &full_bar[st], 0, I * 128, kb, 0);
+        if (!diag) tma_load_4d(a + C::OPER_BYTES, &zmap, &full_bar[st], 0, J * 128, kb, 0);
         ++issued;
         if (++st == C::STAGES) {
           st = 0;
@@ -497,14 +499,17 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   auto enc = tensor_map_encoder();
   if (!enc) return fail(MVB_ERR_UNSUPPORTED, "mvb_herk: cuTensorMapEncodeTiled unavailable");
   CUtensorMap map;
-  cuuint64_t dims[3] = {(cuuint64_t)Kcap, (cuuint64_t)Mpad, (cuuint64_t)(2 * C::P)};
-  cuuint64_t strides[2] = {(cuuint64_t)Kcap * C::ES, (cuuint64_t)Mpad * Kcap * C::ES};
-  cuuint32_t box[3] = {(cuuint32_t)C::KSTEP, 128u, (cuuint32_t)(2 * C::P)};
-  cuuint32_t estr[3] = {1, 1, 1};
+  // k-blocked planes [2P][Kcap / KSTEP][Mpad][KSTEP]: one k-step of 128 rows is a
+  // contiguous 4 KB run per plane; the box lands in shared memory as
+  // [plane][row][32 bytes], the layout of the row-major map it replaces.
+  cuuint64_t dims[4] = {(cuuint64_t)C::KSTEP, (cuuint64_t)Mpad, (cuuint64_t)(Kcap / C::KSTEP), (cuuint64_t)(2 * C::P)};
+  cuuint64_t strides[3] = {(cuuint64_t)kKBlockBytes, (cuuint64_t)Mpad * kKBlockBytes, (cuuint64_t)Mpad * Kcap * C::ES};
+  cuuint32_t box[4] = {(cuuint32_t)C::KSTEP, 128u, 1u, (cuuint32_t)(2 * C::P)};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUtensorMapDataType dt = MODE == MVB_GEMM_TF32_3  ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : MODE == MVB_GEMM_F16_3 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                           : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  CUresult r = enc(&map, dt, 3,
+  CUresult r = enc(&map, dt, 4,
                    const_cast<void *>(z), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(MVB_ERR_CUDA, "mvb_herk: cuTensorMapEncodeTiled failed (%d)", (int)r);

@@ -152,21 +152,23 @@ struct PanelWriter {
 
 constexpr int kTauZThreads = 64;
 constexpr int kTauZSrc = 4;      // consecutive sources per thread
-constexpr int kTauZAnts = 8;     // antennas per CTA
-constexpr int kTauZMaxBFX = 16;  // nbeam * F * X staged per source
+constexpr int kTauZAnts = 32;    // antennas per CTA (the CTA's beam block is read once per 32 antennas)
+constexpr int kTauZMaxBFX = 16;  // beams staged in shared memory up to nbeam * F * X = 16, else read from L2
 constexpr int kTauZBlockSrc = kTauZThreads * kTauZSrc;
 
-// grid.x: blocks of kTauZBlockSrc sources, grid.y: antenna blocks.
+// grid.x: blocks of kTauZBlockSrc sources, grid.y: antenna blocks.  Dynamic
+// shared memory: the CTA's beam values, [q][j][thread] (thread fastest, so the
+// per-antenna reads are conflict-free), q = (beam * F + f) * X + x.
 // EXT = 0: phase from antpos . crd (fused tau); EXT = 1 / 2: phase factor read
 // from a caller exptau (A, e_ld) in complex64 / complex128, multiplied by sflux.
-template <int MODE, int X, int EXT = 0>
+template <int MODE, int X, int EXT = 0, bool STAGED = true>
 __global__ void __launch_bounds__(kTauZThreads)
     tau_z_kernel(const double *__restrict__ antpos, int A, double f_over_c, const double *__restrict__ crd, int64_t ld,
                  const int32_t *__restrict__ n_dev, int64_t nsrc, const float *__restrict__ sflux,
                  const int32_t *__restrict__ sidx, const float2 *__restrict__ beam, int64_t beam_ld, int nbeam,
                  const int32_t *__restrict__ beam_idx, int F, float zscale, void *__restrict__ z, int64_t Mpad,
                  int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
-  __shared__ float2 bsm[kTauZMaxBFX][kTauZThreads][kTauZSrc];
+  extern __shared__ float2 bsm[];
   const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
   const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
   const int64_t s0 = ((int64_t)blockIdx.x * kTauZThreads + threadIdx.x) * kTauZSrc;
@@ -191,10 +193,13 @@ __global__ void __launch_bounds__(kTauZThreads)
     }
   }
   const int nbfx = nbeam * F * X;
-  for (int q = 0; q < nbfx; ++q)
+  if constexpr (STAGED) {
+    for (int q = 0; q < nbfx; ++q)
 #pragma unroll
-    for (int j = 0; j < kTauZSrc; ++j)
-      bsm[q][threadIdx.x][j] = (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
+      for (int j = 0; j < kTauZSrc; ++j)
+        bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x] =
+            (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
+  }
   // (each thread reads only its own entries of bsm: no barrier needed)
 
   const int a0 = blockIdx.y * kTauZAnts;
@@ -236,19 +241,25 @@ __global__ void __launch_bounds__(kTauZThreads)
       for (int j = 0; j < kTauZSrc; ++j)
 #pragma unroll
         for (int x = 0; x < X; ++x) {
-          const float2 bv = bsm[(b * F + f) * X + x][threadIdx.x][j];
+          const int q = (b * F + f) * X + x;
+          float2 bv;
+          if constexpr (STAGED)
+            bv = bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x];
+          else
+            bv = (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
           vr[j * X + x] = er[j] * bv.x - ei[j] * bv.y;
           vi[j * X + x] = er[j] * bv.y + ei[j] * bv.x;
         }
       if (!write) continue;
       const int64_t m = (int64_t)a * F + f;
-      const int64_t off = m * Kcap + s0 * X;
       if constexpr (MODE == MVB_Z_C64) {
-        float2 *zp = static_cast<float2 *>(z) + off;
+        float2 *zp = static_cast<float2 *>(z) + m * Kcap + s0 * X;
 #pragma unroll
         for (int i = 0; i < kTauZSrc * X; i += 2)
           *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
       } else {
+        // kTauZSrc * X consecutive k from a multiple of kTauZSrc * X: inside one k-block
+        const int64_t off = panel_off(m, s0 * X, Mpad, kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2));
         put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr, zscale);
         put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi, zscale);
       }
@@ -296,10 +307,11 @@ __global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, i
         vr[x] = vi[x] = 0.f;
       }
     }
-    const int64_t off = m * Kcap + k;
     if constexpr (MODE == MVB_Z_C64) {
-      *reinterpret_cast<float4 *>(static_cast<float2 *>(z) + off) = make_float4(vr[0], vi[0], vr[1], vi[1]);
+      *reinterpret_cast<float4 *>(static_cast<float2 *>(z) + m * Kcap + k) = make_float4(vr[0], vi[0], vr[1], vi[1]);
     } else {
+      // (k, k + 1), k even: inside one k-block
+      const int64_t off = panel_off(m, k, Mpad, kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2));
       PanelWriter<MODE>::put(z, plane, off, 0, vr, 2, zscale);
       PanelWriter<MODE>::put(z, plane, off, 1, vi, 2, zscale);
     }
@@ -365,8 +377,9 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
                          int nbeam, const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z,
                          int64_t Mpad, int64_t Kcap, void *stream) {
   if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !sflux || (nsrc > 0 && !crd) || (F != 1 && F != 2) ||
-      (X != 1 && X != 2) || nbeam <= 0 || nbeam * F * X > kTauZMaxBFX || beam_ld < nsrc)
+      (X != 1 && X != 2) || nbeam <= 0 || beam_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_tau_z: bad arguments");
+  const bool staged = nbeam * F * X <= kTauZMaxBFX;
   int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z");
   if (rc) return rc;
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z: Kcap too small for nsrc * nax");
@@ -374,11 +387,18 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
   if (s_max == 0) return MVB_OK;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
   const double foc = freq * kInvC;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_TAUZ(M, XX)                                                                                              \
-  tau_z_kernel<M, XX><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld,   \
-                                                    nbeam, beam_idx, F, zscale, z, Mpad, Kcap)
+#define MVB_TAUZ(M, XX)                                                                                        \
+  do {                                                                                                         \
+  if (staged)                                                                                                  \
+    tau_z_kernel<M, XX, 0, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
+                                                                bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
+  else                                                                                                         \
+    tau_z_kernel<M, XX, 0, false><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
+                                                              bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
+  } while (0)
 #define MVB_TAUZ2(M) \
   if (X == 2)        \
     MVB_TAUZ(M, 2);  \
@@ -431,19 +451,29 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
                                  const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X,
                                  int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap, void *stream) {
   if (A <= 0 || nsrc < 0 || !exptau || !z || !beam || !sflux || (F != 1 && F != 2) || (X != 1 && X != 2) ||
-      nbeam <= 0 || nbeam * F * X > kTauZMaxBFX || beam_ld < nsrc || e_ld < nsrc)
+      nbeam <= 0 || beam_ld < nsrc || e_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_z_from_exptau: bad arguments");
+  const bool staged = nbeam * F * X <= kTauZMaxBFX;
   int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_z_from_exptau");
   if (rc) return rc;
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_z_from_exptau: Kcap too small");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_ZX(M, XX, E)                                                                                              \
-  tau_z_kernel<M, XX, E><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, nullptr, bm, \
-                                                       beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, exptau, e_ld)
+#define MVB_ZX(M, XX, E)                                                                                       \
+  do {                                                                                                         \
+  if (staged)                                                                                                  \
+    tau_z_kernel<M, XX, E, true><<<grid, kTauZThreads, smem, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, \
+                                                                nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z, \
+                                                                Mpad, Kcap, exptau, e_ld);                    \
+  else                                                                                                         \
+    tau_z_kernel<M, XX, E, false><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux,  \
+                                                              nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z,  \
+                                                              Mpad, Kcap, exptau, e_ld);                    \
+  } while (0)
 #define MVB_ZX3(M, E) \
   if (X == 2)         \
     MVB_ZX(M, 2, E);  \

@@ -16,6 +16,8 @@ whole job can be captured once as a CUDA graph and replayed.
 
 from __future__ import annotations
 
+import queue
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -46,7 +48,7 @@ class JobSpec:
     polarized: bool = False
     antpairs: np.ndarray | None = None
     precision: int = 1
-    gemm_mode: str = "bf16x6"
+    gemm_mode: str = "fp16x3"
     matprod: str = "MatMul"  # or "VectorDot"
     k_chunk: int | None = None
     source_buffer: float = 1.0
@@ -246,6 +248,63 @@ class VisEngine:
             torch.cuda.current_stream().synchronize()
             _lib.check_status_word(self.status, "VisEngine")
         return self.vis
+
+    def run_to_host(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Run the job and return the visibilities in host memory (``out`` if given).
+
+        As soon as the kernels of a time step have run, a helper thread copies
+        that step's visibilities (all frequencies) into ``out`` on its own
+        stream, so the device -> host copy, and the first touch of freshly
+        allocated host pages (slower than the copy itself), overlap the compute
+        of the later time steps.
+        """
+        if not self._allocated:
+            self.upload()
+        shape = tuple(self.vis.shape)
+        dtype = np.complex64 if self.ctype == torch.complex64 else np.complex128
+        if out is None:
+            out = np.empty(shape, dtype=dtype)
+        elif out.shape != shape or out.dtype != dtype or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous {dtype.__name__} array of shape {shape}")
+        host = torch.from_numpy(out)
+        nf, nt = shape[:2]
+        dev = self.vis.device
+        self.status.zero_()
+        main = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(device=dev)
+        steps: queue.Queue = queue.Queue()
+        errors: list[BaseException] = []
+
+        def copier():
+            try:
+                torch.cuda.set_device(dev)
+                with torch.cuda.stream(side):
+                    while (item := steps.get()) is not None:
+                        t, done = item
+                        side.wait_event(done)
+                        for f in range(nf):
+                            host[f, t].copy_(self.vis[f, t])
+            except BaseException as exc:  # re-raised on the calling thread
+                errors.append(exc)
+                while steps.get() is not None:
+                    pass
+
+        worker = threading.Thread(target=copier, name="mvb-d2h", daemon=True)
+        worker.start()
+        try:
+            for t in range(nt):
+                self.enqueue_time(t)
+                done = torch.cuda.Event()
+                done.record(main)
+                steps.put((t, done))
+        finally:
+            steps.put(None)
+            worker.join()
+        main.synchronize()
+        if errors:
+            raise errors[0]
+        _lib.check_status_word(self.status, "VisEngine")
+        return out
 
     def capture(self):
         """Capture the launch sequence as one CUDA graph (run once uncaptured first)."""

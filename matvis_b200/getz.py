@@ -18,9 +18,11 @@ from ._lib import check, ptr, stream_handle
 class ZPanel:
     """Device Z in split-plane (or plain complex64) layout.
 
-    ``data``: (planes, Mpad, Kcap) for the tensor-core modes, (M, Kcap) complex64
-    for the plain mode.  ``n_dev`` / ``n_host`` give the valid source count; the
-    valid K extent is that count times ``nax``.
+    ``data``: (planes, Kcap / KB, Mpad, KB) for the tensor-core modes -- each
+    plane k-blocked in 32-byte blocks of KB elements, so that one k-step of 128
+    rows is contiguous in HBM -- and (M, Kcap) complex64 for the plain mode.
+    ``n_dev`` / ``n_host`` give the valid source count; the valid K extent is
+    that count times ``nax``.
     """
 
     def __init__(self, mode: int, nant: int, nfeed: int, nax: int, nsrc_cap: int, device):
@@ -34,7 +36,8 @@ class ZPanel:
         if mode == _lib.Z_C64:
             self.data = torch.zeros((self.M, self.Kcap), dtype=dt, device=device)
         else:
-            self.data = torch.zeros((planes, self.Mpad, self.Kcap), dtype=dt, device=device)
+            kb = _lib.zpanel_kblock(mode)
+            self.data = torch.zeros((planes, self.Kcap // kb, self.Mpad, kb), dtype=dt, device=device)
         self.n_dev = None
         self.n_host = 0
         #: power-of-two factor the panel holds Z multiplied by (fp16x3 mode)
@@ -50,7 +53,8 @@ class ZPanel:
         k = n * self.nax
         if self.mode == _lib.Z_C64:
             return self.data[:, :k].to(torch.complex128)
-        d = self.data[:, : self.M, :k].to(torch.float64)
+        p, nkb, mpad, kb = self.data.shape
+        d = self.data.permute(0, 2, 1, 3).reshape(p, mpad, nkb * kb)[:, : self.M, :k].to(torch.float64)
         re = d[0::2].sum(0) / self.scale
         im = d[1::2].sum(0) / self.scale
         return torch.complex(re, im)
@@ -59,7 +63,7 @@ class ZPanel:
 class ZMatrixCalc:
     """Builds Z = A * sqrt(I) * exp(tau) on the device."""
 
-    def __init__(self, nant, nfeed, nax, nsrc, ctype=None, gpu: bool = True, mode: int | str = _lib.GEMM_BF16_6,
+    def __init__(self, nant, nfeed, nax, nsrc, ctype=None, gpu: bool = True, mode: int | str = _lib.GEMM_F16_3,
                  device=None):
         self.device = _lib.require_cuda(device)
         self.nant, self.nfeed, self.nax, self.nsrc = nant, nfeed, nax, nsrc

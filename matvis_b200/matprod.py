@@ -132,7 +132,7 @@ class MatProd(ABC):
 class B200MatMul(MatProd):
     """Hermitian product V = conj(Z) Z^T, upper-triangle tiles on the tensor cores."""
 
-    def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, gemm_mode: str | int = "bf16x6",
+    def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, gemm_mode: str | int = "fp16x3",
                  k_chunk: int | None = None, device=None, drain_ksteps: int = 0):
         super().__init__(nchunks, nfeed, nant, antpairs, precision=precision, device=device)
         #: k-steps per TMEM block before the drain to FP32 registers (0: the mode's default)

@@ -8,7 +8,9 @@ dependencies):
 * ``times`` are local sidereal times in radians and ``telescope_loc`` is the
   latitude in radians (or an object with ``.lat``); the rotation is the rigid
   LST rotation (``coord_method="CoordinateRotationLST"``);
-* beams are :class:`~matvis_b200.beams.GridBeam` / :class:`~matvis_b200.beams.GaussianBeam`;
+* beams are :class:`~matvis_b200.beams.GridBeam` / :class:`~matvis_b200.beams.GaussianBeam`
+  or a beamfits beam (:func:`~matvis_b200.beamfits.read_beamfits`), interpolated to
+  each frequency;
 * ``skycoords`` is an (ra, dec) pair in radians or an object with ``.ra``/``.dec``.
 
 Both run the batched engine (``engine.VisEngine``): every time and frequency of
@@ -26,6 +28,16 @@ from . import _lib
 from ._utils import get_desired_chunks
 from .coordinates import latitude_of, lsts_of, point_source_crd_eq, radec_of
 from .engine import JobSpec, VisEngine, _norm_matprod
+
+
+def _chromatic(beams) -> bool:
+    return any(hasattr(b, "at_frequency") for b in beams)
+
+
+def _beams_at(beams, freq: float) -> list:
+    """Beams at one frequency: beamfits beams (``BeamFits``) are interpolated to
+    ``freq`` and re-gridded (core/beams.py:82-93), grid / analytic beams pass."""
+    return [b.to_grid_beam(freq) if hasattr(b, "at_frequency") else b for b in beams]
 
 logger = logging.getLogger(__name__)
 
@@ -86,7 +98,7 @@ def simulate(
     source_buffer: float = 1.0,
     memory_buffer: float = 0.9,
     coord_method_params=None,
-    gemm_mode: str = "bf16x6",
+    gemm_mode: str = "fp16x3",
     k_chunk: int | None = None,
     device=None,
 ):
@@ -107,13 +119,13 @@ def simulate(
                                     precision, source_buffer=source_buffer, memory_buffer=memory_buffer)
     spec = JobSpec(
         antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=I_sky[:, None], freqs=np.array([float(freq)]),
-        lsts=lsts, latitude=latitude_of(telescope_loc), beams=list(beam_list), beam_idx=beam_idx, polarized=polarized,
+        lsts=lsts, latitude=latitude_of(telescope_loc), beams=_beams_at(beam_list, freq), beam_idx=beam_idx,
+        polarized=polarized,
         antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
         k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks, **rot_kw,
     )
     eng = VisEngine(spec, device=dev)
-    vis = eng.run()[0]
-    out = vis.cpu().numpy()
+    out = eng.run_to_host()[0]
     return out if polarized else out[:, :, 0, 0]
 
 
@@ -137,7 +149,7 @@ def simulate_vis(
     coord_method: str = "CoordinateRotationLST",
     coord_method_params=None,
     matprod_method: str = "MatMul",
-    gemm_mode: str = "bf16x6",
+    gemm_mode: str = "fp16x3",
     k_chunk: int | None = None,
     min_chunks: int = 1,
     device=None,
@@ -159,12 +171,17 @@ def simulate_vis(
     antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
     if not 0 < source_buffer <= 1:
         raise ValueError("source_buffer must satisfy 0 < source_buffer <= 1")
-    spec = JobSpec(
-        antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=fluxes, freqs=freqs, lsts=lsts_of(times),
-        latitude=latitude_of(telescope_loc), beams=list(beams), beam_idx=beam_idx, polarized=polarized,
-        antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
-        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=max(1, int(min_chunks)), **rot_kw,
+    common = dict(
+        antpos=antpos, eci=point_source_crd_eq(ra, dec), lsts=lsts_of(times), latitude=latitude_of(telescope_loc),
+        beam_idx=beam_idx, polarized=polarized, antpairs=antpairs, precision=precision, gemm_mode=gemm_mode,
+        matprod=_norm_matprod(matprod_method), k_chunk=k_chunk, source_buffer=source_buffer,
+        nchunks=max(1, int(min_chunks)), **rot_kw,
     )
-    eng = VisEngine(spec, device=device)
-    vis = eng.run().cpu().numpy()
+    if _chromatic(beams):
+        # frequency-dependent beams: one job per frequency (wrapper.py:180-199)
+        parts = [VisEngine(JobSpec(fluxes=fluxes[:, i : i + 1], freqs=freqs[i : i + 1], beams=_beams_at(beams, f),
+                                   **common), device=device).run_to_host() for i, f in enumerate(freqs)]
+        vis = np.concatenate(parts, axis=0)
+    else:
+        vis = VisEngine(JobSpec(fluxes=fluxes, freqs=freqs, beams=list(beams), **common), device=device).run_to_host()
     return vis if polarized else vis[..., 0, 0]

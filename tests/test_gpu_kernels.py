@@ -212,6 +212,26 @@ def test_matmul_random_vs_oracle(device, mode, tol, nant, nfeed, K, k_chunk):
     assert err <= tol, f"{mode}: cosine error {err:.3e} > {tol}"
 
 
+@pytest.mark.parametrize("mode", ["fp16x3", "bf16x6"])
+def test_matmul_row_dynamic_range(device, mode):
+    """Rows whose magnitude is 1 .. 1e-4 of the panel maximum.  fp16x3 scales the
+    whole panel by one power of two, so a row keeps its ~22-bit split while its
+    largest element stays above ~1e-5 of the maximum; the normalised error
+    (by each row's own autocorrelation) stays <= 1e-6."""
+    rng = np.random.default_rng(77)
+    nant, K = 40, 6000
+    z = rng.normal(size=(nant, K)) + 1j * rng.normal(size=(nant, K))
+    z *= (10.0 ** -rng.integers(0, 5, nant))[:, None]
+    mp = mv.B200MatMul(nchunks=1, nfeed=1, nant=nant, antpairs=None, precision=2, gemm_mode=mode, k_chunk=1024)
+    mp.setup()
+    out = torch.zeros((mp.npairs, 1, 1), dtype=torch.complex128, device=DEV)
+    mp(z, 0)
+    mp.sum_chunks(out)
+    ref = orc.matmul_vis(z.astype(np.complex64).astype(np.complex128), nant, 1)
+    err = _cos_err(out.cpu().numpy(), ref, nant, 1)
+    assert err <= 1e-6, f"{mode}: cosine error {err:.3e}"
+
+
 def test_matmul_sparse_pairs_vs_reference(device):
     g = golden("matprod")
     z, pairs = g["random_z"], g["random_pairs"]

@@ -216,3 +216,70 @@ def test_redundant_pairs_through_products(device, matprod):
     full = _oracle_job(dict(cfg, antpairs=None))
     scale = np.abs(full).max()
     np.testing.assert_allclose(vis, ref, rtol=0, atol=1e-6 * scale)
+
+
+def test_run_to_host_matches_device_result(device):
+    """The streamed device -> host path returns exactly the device visibilities."""
+    cfg = wl.config1()
+    eng = _engine(cfg, precision=1)
+    dev_vis = eng.run().cpu().numpy()
+    host = eng.run_to_host()
+    np.testing.assert_array_equal(host, dev_vis)
+    out = np.zeros_like(dev_vis)
+    assert eng.run_to_host(out) is out
+    np.testing.assert_array_equal(out, dev_vis)
+    with pytest.raises(ValueError):
+        eng.run_to_host(np.zeros(dev_vis.shape, dtype=np.complex128))
+
+
+def test_beamfits_beam_through_simulate_vis(device, tmp_path):
+    """A beamfits E-field beam (written and read back) interpolated to two
+    frequencies inside its range, against the oracle driven with the same
+    re-gridded grids."""
+    from matvis_b200.beamfits import BeamFits, read_beamfits, write_beamfits
+
+    rng = np.random.default_rng(12)
+    naz, nza = 180, 46
+    az = np.deg2rad(np.arange(naz) * (359.0 / (naz - 1)))
+    za = np.deg2rad(np.linspace(0, 90, nza))
+    A, Z = np.meshgrid(az, za)
+    data = np.zeros((2, 2, 2, nza, naz), dtype=complex)
+    for i in range(2):
+        g = 1.0 + 0.05 * i
+        data[0, 0, i], data[1, 0, i] = g * np.cos(Z) * np.cos(A), -g * np.sin(A)
+        data[0, 1, i], data[1, 1, i] = g * np.cos(Z) * np.sin(A), g * np.cos(A)
+    path = tmp_path / "beam.fits"
+    write_beamfits(path, BeamFits("efield", data, az, za, np.array([100e6, 110e6]), ["x", "y"], [], "linear"))
+    beam = read_beamfits(path)
+    cfg = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=3000, nfreq=2, ntimes=2, nant=12, seed=5)
+    freqs = np.array([102e6, 107.5e6])
+    fluxes = cfg["fluxes"][:, :2]
+    ants = {i: tuple(p) for i, p in enumerate(cfg["antpos"])}
+    vis = mv.simulate_vis(ants, fluxes, cfg["ra"], cfg["dec"], freqs, cfg["lsts"], [beam], cfg["latitude"],
+                          polarized=True, precision=2)
+    ref = []
+    for i, f in enumerate(freqs):
+        g = beam.to_grid_beam(f)
+        ob = [orc.GridBeam(data=g.data.astype(np.complex128), az=g.az, za=g.za)]
+        ref.append(orc.simulate_vis(ants=ants, fluxes=fluxes[:, i : i + 1], ra=cfg["ra"], dec=cfg["dec"],
+                                    freqs=freqs[i : i + 1], lsts=cfg["lsts"], latitude=cfg["latitude"], beams=ob,
+                                    polarized=True)[0])
+    ref = np.asarray(ref)
+    assert vis.shape == ref.shape
+    assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6
+
+
+def test_one_beam_per_antenna(device):
+    """nbeam == nant (beam_idx None -> beam a for antenna a, core/beams.py:64-68)
+    with 10 polarised beams: nbeam * F * X = 40 reads the beams from L2 instead
+    of staging them in shared memory."""
+    cfg = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=2500, nfreq=1, ntimes=2, nant=10, seed=9)
+    rng = np.random.default_rng(4)
+    base = cfg["beams"][0]
+    cfg["beams"] = [mv.GridBeam(data=(base.data * (1 + 0.05 * rng.normal(size=base.data.shape))).astype(np.complex64),
+                                az=base.az, za=base.za) for _ in range(10)]
+    cfg["beam_idx"] = None
+    ref = _oracle_job(cfg)
+    for mode in ("fp16x3", "bf16x6"):
+        vis = _engine(cfg, precision=2, gemm_mode=mode).run().cpu().numpy()
+        assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6, mode
