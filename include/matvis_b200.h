@@ -201,7 +201,8 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
  * (cpu/matprod.py:11-32); computes only the upper-triangle tiles. */
 int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
              int k_chunk, int drain_ksteps, void *ws, size_t ws_bytes, int32_t *status, void *stream);
-/* Reduces the FP32 partial tiles in FP64 and writes the visibilities in the
+/* Sums the FP32 partial tiles over k-slices in float-float (TwoSum, about
+ * 2^-44 relative), rounds to FP64 and writes the visibilities in the
  * reference layout out[pair, p, q] = V[ant_i*F + q, ant_j*F + p]
  * (cpu/matprod.py:21-30): all nant^2 pairs (pairs = NULL, i slow) or the
  * npairs listed in pairs (int32 [npairs][2]).  out: complex64 (out_c128 = 0)
@@ -223,6 +224,39 @@ size_t mvb_vecdot_ws_bytes(int64_t npairs, int nfeed, int64_t Kcap, int k_chunk)
 int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul, int nfeed,
                const int32_t *pairs, int64_t npairs, int k_chunk, void *ws, size_t ws_bytes, void *out, int out_c128,
                int accumulate, void *stream);
+
+/* ---- Polarised sky ------------------------------------------------------- */
+/* Frame rotation of the source coherency, per above-horizon source slot s < n
+ * (n = *n_dev, or cap): rot[2 s] = cos X, rot[2 s + 1] = sin X of the 2 x 2
+ * rotation [[cos X, sin X], [-sin X, cos X]] that carries the coherency from
+ * the (ra, dec) basis to the (alt, az) basis.  radec: (2, N) float64 (ra row,
+ * dec row, radians); kept: original source index per slot (mvb_horizon_compact's
+ * idx_out); crd: (3, ld) topocentric (E, N, U) of the slots; r_avg: host 3 x 3
+ * row-major rigid ICRS -> alt/az-cartesian rotation of this time (x north,
+ * y east, z up).  Replaces calc_coherency_rotation (coordinates.py:288-330) with
+ * the astropy-derived average rotation supplied by the caller; where the
+ * rotated and the alt/az unit vectors coincide exactly the perturbation is the
+ * identity (the reference's vecs2rot divides 0 by 0 there). */
+int mvb_coherency_rotation(const double *radec, int64_t N, const int32_t *kept, const double *crd, int64_t ld,
+                           const int32_t *n_dev, int64_t cap, const double *r_avg, double *rot, void *stream);
+/* C' = R^T C R for the slots (CoordinateRotation._rotate_frame_coherency,
+ * core/coords.py:152-175, and the flux gather of select_chunk, :128-147):
+ * coh (N, nf, 2, 2) complex128 -> out (cap, nf, 2, 2) complex128, slots >= n
+ * zeroed. */
+int mvb_rotate_coherency(const double *rot, const int32_t *kept, const int32_t *n_dev, const void *coh, int64_t N,
+                         int nf, void *out, int64_t cap, void *stream);
+/* mvb_tau_z for a polarised sky (F = X = 2): the source carries its coherency
+ * coh[sidx[s]] = (C00, C11, Re C01, Im C01) float32 (16-byte aligned, one
+ * frequency) and rotation rot[s] (from mvb_coherency_rotation); with
+ * C' = R^T C R = L L^H, Z[a*2+f, s*2+y] = exptau(a, s) sum_x beam[bidx[a], f, x, s]
+ * L[x, y], so that the Hermitian product gives V_ij = exptau_j conj(exptau_i)
+ * E_j C' E_i^H, the beam's axis x being the coherency's index.  An unpolarised
+ * source (C = I/2 x identity) gives the Z of mvb_tau_z.  No counterpart runs
+ * in the reference: its ZMatrixCalc takes a scalar flux only (core/getz.py:80). */
+int mvb_tau_z_pol(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
+                  int64_t nsrc, const float *coh, const int32_t *sidx, const double *rot, const void *beam,
+                  int64_t beam_ld, int nbeam, const int32_t *beam_idx, int mode, float zscale, void *z, int64_t Mpad,
+                  int64_t Kcap, void *stream);
 
 /* ---- Redundant-baseline pair selection (host memory, no device work) ------- */
 /* bls: (nant, nant, 2) float64 baselines, bls[i, j] = pos[j, :2] - pos[i, :2].

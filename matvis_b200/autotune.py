@@ -8,8 +8,10 @@ accumulation error below 1e-6 (each 32-byte k-step is summed in a fresh TMEM
 block and slices are reduced in FP64), so the choice is speed only.
 
 ``tune_k_chunk`` times each candidate on the job's own Z panel (a few launches,
-CUDA events on a side stream) and caches the winner per (mode, Mpad, K bucket)
-for the life of the process.
+CUDA events on a side stream) -- the product together with its reduction when
+the caller passes ``run``, since shorter slices also mean more partial tiles to
+reduce -- and caches the winner per (mode, Mpad, K bucket) for the life of the
+process.
 """
 
 from __future__ import annotations
@@ -29,15 +31,20 @@ def _bucket(k: int) -> int:
     return b
 
 
-def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidates=CANDIDATES) -> int:
-    """Fastest k_chunk for this panel shape (panel.n_dev / n_host give the valid K)."""
+def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidates=CANDIDATES, run=None) -> int:
+    """Fastest k_chunk for this panel shape (panel.n_dev / n_host give the valid K).
+
+    ``run(k_chunk, stream)``, if given, enqueues everything that depends on the
+    k-slice (product and reduction); otherwise the product alone is timed."""
     kvalid = panel.n_host * panel.nax if panel.n_dev is None else int(panel.n_dev.item()) * panel.nax
     key = (mode, panel.Mpad, _bucket(max(kvalid, 1)), torch.cuda.current_device())
     if key in _cache:
         return _cache[key]
     cands = [c for c in candidates if c <= max(kvalid, candidates[0])] or [candidates[0]]
-    nbytes = max(_lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, c) for c in cands)
-    ws = torch.empty(nbytes, dtype=torch.uint8, device=panel.data.device)
+    ws = None
+    if run is None:
+        nbytes = max(_lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, c) for c in cands)
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=panel.data.device)
     s = torch.cuda.Stream(device=panel.data.device)
     s.wait_stream(torch.cuda.current_stream())
     best, best_ms = cands[0], float("inf")
@@ -47,6 +54,9 @@ def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidat
             for r in range(reps + 1):
                 if r == 1:
                     e0.record(s)
+                if run is not None:
+                    run(c, s)
+                    continue
                 _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), mode, panel.Mpad, panel.Kcap, _lib.ptr(panel.n_dev),
                                              panel.n_host, panel.nax, c, 0, _lib.ptr(ws), ws.numel(), _lib.ptr(status),
                                              _lib.stream_handle(s)))

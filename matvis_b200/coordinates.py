@@ -103,6 +103,10 @@ class SkyCoords:
         return len(self.ra)
 
 
+#: ENU (east, north, up) -> the alt/az cartesian frame (x north, y east, z up)
+#: that coordinates.point_source_crd_eq(az, alt) uses in the reference
+ENU_TO_ALTAZ = np.array([[0.0, 1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+
 ASTROM_KEYS = ("eh", "em", "v", "bm1", "bpn", "eral", "xpl", "ypl", "sphi", "cphi")
 
 

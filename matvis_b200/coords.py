@@ -24,6 +24,7 @@ import torch
 from . import _lib
 from ._lib import check, ptr, stream_handle
 from .coordinates import (
+    ENU_TO_ALTAZ,
     atioq_matrix,
     eci_to_enu_matrix,
     latitude_of,
@@ -60,9 +61,11 @@ class CoordinateRotation(ABC):
         self.gpu = True
         self.precision = precision
         flux = np.asarray(flux)
-        if flux.ndim != 1:
-            raise ValueError("flux must have shape (NSRCS,): polarised skies are not supported")
-        self.flux_host = flux.astype(np.float64)
+        # core/coords.py:64: a (NSRCS, NFREQS, 2, 2) coherency is a polarised sky
+        self._polarized = flux.ndim == 4
+        if flux.ndim != 1 and not (self._polarized and flux.shape[2:] == (2, 2)):
+            raise ValueError("flux must have shape (NSRCS,) or, for a polarised sky, (NSRCS, NFREQS, 2, 2)")
+        self.flux_host = flux.astype(np.complex128 if self._polarized else np.float64)
         self.nsrc = len(flux)
         self.times = lsts_of(times)
         self.telescope_loc = telescope_loc
@@ -85,26 +88,48 @@ class CoordinateRotation(ABC):
         self.flux = torch.as_tensor(self.flux_host, device=dev)
         self.all_coords_topo = torch.zeros((3, self.nsrc), dtype=torch.float64, device=dev)
         self.coords_above_horizon = torch.zeros((3, self.nsrc_alloc), dtype=torch.float64, device=dev)
-        self.flux_above_horizon = torch.zeros((self.nsrc_alloc,), dtype=torch.float64, device=dev)
+        self.flux_above_horizon = torch.zeros((self.nsrc_alloc,) + tuple(self.flux_host.shape[1:]),
+                                              dtype=self.flux.dtype, device=dev)
+        if self._polarized:
+            self.radec = torch.as_tensor(np.stack([self._ra, self._dec]), dtype=torch.float64, device=dev)
+            self.frame_rotation = torch.zeros((self.nsrc_alloc, 2), dtype=torch.float64, device=dev)
         self.kept_index = torch.zeros((max(self.nsrc_alloc, 1),), dtype=torch.int32, device=dev)
         self.n_above = torch.zeros(1, dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         nbytes = _lib.lib.mvb_horizon_ws_bytes(self.chunk_size)
         self._ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
 
-    def enqueue_select(self, chunk: int, stream=None):
-        """Enqueue the selection of one chunk; the count stays on the device (``n_above``)."""
+    def enqueue_select(self, chunk: int, stream=None, t: int = 0):
+        """Enqueue the selection of one chunk; the count stays on the device (``n_above``).
+
+        For a polarised sky the gathered coherency is also rotated from the
+        (ra, dec) frame to the (alt, az) frame of time ``t`` (core/coords.py:128-147)."""
         c0 = chunk * self.chunk_size
         c1 = min((chunk + 1) * self.chunk_size, self.nsrc)
         c1 = max(c0, c1)
+        sh = stream_handle(stream)
+        scalar = not self._polarized
         check(
             _lib.lib.mvb_horizon_compact(
-                ptr(self.all_coords_topo), self.nsrc, min(c0, self.nsrc), min(c1, self.nsrc), ptr(self.flux),
-                ptr(self.coords_above_horizon), ptr(self.kept_index), ptr(self.flux_above_horizon),
-                ptr(self.n_above), self.nsrc_alloc, ptr(self.status), ptr(self._ws), self._ws.numel(),
-                stream_handle(stream),
+                ptr(self.all_coords_topo), self.nsrc, min(c0, self.nsrc), min(c1, self.nsrc),
+                ptr(self.flux) if scalar else None, ptr(self.coords_above_horizon), ptr(self.kept_index),
+                ptr(self.flux_above_horizon) if scalar else None, ptr(self.n_above), self.nsrc_alloc,
+                ptr(self.status), ptr(self._ws), self._ws.numel(), sh,
             )
         )
+        if self._polarized:
+            r_avg = np.ascontiguousarray(ENU_TO_ALTAZ @ self.rigid_rotation(t))
+            check(_lib.lib.mvb_coherency_rotation(
+                ptr(self.radec), self.nsrc, ptr(self.kept_index), ptr(self.coords_above_horizon), self.nsrc_alloc,
+                ptr(self.n_above), self.nsrc_alloc, r_avg.ctypes.data_as(_lib.c_void_p), ptr(self.frame_rotation),
+                sh))
+            check(_lib.lib.mvb_rotate_coherency(
+                ptr(self.frame_rotation), ptr(self.kept_index), ptr(self.n_above), ptr(self.flux), self.nsrc,
+                self.flux_host.shape[1], ptr(self.flux_above_horizon), self.nsrc_alloc, sh))
+
+    def rigid_rotation(self, t: int) -> np.ndarray:
+        """The rigid ICRS -> ENU rotation of time t (the frame of the coherency rotation)."""
+        raise NotImplementedError
 
     def select_chunk(self, chunk: int, t: int):
         """Above-horizon sources of one chunk at time t; core/coords.py:99-150.
@@ -113,7 +138,7 @@ class CoordinateRotation(ABC):
         read back to the host (one synchronisation, as in the reference).
         """
         self.status.zero_()
-        self.enqueue_select(chunk)
+        self.enqueue_select(chunk, t=t)
         n = int(self.n_above.item())
         if int(self.status.item()) & _lib.MVB_DEV_OVERFLOW:
             raise ValueError(
@@ -136,6 +161,9 @@ class CoordinateRotationLST(CoordinateRotation):
 
     def rotation_matrix(self, t: int) -> np.ndarray:
         return np.ascontiguousarray(eci_to_enu_matrix(self.times[t], self.latitude), dtype=np.float64)
+
+    def rigid_rotation(self, t: int) -> np.ndarray:
+        return self.rotation_matrix(t)
 
     def enqueue_rotate(self, t: int, stream=None):
         R = self.rotation_matrix(t)
@@ -186,6 +214,10 @@ class CoordinateRotationERFA(CoordinateRotation):
         R = np.ascontiguousarray(atioq_matrix(self.astrom[t]))
         check(_lib.lib.mvb_rotate(ptr(self._bcrs), self.nsrc, R.ctypes.data_as(_lib.c_void_p),
                                   ptr(self.all_coords_topo), sh))
+
+    def rigid_rotation(self, t: int) -> np.ndarray:
+        # BPN then CIRS -> ENU; light deflection and aberration enter per source
+        return atioq_matrix(self.astrom[t]) @ np.asarray(self.astrom[t]["bpn"], dtype=np.float64).reshape(3, 3)
 
     def rotate(self, t: int):
         self.enqueue_rotate(t)

@@ -23,13 +23,14 @@
 // only the final hi x hi UMMAs round at full magnitude, and the block is drained
 // by the epilogue warps into FP32 registers with round-to-nearest adds.  One
 // k-slice (k_chunk columns) of register sums is one partial tile; slices are
-// summed in FP64 by herk_reduce_*.
+// summed in float-float (TwoSum, ~2^-44) and rounded to FP64 by herk_reduce_*.
 //
 // Schedule.  Work unit u = (k-slice s, tile t), t fastest so the CTAs that run
 // together read the same Z columns (L2 reuse).  Persistent CTAs (one per SM,
-// 192 KB of shared memory) loop over units.  Warp roles (320 threads):
-//   warp 0 lane 0 : TMA producer, one 3-D box per operand per stage (all 2P
-//                   split/component planes of 128 rows x 32 bytes, SWIZZLE_32B);
+// 192 KB of shared memory) loop over units.  Warp roles (576 threads):
+//   warp 0 lane 0 : TMA producer, one 4-D box per operand per stage (all 2P
+//                   split/component planes of 128 rows x 32 bytes, one k-block of
+//                   the k-blocked panel, SWIZZLE_32B);
 //   warp 1        : TMEM owner (512 columns = two k-step blocks); lane 0 issues
 //                   the UMMAs and tcgen05.commit's the stage / block barriers;
 //   warps 2..17   : epilogue; warp w drains TMEM lane quadrant (w % 4), column
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 // FP64 reduction of the partial tiles into the reference output layout
 // out[pair, p, q] = V[ant_i * F + q, ant_j * F + p].
 // ---------------------------------------------------------------------------
-constexpr int kRedRows = 32, kRedCols = 32;
+constexpr int kRedGroups = 16;  // 8-column groups per 128-column tile
 
 __device__ __forceinline__ int tile_index(int I, int J, int T) { return I * T - (I * (I - 1)) / 2 + (J - I); }
 
@@ -370,60 +371,86 @@ __device__ __forceinline__ void store_out(void *out, int64_t idx, double re, dou
   }
 }
 
-// One CTA (256 threads) per 32 x 32 sub-block of an upper tile.
-template <typename OT>
+// Float-float accumulator: Knuth's TwoSum keeps the exact rounding error of each
+// FP32 addition in a second FP32 word (about 2^-44 relative), on the FP32 pipe;
+// the per-element float -> double conversions it replaces ran on the
+// conversion unit and bounded the reduction's rate.
+struct FF {
+  float hi = 0.f, lo = 0.f;
+  __device__ __forceinline__ void add(float v) {
+    const float s = __fadd_rn(hi, v);
+    const float bb = __fsub_rn(s, hi);
+    const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(v, bb));
+    hi = s;
+    lo = __fadd_rn(lo, err);
+  }
+  __device__ __forceinline__ double value() const { return (double)hi + (double)lo; }
+};
+
+// One CTA (256 threads) per 8 columns of an upper tile: thread (r, h) sums rows
+// r of columns c0 + 4h .. c0 + 4h + 3 (real and imaginary) over the k-slices,
+// so each slice contributes two contiguous 4 KB runs per CTA.  F is a template
+// parameter (no runtime integer division in the index arithmetic).
+template <typename OT, int F>
 __global__ void __launch_bounds__(256)
     herk_reduce_all_kernel(const float *__restrict__ part, int T, int n_tiles, const int32_t *__restrict__ n_dev,
-                           int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, int A, int F,
+                           int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, int A,
                            void *__restrict__ out, double vscale, int accumulate) {
-  __shared__ double sre[kRedRows][kRedCols + 1], sim[kRedRows][kRedCols + 1];
-  const int t = blockIdx.x / 16, sub = blockIdx.x % 16;
+  const int t = blockIdx.x / kRedGroups, g = blockIdx.x % kRedGroups;
   int I, J;
   decode_tile(t, T, I, J);
-  const int r0 = (sub / 4) * kRedRows, c0 = (sub % 4) * kRedCols;
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
   int nsplit;
   int64_t kc;
   plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
   const int M = A * F;
-  const int mbase = I * 128 + r0, nbase = J * 128 + c0;
-  if (mbase >= M || nbase >= M) return;
-
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double are[4] = {0, 0, 0, 0}, aim[4] = {0, 0, 0, 0};
-  for (int s = 0; s < nsplit; ++s) {
-    const float *p = part + ((size_t)s * n_tiles + t) * (256 * 128);
+  const int r = threadIdx.x & 127, h = threadIdx.x >> 7;
+  const int c0 = g * 8 + h * 4;
+  const int m = I * 128 + r;
+  if (J * 128 + c0 >= M || I * 128 >= M) return;  // columns (or the whole tile) past M: nothing to write
+  FF are[4], aim[4];
+  const size_t sstride = (size_t)n_tiles * (256 * 128);
+  const float *p0 = part + (size_t)t * (256 * 128) + r;
+  int s = 0;
+  // four slices per step: 32 independent loads in flight per thread, sums in slice order
+  for (; s + 4 <= nsplit; s += 4) {
+    float vr[4][4], vi[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        vr[u][j] = __ldg(p0 + (s + u) * sstride + (c0 + j) * 128);
+        vi[u][j] = __ldg(p0 + (s + u) * sstride + (128 + c0 + j) * 128);
+      }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        are[j].add(vr[u][j]);
+        aim[j].add(vi[u][j]);
+      }
+  }
+  for (; s < nsplit; ++s) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int c = c0 + w * 4 + j;
-      are[j] += (double)p[c * 128 + r0 + lane];
-      aim[j] += (double)p[(128 + c) * 128 + r0 + lane];
+      are[j].add(__ldg(p0 + s * sstride + (c0 + j) * 128));
+      aim[j].add(__ldg(p0 + s * sstride + (128 + c0 + j) * 128));
     }
   }
+  if (m >= M) return;
+  const int64_t AF2 = (int64_t)A * F * F;
+  const int i = m / F, q = m % F;  // F is 1 or 2: shifts and masks
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    sre[lane][w * 4 + j] = are[j] * vscale;
-    sim[lane][w * 4 + j] = aim[j] * vscale;
-  }
-  __syncthreads();
-
-  const int64_t AF2 = (int64_t)A * F * F;
-  // direct: rows m -> (i, q), columns n -> (j, p); out[(i*A + j)*F*F + p*F + q]
-  for (int e = threadIdx.x; e < kRedRows * kRedCols; e += 256) {
-    const int rl = e % kRedRows, cl = e / kRedRows;  // consecutive threads: consecutive rows
-    const int m = mbase + rl, n = nbase + cl;
-    if (m >= M || n >= M) continue;
-    const int i = m / F, q = m % F, j = n / F, p = n % F;
-    store_out<OT>(out, i * AF2 + (int64_t)j * F * F + p * F + q, sre[rl][cl], sim[rl][cl], accumulate);
-  }
-  if (I == J) return;
-  // mirror: V[n, m] = conj(V[m, n]); rows n -> (i2, q2), columns m -> (j2, p2)
-  for (int e = threadIdx.x; e < kRedRows * kRedCols; e += 256) {
-    const int cl = e % kRedCols, rl = e / kRedCols;  // consecutive threads: consecutive m
-    const int m = mbase + rl, n = nbase + cl;
-    if (m >= M || n >= M) continue;
-    const int i2 = n / F, q2 = n % F, j2 = m / F, p2 = m % F;
-    store_out<OT>(out, i2 * AF2 + (int64_t)j2 * F * F + p2 * F + q2, sre[rl][cl], -sim[rl][cl], accumulate);
+    const int n = J * 128 + c0 + j;
+    if (n >= M) break;
+    const double re = are[j].value() * vscale, im = aim[j].value() * vscale;
+    const int jj = n / F, pp = n % F;
+    // direct: rows m -> (i, q), columns n -> (j, p); out[(i*A + j)*F*F + p*F + q]
+    store_out<OT>(out, i * AF2 + (int64_t)jj * F * F + pp * F + q, re, im, accumulate);
+    // mirror: V[n, m] = conj(V[m, n]) for the off-diagonal tiles (a diagonal tile
+    // holds both triangles and is written directly)
+    if (I != J) store_out<OT>(out, jj * AF2 + (int64_t)i * F * F + q * F + pp, re, -im, accumulate);
   }
 }
 
@@ -452,13 +479,13 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
     }
     const int t = tile_index(m / 128, n / 128, T);
     const int r = m % 128, c = n % 128;
-    double re = 0, im = 0;
+    FF re, im;
     for (int s = 0; s < nsplit; ++s) {
       const float *p0 = part + ((size_t)s * n_tiles + t) * (256 * 128);
-      re += (double)p0[c * 128 + r];
-      im += (double)p0[(128 + c) * 128 + r];
+      re.add(__ldg(p0 + c * 128 + r));
+      im.add(__ldg(p0 + (128 + c) * 128 + r));
     }
-    store_out<OT>(out, e, re * vscale, (conj ? -im : im) * vscale, accumulate);
+    store_out<OT>(out, e, re.value() * vscale, (conj ? -im.value() : im.value()) * vscale, accumulate);
   }
 }
 
@@ -577,13 +604,16 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
   const float *part = static_cast<const float *>(ws);
   cudaStream_t s = as_stream(stream);
   if (!pairs) {
-    const int grid = n_tiles * 16;
-    if (out_c128)
-      herk_reduce_all_kernel<double2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, nant,
-                                                           nfeed, out, vscale, accumulate);
-    else
-      herk_reduce_all_kernel<float2><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, nant,
-                                                          nfeed, out, vscale, accumulate);
+    const int grid = n_tiles * kRedGroups;
+#define MVB_RED(OT, FF_)                                                                                          \
+  herk_reduce_all_kernel<OT, FF_><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, \
+                                                       nant, out, vscale, accumulate)
+    if (out_c128) {
+      if (nfeed == 2) MVB_RED(double2, 2); else MVB_RED(double2, 1);
+    } else {
+      if (nfeed == 2) MVB_RED(float2, 2); else MVB_RED(float2, 1);
+    }
+#undef MVB_RED
   } else {
     if (npairs == 0) return MVB_OK;
     const int64_t total = npairs * nfeed * nfeed;

@@ -24,36 +24,60 @@ namespace mvb {
 
 constexpr double kInvC = 1.0 / 299792458.0;
 
+// Nearest integer (ties to even) of |t| < 2^51 with two FP64 adds: adding and
+// subtracting 1.5 * 2^52 leaves no fraction bits, so the first add rounds t to
+// an integer in the current (round-to-nearest-even) mode -- the same value as
+// rint(t), on the FP64 add pipe instead of the conversion unit.  |t| here is a
+// path difference in wavelengths (< 2^40 for any physical array).
+__device__ __forceinline__ double round_half_even(double t) {
+  const double magic = 6755399441055744.0;  // 1.5 * 2^52
+  return __dsub_rn(__dadd_rn(t, magic), magic);
+}
+
 __device__ __forceinline__ float tf32_rna(float v) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
   return __uint_as_float(r);
 }
 
+// Vector stores of W consecutive 32-bit words (W = 1, 2, 4, 8: 4 to 32 bytes,
+// aligned to min(size, 16) bytes by the callers).
+template <int W>
+__device__ __forceinline__ void store_words(void *p, const uint32_t *w) {
+  static_assert(W == 1 || W == 2 || W == 4 || W == 8, "1, 2, 4 or 8 words");
+  if constexpr (W == 8) {
+    *reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    *(reinterpret_cast<uint4 *>(p) + 1) = make_uint4(w[4], w[5], w[6], w[7]);
+  } else if constexpr (W == 4)
+    *reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+  else if constexpr (W == 2)
+    *reinterpret_cast<uint2 *>(p) = make_uint2(w[0], w[1]);
+  else
+    *reinterpret_cast<uint32_t *>(p) = w[0];
+}
+
 // Writes NV consecutive real values of one component (c = 0 real, 1 imaginary)
 // as the P split terms into planes [2p + c] of a panel row, with vector stores:
-// NV = 8 bf16 (16 bytes) or NV = 4 bf16 (8 bytes), NV float32 (16-byte stores).
+// NV = 4 or 8 values: 8- or 16-byte stores of bf16 / fp16, 16- or 32-byte of float32.
 template <int MODE, int NV>
 __device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t off, int comp, const float *v,
                                           float zscale) {
   if constexpr (MODE == MVB_GEMM_F16_3) {
+    // one paired conversion per two values for each term (cvt.rn.f16x2.f32)
+    uint32_t whi[NV / 2], wlo[NV / 2];
 #pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      uint32_t w[NV / 2];
-#pragma unroll
-      for (int i = 0; i < NV; i += 2) {
-        const float r0 = v[i] * zscale, r1 = v[i + 1] * zscale;
-        const __half h0 = __float2half_rn(r0), h1 = __float2half_rn(r1);
-        const __half q0 = p == 0 ? h0 : __float2half_rn(r0 - __half2float(h0));
-        const __half q1 = p == 0 ? h1 : __float2half_rn(r1 - __half2float(h1));
-        w[i / 2] = (uint32_t)__half_as_ushort(q0) | ((uint32_t)__half_as_ushort(q1) << 16);
-      }
-      __half *pp = static_cast<__half *>(z) + off + (int64_t)(2 * p + comp) * plane_stride;
-      if constexpr (NV == 8)
-        *reinterpret_cast<uint4 *>(pp) = make_uint4(w[0], w[1], w[2], w[3]);
-      else
-        *reinterpret_cast<uint2 *>(pp) = make_uint2(w[0], w[1]);
+    for (int i = 0; i < NV; i += 2) {
+      const float r0 = v[i] * zscale, r1 = v[i + 1] * zscale;
+      const __half2 hi = __floats2half2_rn(r0, r1);
+      const float2 back = __half22float2(hi);
+      const __half2 lo = __floats2half2_rn(r0 - back.x, r1 - back.y);
+      whi[i / 2] = *reinterpret_cast<const uint32_t *>(&hi);
+      wlo[i / 2] = *reinterpret_cast<const uint32_t *>(&lo);
     }
+    __half *p0 = static_cast<__half *>(z) + off + (int64_t)(0 + comp) * plane_stride;
+    __half *p1 = static_cast<__half *>(z) + off + (int64_t)(2 + comp) * plane_stride;
+    store_words<NV / 2>(p0, whi);
+    store_words<NV / 2>(p1, wlo);
   } else if constexpr (MODE == MVB_GEMM_TF32_3) {
     float hi[NV], lo[NV];
 #pragma unroll
@@ -63,11 +87,14 @@ __device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t
     }
     float *p0 = static_cast<float *>(z) + off + (int64_t)(0 + comp) * plane_stride;
     float *p1 = static_cast<float *>(z) + off + (int64_t)(2 + comp) * plane_stride;
+    uint32_t whi[NV], wlo[NV];
 #pragma unroll
-    for (int i = 0; i < NV; i += 4) {
-      *reinterpret_cast<float4 *>(p0 + i) = make_float4(hi[i], hi[i + 1], hi[i + 2], hi[i + 3]);
-      *reinterpret_cast<float4 *>(p1 + i) = make_float4(lo[i], lo[i + 1], lo[i + 2], lo[i + 3]);
+    for (int i = 0; i < NV; ++i) {
+      whi[i] = __float_as_uint(hi[i]);
+      wlo[i] = __float_as_uint(lo[i]);
     }
+    store_words<NV>(p0, whi);
+    store_words<NV>(p1, wlo);
   } else {
     constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
     float r[NV];
@@ -78,17 +105,15 @@ __device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t
       uint32_t w[NV / 2];
 #pragma unroll
       for (int i = 0; i < NV; i += 2) {
-        const __nv_bfloat16 t0 = __float2bfloat16_rn(r[i]);
-        const __nv_bfloat16 t1 = __float2bfloat16_rn(r[i + 1]);
-        r[i] -= __bfloat162float(t0);
-        r[i + 1] -= __bfloat162float(t1);
-        w[i / 2] = (uint32_t)__bfloat16_as_ushort(t0) | ((uint32_t)__bfloat16_as_ushort(t1) << 16);
+        // one paired conversion per two values (cvt.rn.bf16x2.f32); bf16 -> f32 is exact
+        const __nv_bfloat162 t = __floats2bfloat162_rn(r[i], r[i + 1]);
+        const float2 back = __bfloat1622float2(t);
+        r[i] -= back.x;
+        r[i + 1] -= back.y;
+        w[i / 2] = *reinterpret_cast<const uint32_t *>(&t);
       }
       __nv_bfloat16 *pp = static_cast<__nv_bfloat16 *>(z) + off + (int64_t)(2 * p + comp) * plane_stride;
-      if constexpr (NV == 8)
-        *reinterpret_cast<uint4 *>(pp) = make_uint4(w[0], w[1], w[2], w[3]);
-      else
-        *reinterpret_cast<uint2 *>(pp) = make_uint2(w[0], w[1]);
+      store_words<NV / 2>(pp, w);
     }
   }
 }
@@ -151,24 +176,29 @@ struct PanelWriter {
 };
 
 constexpr int kTauZThreads = 64;
-constexpr int kTauZSrc = 4;      // consecutive sources per thread
+constexpr int kTauZSrc = 4;      // consecutive sources per thread (16-byte stores per plane at X = 2)
 constexpr int kTauZAnts = 32;    // antennas per CTA (the CTA's beam block is read once per 32 antennas)
 constexpr int kTauZMaxBFX = 16;  // beams staged in shared memory up to nbeam * F * X = 16, else read from L2
 constexpr int kTauZBlockSrc = kTauZThreads * kTauZSrc;
 
-// grid.x: blocks of kTauZBlockSrc sources, grid.y: antenna blocks.  Dynamic
-// shared memory: the CTA's beam values, [q][j][thread] (thread fastest, so the
-// per-antenna reads are conflict-free), q = (beam * F + f) * X + x.
+// grid.x: blocks of kTauZBlockSrc sources, grid.y: antenna blocks (kTauZAnts).
 // EXT = 0: phase from antpos . crd (fused tau); EXT = 1 / 2: phase factor read
 // from a caller exptau (A, e_ld) in complex64 / complex128, multiplied by sflux.
-template <int MODE, int X, int EXT = 0, bool STAGED = true>
+// POL (EXT = 0, X = 2): polarised sky.  Instead of sqrt(0.5 I) the source
+// carries its coherency C (coh[sidx[s]] = C00, C11, Re C01, Im C01 at this
+// frequency) and frame rotation R (rot[s] = cos X, sin X); with C' = R^T C R =
+// L L^H (lower-triangular L), Z[a, f, (s, y)] = exptau(a, s) sum_x
+// beam[f, x, s] L[x, y, s], so that Z Z^H gives exptau_j conj(exptau_i)
+// E_j C' E_i^H per source.
+template <int MODE, int X, int EXT = 0, bool STAGED = true, bool POL = false>
 __global__ void __launch_bounds__(kTauZThreads)
     tau_z_kernel(const double *__restrict__ antpos, int A, double f_over_c, const double *__restrict__ crd, int64_t ld,
                  const int32_t *__restrict__ n_dev, int64_t nsrc, const float *__restrict__ sflux,
                  const int32_t *__restrict__ sidx, const float2 *__restrict__ beam, int64_t beam_ld, int nbeam,
                  const int32_t *__restrict__ beam_idx, int F, float zscale, void *__restrict__ z, int64_t Mpad,
-                 int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0) {
-  extern __shared__ float2 bsm[];
+                 int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0,
+                 const float4 *__restrict__ coh = nullptr, const double2 *__restrict__ rot = nullptr) {
+  static_assert(!POL || (X == 2 && EXT == 0), "the polarised sky needs two beam axes and the fused phase");
   const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
   const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
   const int64_t s0 = ((int64_t)blockIdx.x * kTauZThreads + threadIdx.x) * kTauZSrc;
@@ -177,6 +207,7 @@ __global__ void __launch_bounds__(kTauZThreads)
 
   double cx[kTauZSrc], cy[kTauZSrc], cz[kTauZSrc];
   float sf[kTauZSrc];
+  float l00[POL ? kTauZSrc : 1], l10r[POL ? kTauZSrc : 1], l10i[POL ? kTauZSrc : 1], l11[POL ? kTauZSrc : 1];
 #pragma unroll
   for (int j = 0; j < kTauZSrc; ++j) {
     const int64_t s = s0 + j;
@@ -189,79 +220,119 @@ __global__ void __launch_bounds__(kTauZThreads)
         cy[j] = crd[ld + s];
         cz[j] = crd[2 * ld + s];
       }
-      sf[j] = sflux[sidx ? sidx[s] : s];
+      if constexpr (POL) {
+        // C' = R^T C R, then its Cholesky factor (clamped at the PSD boundary)
+        const float4 c = coh[sidx ? sidx[s] : s];
+        const double2 r = rot[s];
+        const double cr = r.x, sr = r.y;
+        const double a = c.x, d = c.y, br = c.z, bi = c.w;
+        const double c00 = cr * cr * a + sr * sr * d - 2.0 * cr * sr * br;
+        const double c11 = sr * sr * a + cr * cr * d + 2.0 * cr * sr * br;
+        // C'_10 = conj(C'_01), C'_01 = cr sr (a - d) + cr^2 b - sr^2 conj(b)
+        const double c10r = cr * sr * (a - d) + (cr * cr - sr * sr) * br;
+        const double c10i = -(cr * cr + sr * sr) * bi;
+        const double L00 = sqrt(fmax(c00, 0.0));
+        const double L10r = L00 > 0.0 ? c10r / L00 : 0.0, L10i = L00 > 0.0 ? c10i / L00 : 0.0;
+        l00[j] = (float)L00;
+        l10r[j] = (float)L10r;
+        l10i[j] = (float)L10i;
+        l11[j] = (float)sqrt(fmax(c11 - L10r * L10r - L10i * L10i, 0.0));
+        sf[j] = 1.f;
+      } else {
+        sf[j] = sflux[sidx ? sidx[s] : s];
+      }
+    } else if constexpr (POL) {
+      l00[j] = l10r[j] = l10i[j] = l11[j] = 0.f;
     }
   }
-  const int nbfx = nbeam * F * X;
+  // STAGED: the CTA's beam values in shared memory, [q][j][thread] (thread
+  // fastest: the per-antenna reads are conflict-free; each thread reads only its
+  // own entries, so no barrier is needed), q = (beam * F + f) * X + x.
+  // Otherwise (many beams) the values are read from L2 per antenna.
+  extern __shared__ float2 bsm[];
   if constexpr (STAGED) {
+    const int nbfx = nbeam * F * X;
     for (int q = 0; q < nbfx; ++q)
 #pragma unroll
       for (int j = 0; j < kTauZSrc; ++j)
         bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x] =
             (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
   }
-  // (each thread reads only its own entries of bsm: no barrier needed)
-
   const int a0 = blockIdx.y * kTauZAnts;
   const int a1 = min(a0 + kTauZAnts, A);
   const int64_t plane = Mpad * Kcap;
-  for (int a = a0; a < a1; ++a) {
-    float er[kTauZSrc], ei[kTauZSrc];
-    double dx = 0, dy = 0, dz = 0;
-    if (EXT == 0) {
-      dx = antpos[3 * a];
-      dy = antpos[3 * a + 1];
-      dz = antpos[3 * a + 2];
-    }
-#pragma unroll
-    for (int j = 0; j < kTauZSrc; ++j) {
-      er[j] = ei[j] = 0.f;
-      if (s0 + j >= n) continue;
-      if (EXT == 1) {
-        const float2 e = static_cast<const float2 *>(ext)[(int64_t)a * e_ld + s0 + j];
-        er[j] = e.x * sf[j];
-        ei[j] = e.y * sf[j];
-      } else if (EXT == 2) {
-        const double2 e = static_cast<const double2 *>(ext)[(int64_t)a * e_ld + s0 + j];
-        er[j] = (float)(e.x * (double)sf[j]);
-        ei[j] = (float)(e.y * (double)sf[j]);
-      } else {
-        const double t = (dx * cx[j] + dy * cy[j] + dz * cz[j]) * f_over_c;
-        const double r = t - rint(t);
-        float sn, cs;
-        sincospif((float)(2.0 * r), &sn, &cs);
-        er[j] = cs * sf[j];
-        ei[j] = sn * sf[j];
+  {
+    for (int a = a0; a < a1; ++a) {
+      const int b = beam_idx ? beam_idx[a] : 0;
+      float er[kTauZSrc], ei[kTauZSrc];
+      double dx = 0, dy = 0, dz = 0;
+      if (EXT == 0) {
+        dx = antpos[3 * a];
+        dy = antpos[3 * a + 1];
+        dz = antpos[3 * a + 2];
       }
-    }
-    const int b = beam_idx ? beam_idx[a] : 0;
-    for (int f = 0; f < F; ++f) {
-      float vr[kTauZSrc * X], vi[kTauZSrc * X];
 #pragma unroll
-      for (int j = 0; j < kTauZSrc; ++j)
-#pragma unroll
-        for (int x = 0; x < X; ++x) {
-          const int q = (b * F + f) * X + x;
-          float2 bv;
-          if constexpr (STAGED)
-            bv = bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x];
-          else
-            bv = (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
-          vr[j * X + x] = er[j] * bv.x - ei[j] * bv.y;
-          vi[j * X + x] = er[j] * bv.y + ei[j] * bv.x;
+      for (int j = 0; j < kTauZSrc; ++j) {
+        er[j] = ei[j] = 0.f;
+        if (s0 + j >= n) continue;
+        if (EXT == 1) {
+          const float2 e = static_cast<const float2 *>(ext)[(int64_t)a * e_ld + s0 + j];
+          er[j] = e.x * sf[j];
+          ei[j] = e.y * sf[j];
+        } else if (EXT == 2) {
+          const double2 e = static_cast<const double2 *>(ext)[(int64_t)a * e_ld + s0 + j];
+          er[j] = (float)(e.x * (double)sf[j]);
+          ei[j] = (float)(e.y * (double)sf[j]);
+        } else {
+          const double t = (dx * cx[j] + dy * cy[j] + dz * cz[j]) * f_over_c;
+          const double r = t - round_half_even(t);
+          float sn, cs;
+          sincospif((float)(2.0 * r), &sn, &cs);
+          er[j] = cs * sf[j];
+          ei[j] = sn * sf[j];
         }
-      if (!write) continue;
-      const int64_t m = (int64_t)a * F + f;
-      if constexpr (MODE == MVB_Z_C64) {
-        float2 *zp = static_cast<float2 *>(z) + m * Kcap + s0 * X;
+      }
 #pragma unroll
-        for (int i = 0; i < kTauZSrc * X; i += 2)
-          *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
-      } else {
-        // kTauZSrc * X consecutive k from a multiple of kTauZSrc * X: inside one k-block
-        const int64_t off = panel_off(m, s0 * X, Mpad, kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2));
-        put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr, zscale);
-        put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi, zscale);
+      for (int f = 0; f < 2; ++f) {
+        if (f >= F) break;
+        float vr[kTauZSrc * X], vi[kTauZSrc * X];
+#pragma unroll
+        for (int j = 0; j < kTauZSrc; ++j)
+#pragma unroll
+          for (int x = 0; x < X; ++x) {
+            const int q = (b * F + f) * X + x;
+            float2 bv;
+            if constexpr (STAGED)
+              bv = bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x];
+            else
+              bv = (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
+            vr[j * X + x] = er[j] * bv.x - ei[j] * bv.y;
+            vi[j * X + x] = er[j] * bv.y + ei[j] * bv.x;
+          }
+        if constexpr (POL) {
+          // (g0, g1) = exptau * beam[f, 0:2]  ->  (g0 L00 + g1 L10, g1 L11)
+#pragma unroll
+          for (int j = 0; j < kTauZSrc; ++j) {
+            const float g0r = vr[2 * j], g0i = vi[2 * j], g1r = vr[2 * j + 1], g1i = vi[2 * j + 1];
+            vr[2 * j] = g0r * l00[j] + g1r * l10r[j] - g1i * l10i[j];
+            vi[2 * j] = g0i * l00[j] + g1r * l10i[j] + g1i * l10r[j];
+            vr[2 * j + 1] = g1r * l11[j];
+            vi[2 * j + 1] = g1i * l11[j];
+          }
+        }
+        if (!write) continue;
+        const int64_t m = (int64_t)a * F + f;
+        if constexpr (MODE == MVB_Z_C64) {
+          float2 *zp = static_cast<float2 *>(z) + m * Kcap + s0 * X;
+#pragma unroll
+          for (int i = 0; i < kTauZSrc * X; i += 2)
+            *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
+        } else {
+          // kTauZSrc * X consecutive k from a multiple of kTauZSrc * X: inside one k-block
+          const int64_t off = panel_off(m, s0 * X, Mpad, kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2));
+          put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr, zscale);
+          put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi, zscale);
+        }
       }
     }
   }
@@ -380,6 +451,7 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
       (X != 1 && X != 2) || nbeam <= 0 || beam_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_tau_z: bad arguments");
   const bool staged = nbeam * F * X <= kTauZMaxBFX;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z");
   if (rc) return rc;
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z: Kcap too small for nsrc * nax");
@@ -387,7 +459,6 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
   if (s_max == 0) return MVB_OK;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
   const double foc = freq * kInvC;
-  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
 #define MVB_TAUZ(M, XX)                                                                                        \
@@ -396,7 +467,7 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
     tau_z_kernel<M, XX, 0, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
                                                                 bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
   else                                                                                                         \
-    tau_z_kernel<M, XX, 0, false><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
+    tau_z_kernel<M, XX, 0, false><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
                                                               bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
   } while (0)
 #define MVB_TAUZ2(M) \
@@ -447,6 +518,54 @@ extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, in
   return check_launch("z_pack_kernel");
 }
 
+extern "C" int mvb_tau_z_pol(const double *antpos, int A, double freq, const double *crd, int64_t ld,
+                             const int32_t *n_dev, int64_t nsrc, const float *coh, const int32_t *sidx,
+                             const double *rot, const void *beam, int64_t beam_ld, int nbeam,
+                             const int32_t *beam_idx, int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap,
+                             void *stream) {
+  const int F = 2, X = 2;
+  if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !coh || !rot || (nsrc > 0 && !crd) || nbeam <= 0 ||
+      beam_ld < nsrc)
+    return fail(MVB_ERR_ARG, "mvb_tau_z_pol: bad arguments");
+  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z_pol");
+  if (rc) return rc;
+  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z_pol: Kcap too small for nsrc * nax");
+  if (reinterpret_cast<uintptr_t>(coh) % 16 || reinterpret_cast<uintptr_t>(rot) % 16)
+    return fail(MVB_ERR_ARG, "mvb_tau_z_pol: coh and rot must be 16-byte aligned");
+  const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
+  if (s_max == 0) return MVB_OK;
+  const bool staged = nbeam * F * X <= kTauZMaxBFX;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
+  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  const double foc = freq * kInvC;
+  const float2 *bm = static_cast<const float2 *>(beam);
+  const float4 *c4 = reinterpret_cast<const float4 *>(coh);
+  const double2 *r2 = reinterpret_cast<const double2 *>(rot);
+  cudaStream_t s = as_stream(stream);
+#define MVB_TZP(M)                                                                                                \
+  do {                                                                                                            \
+    if (staged)                                                                                                   \
+      tau_z_kernel<M, 2, 0, true, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,    \
+                                                                        nullptr, sidx, bm, beam_ld, nbeam,        \
+                                                                        beam_idx, F, zscale, z, Mpad, Kcap,       \
+                                                                        nullptr, 0, c4, r2);                      \
+    else                                                                                                          \
+      tau_z_kernel<M, 2, 0, false, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,      \
+                                                                      nullptr, sidx, bm, beam_ld, nbeam,          \
+                                                                      beam_idx, F, zscale, z, Mpad, Kcap,         \
+                                                                      nullptr, 0, c4, r2);                        \
+  } while (0)
+  switch (mode) {
+    case MVB_GEMM_BF16_3: MVB_TZP(MVB_GEMM_BF16_3); break;
+    case MVB_GEMM_BF16_6: MVB_TZP(MVB_GEMM_BF16_6); break;
+    case MVB_GEMM_TF32_3: MVB_TZP(MVB_GEMM_TF32_3); break;
+    case MVB_GEMM_F16_3: MVB_TZP(MVB_GEMM_F16_3); break;
+    default: MVB_TZP(MVB_Z_C64); break;
+  }
+#undef MVB_TZP
+  return check_launch("tau_z_kernel(pol)");
+}
+
 extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, int A, int64_t nsrc, const float *sflux,
                                  const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X,
                                  int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap, void *stream) {
@@ -454,13 +573,13 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
       nbeam <= 0 || beam_ld < nsrc || e_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_z_from_exptau: bad arguments");
   const bool staged = nbeam * F * X <= kTauZMaxBFX;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_z_from_exptau");
   if (rc) return rc;
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_z_from_exptau: Kcap too small");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
-  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
 #define MVB_ZX(M, XX, E)                                                                                       \
@@ -470,7 +589,7 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
                                                                 nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z, \
                                                                 Mpad, Kcap, exptau, e_ld);                    \
   else                                                                                                         \
-    tau_z_kernel<M, XX, E, false><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux,  \
+    tau_z_kernel<M, XX, E, false><<<grid, kTauZThreads, smem, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux,  \
                                                               nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z,  \
                                                               Mpad, Kcap, exptau, e_ld);                    \
   } while (0)

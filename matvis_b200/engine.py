@@ -25,7 +25,14 @@ import torch
 
 from . import _lib
 from .beams import B200BeamInterpolator, GaussianBeam, GridBeam
-from .coordinates import atioq_matrix, bcrs_refresh_plan, eci_to_enu_matrix, pack_astrom, point_source_crd_eq
+from .coordinates import (
+    ENU_TO_ALTAZ,
+    atioq_matrix,
+    bcrs_refresh_plan,
+    eci_to_enu_matrix,
+    pack_astrom,
+    point_source_crd_eq,
+)
 from .getz import ZMatrixCalc
 from .autotune import tune_k_chunk
 from .matprod import B200MatMul, B200VectorDot, choose_k_chunk
@@ -39,7 +46,7 @@ DEFAULT_K_CHUNK = 2048
 class JobSpec:
     antpos: np.ndarray  # (A, 3) metres
     eci: np.ndarray  # (3, N) unit vectors
-    fluxes: np.ndarray  # (N, Nf) Stokes I
+    fluxes: np.ndarray  # (N, Nf) Stokes I, or (N, Nf, 2, 2) coherency (polarised sky)
     freqs: np.ndarray  # (Nf,) Hz
     lsts: np.ndarray  # (Nt,) radians
     latitude: float  # radians
@@ -57,6 +64,8 @@ class JobSpec:
     astrom: list | None = None
     update_bcrs_every: float = 0.0
     time_s: np.ndarray | None = None
+    #: (2, N) ra / dec in radians for the polarised sky's frame rotation (else from eci)
+    radec: np.ndarray | None = None
 
 
 def _norm_matprod(name: str) -> str:
@@ -85,11 +94,30 @@ class VisEngine:
         self.nsrc = self.eci_host.shape[1]
         self.freqs = np.asarray(s.freqs, dtype=np.float64)
         self.lsts = np.asarray(s.lsts, dtype=np.float64)
-        fl = np.asarray(s.fluxes, dtype=np.float64)
-        if fl.shape != (self.nsrc, len(self.freqs)):
-            raise ValueError("The `fluxes` array must have shape (NSRCS, NFREQS).")
-        # sqrt(0.5 I) per frequency (cpu/cpu.py:188), frequency-major, float32
-        self.sflux_host = np.ascontiguousarray(np.sqrt(0.5 * fl).T.astype(np.float32))
+        fl = np.asarray(s.fluxes)
+        self.pol_sky = fl.ndim == 4
+        if fl.shape[:2] != (self.nsrc, len(self.freqs)) or (self.pol_sky and fl.shape[2:] != (2, 2)) or \
+                fl.ndim not in (2, 4):
+            raise ValueError("The `fluxes` array must have shape (NSRCS, NFREQS) or (NSRCS, NFREQS, 2, 2).")
+        if self.pol_sky:
+            if not s.polarized:
+                raise ValueError("a polarised sky (coherency fluxes) needs polarized=True")
+            # per frequency and source: C00, C11, Re C01, Im C01 (float32, 16 bytes)
+            c = np.asarray(fl, dtype=np.complex128)
+            self.coh_host = np.ascontiguousarray(np.stack(
+                [c[..., 0, 0].real, c[..., 1, 1].real, c[..., 0, 1].real, c[..., 0, 1].imag], axis=-1
+            ).transpose(1, 0, 2).astype(np.float32))
+            trace = np.maximum(c[..., 0, 0].real + c[..., 1, 1].real, 0.0)
+            self.sflux_host = np.ascontiguousarray(np.sqrt(0.5 * trace).T.astype(np.float32))
+            if s.radec is not None:
+                self.radec_host = np.ascontiguousarray(np.asarray(s.radec, dtype=np.float64).reshape(2, self.nsrc))
+            else:
+                e = self.eci_host
+                self.radec_host = np.ascontiguousarray(np.stack([np.arctan2(e[1], e[0]), np.arcsin(np.clip(e[2], -1, 1))]))
+        else:
+            fl = fl.astype(np.float64)
+            # sqrt(0.5 I) per frequency (cpu/cpu.py:188), frequency-major, float32
+            self.sflux_host = np.ascontiguousarray(np.sqrt(0.5 * fl).T.astype(np.float32))
         self.method = _norm_matprod(s.matprod)
         self.nchunks = max(1, int(s.nchunks))
         self.chunk_size = int(np.ceil(self.nsrc / self.nchunks)) if self.nsrc else 1
@@ -112,10 +140,19 @@ class VisEngine:
             self.rot = (np.stack([eci_to_enu_matrix(l, s.latitude) for l in self.lsts]) if len(self.lsts)
                         else np.zeros((0, 3, 3)))
             self.bcrs_plan = None
+        if self.pol_sky:
+            # rigid ICRS -> alt/az-cartesian rotation per time for the coherency frame
+            if s.astrom is not None:
+                rigid = [atioq_matrix(a) @ np.asarray(a["bpn"], dtype=np.float64).reshape(3, 3) for a in s.astrom]
+            else:
+                rigid = list(self.rot)
+            self.ravg = [np.ascontiguousarray(ENU_TO_ALTAZ @ r) for r in rigid]
         self.zscale = 1.0
         if self.method == "MatMul" and _lib.GEMM_MODES.get(s.gemm_mode, s.gemm_mode) == _lib.GEMM_F16_3:
-            # |Z| <= max sqrt(0.5 I) * max |beam| (bilinear weights are convex, |exptau| = 1)
-            self.zscale = _lib.f16_scale(float(self.sflux_host.max(initial=0.0)) * beam_bound(s.beams) * (1 + 2**-10))
+            # |Z| <= max sqrt(0.5 I) * max |beam| (bilinear weights are convex, |exptau| = 1); for a
+            # polarised sky |sum_x beam_x L_xy| <= sqrt(2) max|beam| sqrt(trace C) = 2 max|beam| sqrt(I / 2)
+            zmax = float(self.sflux_host.max(initial=0.0)) * beam_bound(s.beams) * (2.0 if self.pol_sky else 1.0)
+            self.zscale = _lib.f16_scale(zmax * (1 + 2**-10))
         self._graph = None
         self._allocated = False
 
@@ -129,6 +166,10 @@ class VisEngine:
         self.sflux = torch.empty((len(self.freqs), N), dtype=torch.float32, device=dev)
         self.topo = torch.zeros((3, N), dtype=torch.float64, device=dev)
         self.bcrs = torch.zeros((3, N), dtype=torch.float64, device=dev) if self.bcrs_plan is not None else None
+        if self.pol_sky:
+            self.coh = torch.empty((len(self.freqs), N, 4), dtype=torch.float32, device=dev)
+            self.radec = torch.empty((2, N), dtype=torch.float64, device=dev)
+            self.rot2 = torch.zeros((self.cap, 2), dtype=torch.float64, device=dev)
         self.crd = torch.zeros((3, self.cap), dtype=torch.float64, device=dev)
         self.kept = torch.zeros((self.cap,), dtype=torch.int32, device=dev)
         self.n_above = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -168,9 +209,15 @@ class VisEngine:
         self.eci.copy_(torch.from_numpy(self.eci_host), non_blocking=False)
         self.antpos.copy_(torch.from_numpy(self.antpos_host))
         self.sflux.copy_(torch.from_numpy(self.sflux_host))
+        if self.pol_sky:
+            self.coh.copy_(torch.from_numpy(self.coh_host))
+            self.radec.copy_(torch.from_numpy(self.radec_host))
 
     def h2d_bytes(self) -> int:
-        return self.eci_host.nbytes + self.antpos_host.nbytes + self.sflux_host.nbytes
+        n = self.eci_host.nbytes + self.antpos_host.nbytes + self.sflux_host.nbytes
+        if self.pol_sky:
+            n += self.coh_host.nbytes + self.radec_host.nbytes
+        return n
 
     # ----------------------------------------------------------------- launch
     def enqueue(self, stream=None):
@@ -204,12 +251,25 @@ class VisEngine:
             self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, self.bmfunc.interpolated_beam,
                                stream=stream, status=self.status)
             beam = self.bmfunc.interpolated_beam
+            if self.pol_sky:
+                chk(L.mvb_coherency_rotation(
+                    _lib.ptr(self.radec), self.nsrc, _lib.ptr(self.kept), _lib.ptr(self.crd), self.cap,
+                    _lib.ptr(self.n_above), self.cap, self.ravg[t].ctypes.data_as(_lib.c_void_p), _lib.ptr(self.rot2),
+                    sh))
             for f in range(len(self.freqs)):
-                chk(L.mvb_tau_z(
-                    _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
-                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f]), _lib.ptr(self.kept), _lib.ptr(beam),
-                    beam.shape[-1], beam.shape[0], _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode,
-                    self.zscale, _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
+                if self.pol_sky:
+                    chk(L.mvb_tau_z_pol(
+                        _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
+                        _lib.ptr(self.n_above), self.cap, _lib.ptr(self.coh[f]), _lib.ptr(self.kept),
+                        _lib.ptr(self.rot2), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
+                        _lib.ptr(self.bmfunc.beam_index_dev), self.zcalc.mode, self.zscale, _lib.ptr(panel.data),
+                        panel.Mpad, panel.Kcap, sh))
+                else:
+                    chk(L.mvb_tau_z(
+                        _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
+                        _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f]), _lib.ptr(self.kept),
+                        _lib.ptr(beam), beam.shape[-1], beam.shape[0], _lib.ptr(self.bmfunc.beam_index_dev), F, X,
+                        self.zcalc.mode, self.zscale, _lib.ptr(panel.data), panel.Mpad, panel.Kcap, sh))
                 panel.n_dev = self.n_above
                 panel.n_host = self.cap
                 panel.scale = self.zscale
@@ -231,7 +291,7 @@ class VisEngine:
 
     def launches_per_run(self) -> int:
         per_f = 3 if self.method == "MatMul" else 2
-        per_chunk = 3 + per_f * len(self.freqs)  # count + scatter + beam, then per frequency
+        per_chunk = 3 + per_f * len(self.freqs) + int(self.pol_sky)  # count + scatter + beam (+ frame), per frequency
         n = len(self.lsts) * (1 + self.nchunks * per_chunk)
         return n + (sum(self.bcrs_plan) if self.bcrs_plan is not None else 0)
 
@@ -314,7 +374,10 @@ class VisEngine:
         torch.cuda.synchronize()
         if self.method == "MatMul" and not self.spec.k_chunk:
             # the panel holds the last slice: time the k-slice candidates on it
-            self.k_chunk = tune_k_chunk(self.zcalc.z, self.matprod.mode, self.status)
+            panel, scratch = self.zcalc.z, torch.empty_like(self.vis[0, 0])
+            self.k_chunk = tune_k_chunk(
+                panel, self.matprod.mode, self.status,
+                run=lambda kc, st: self.matprod.enqueue(panel, scratch, accumulate=False, stream=st, k_chunk=kc))
             self.matprod.workspace(self.zcalc.z, self.k_chunk)
             torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -338,6 +401,7 @@ def job_from_arrays(*, ants, fluxes, ra, dec, freqs, lsts, latitude, beams, **kw
         antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
     else:
         antpos = np.asarray(ants, dtype=np.float64)
+    kw.setdefault("radec", np.stack([np.asarray(ra, dtype=np.float64), np.asarray(dec, dtype=np.float64)]))
     return JobSpec(antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=np.asarray(fluxes), freqs=np.asarray(freqs),
                    lsts=np.asarray(lsts), latitude=float(latitude), beams=list(beams), **kw)
 
@@ -368,8 +432,10 @@ def estimate_device_bytes(spec: JobSpec) -> int:
     else:
         ws = _lib.lib.mvb_vecdot_ws_bytes(npairs, F, kcap, spec.k_chunk or 4096)
     nbeam = len(spec.beams)
+    pol_sky = np.ndim(spec.fluxes) == 4
+    extra = (16 * Nf * N + 16 * N + 16 * cap) if pol_sky else 0  # coherency, ra/dec, frame rotations
     return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + 8 * nbeam * F * X * cap + panel + ws
-               + Nf * Nt * npairs * F * F * csize)
+               + Nf * Nt * npairs * F * F * csize + extra)
 
 
 def beam_bound(beams) -> float:

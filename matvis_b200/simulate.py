@@ -167,12 +167,14 @@ def simulate_vis(
     ra = np.asarray(ra, dtype=np.float64)
     dec = np.asarray(dec, dtype=np.float64)
     freqs = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
-    assert fluxes.shape == (ra.size, freqs.size), "The `fluxes` array must have shape (NSRCS, NFREQS)."
+    assert fluxes.shape[:2] == (ra.size, freqs.size) and fluxes.ndim in (2, 4), \
+        "The `fluxes` array must have shape (NSRCS, NFREQS) or, for a polarised sky, (NSRCS, NFREQS, 2, 2)."
     antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
     if not 0 < source_buffer <= 1:
         raise ValueError("source_buffer must satisfy 0 < source_buffer <= 1")
     common = dict(
-        antpos=antpos, eci=point_source_crd_eq(ra, dec), lsts=lsts_of(times), latitude=latitude_of(telescope_loc),
+        antpos=antpos, eci=point_source_crd_eq(ra, dec), radec=np.stack([ra, dec]), lsts=lsts_of(times),
+        latitude=latitude_of(telescope_loc),
         beam_idx=beam_idx, polarized=polarized, antpairs=antpairs, precision=precision, gemm_mode=gemm_mode,
         matprod=_norm_matprod(matprod_method), k_chunk=k_chunk, source_buffer=source_buffer,
         nchunks=max(1, int(min_chunks)), **rot_kw,

@@ -299,8 +299,14 @@ def simulate(
     astrom=None,
     time_s=None,
     update_bcrs_every=0.0,
+    coherency=None,
 ):
     """One frequency, all times; ``cpu/cpu.py:163-277`` at precision=2.
+
+    ``coherency`` (N, 2, 2) complex (polarised only): a polarised sky.  Each
+    time its frame is rotated to alt/az (``coherency_rotation`` with the time's
+    rigid ICRS -> alt/az rotation) and the visibilities are summed directly as
+    V_ij = exptau_j conj(exptau_i) E_j C' E_i^H.
 
     With ``astrom`` (one apco parameter dict per time) the rotation is the
     ERFA-style apparent place of ``CoordinateRotationERFA`` (cpu/coords.py:186-230),
@@ -337,6 +343,12 @@ def simulate(
             if last is None or time_s is None or time_s[t] - time_s[last] > update_bcrs_every:
                 bcrs, last = erfa_bcrs(eci, astrom[t]), t
             topo = rotate_fixed_order(erfa_atioq_matrix(astrom[t]), bcrs)
+        if coherency is not None:
+            rigid = (eci_to_enu_matrix(lst, latitude) if astrom is None
+                     else erfa_atioq_matrix(astrom[t]) @ np.asarray(astrom[t]["bpn"], dtype=np.float64))
+            vis[t] += _polsky_vis_time(topo, eci, coherency, rigid, antpos, freq, beam_list, beam_idx, nchunks,
+                                       chunk_size, alloc, pairs if antpairs is not None else None, nant, ra, dec)
+            continue
         for c in range(nchunks):
             crd, fl, n, _ = select_chunk(topo, flux, c, chunk_size, alloc)
             if n == 0:
@@ -351,6 +363,32 @@ def simulate(
             else:
                 vis[t] += vectordot_vis(z, nant, nfeed, pairs)
     return vis if polarized else vis[:, :, 0, 0]
+
+
+def _polsky_vis_time(topo, eci, coherency, rigid, antpos, freq, beam_list, beam_idx, nchunks, chunk_size, alloc,
+                     pairs, nant, ra, dec):
+    """One time of the polarised-sky sum (chunks as in cpu/cpu.py:247-272)."""
+    nf = 2
+    out = np.zeros((nant * nant if pairs is None else len(pairs), nf, nf), dtype=np.complex128)
+    r_avg = ENU_TO_ALTAZ @ rigid
+    for c in range(nchunks):
+        c0 = c * chunk_size
+        sel = np.flatnonzero(topo[2, c0 : c0 + chunk_size] > 0) + c0
+        if len(sel) == 0:
+            continue
+        if len(sel) > alloc:
+            raise ValueError("nsrc_alloc too small")
+        crd = topo[:, sel]
+        az, za = enu_to_az_za(crd[0], crd[1], orientation="astropy")
+        rot = coherency_rotation(ra[sel], dec[sel], np.pi / 2 - za, az, r_avg)
+        cp = rotate_coherency(coherency[sel][:, None], rot)[:, 0]
+        beam = beam_response(beam_list, True, crd[0], crd[1])  # (B, F, X, n)
+        ext = exptau(antpos, freq, crd)  # (A, n)
+        y = ext[:, None, None, :] * beam[beam_idx]  # (A, F, X, n)
+        w = np.einsum("apxs,sxy->apys", y, cp)
+        v = np.einsum("jpys,iqys->ijpq", w, np.conj(y))
+        out += v.reshape(nant * nant, nf, nf) if pairs is None else v[pairs[:, 0], pairs[:, 1]]
+    return out
 
 
 def simulate_vis(
@@ -376,7 +414,8 @@ def simulate_vis(
     update_bcrs_every)."""
     antpos = np.array([ants[k] for k in ants.keys()], dtype=np.float64)
     fluxes = np.asarray(fluxes)
-    assert fluxes.shape == (len(ra), len(freqs)), "The `fluxes` array must have shape (NSRCS, NFREQS)."
+    assert fluxes.shape[:2] == (len(ra), len(freqs)), "The `fluxes` array must have shape (NSRCS, NFREQS[, 2, 2])."
+    pol_sky = fluxes.ndim == 4
     eci = point_source_crd_eq(ra, dec)
     out = []
     for i, freq in enumerate(freqs):
@@ -388,7 +427,8 @@ def simulate_vis(
                 latitude=latitude,
                 ra=ra,
                 dec=dec,
-                I_sky=fluxes[:, i],
+                I_sky=np.real(np.trace(fluxes[:, i], axis1=-2, axis2=-1)) if pol_sky else fluxes[:, i],
+                coherency=fluxes[:, i] if pol_sky else None,
                 beam_list=beams,
                 polarized=polarized,
                 beam_idx=beam_idx,
@@ -501,3 +541,67 @@ def erfa_bcrs(eci, astrom, dlim=1e-6):
     p = erfa_ld(eci, astrom["eh"], astrom["em"], dlim)
     p = erfa_ab(p, astrom["v"], astrom["em"], astrom["bm1"])
     return np.asarray(astrom["bpn"], dtype=np.float64) @ p
+
+
+# ---------------------------------------------------------------------------
+# Polarised sky: frame rotation of the source coherency
+# (coordinates.py:288-580, core/coords.py:152-175)
+# ---------------------------------------------------------------------------
+ENU_TO_ALTAZ = np.array([[0.0, 1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+
+
+def _theta_hat(theta, phi):
+    """coordinates.py:537-556."""
+    return np.stack([np.cos(phi) * np.cos(theta), np.sin(phi) * np.cos(theta), -np.sin(theta)])
+
+
+def _phi_hat(theta, phi):
+    """coordinates.py:559-576."""
+    return np.stack([-np.sin(phi), np.cos(phi), np.zeros_like(phi)])
+
+
+def coherency_rotation(ra, dec, alt, az, r_avg):
+    """2x2 (cos X, sin X; -sin X, cos X) per source, shape (2, 2, N):
+    calc_coherency_rotation (coordinates.py:288-330) with the average
+    ICRS -> alt/az rotation ``r_avg`` supplied.  The perturbation rotation
+    carrying r_avg . frame_vec onto the alt/az vector (vecs2rot,
+    coordinates.py:387-452) is the identity where the two vectors coincide
+    exactly (the reference divides 0 by 0 there)."""
+    ra, dec, alt, az = (np.asarray(x, dtype=np.float64) for x in (ra, dec, alt, az))
+    frame = point_source_crd_eq(ra, dec)
+    altaz = point_source_crd_eq(az, alt)
+    r1 = r_avg @ frame
+    axis = np.cross(r1, altaz, axis=0)
+    sin_psi = np.linalg.norm(axis, axis=0)
+    cos_psi = np.sum(r1 * altaz, axis=0)
+    psi = np.arctan2(sin_psi, cos_psi)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        n = np.where(sin_psi > 0, axis / np.where(sin_psi > 0, sin_psi, 1.0), 0.0)
+    zero = np.zeros_like(ra)
+    k = np.array([[zero, -n[2], n[1]], [n[2], zero, -n[0]], [-n[1], n[0], zero]])
+    k2 = np.einsum("abn,bcn->acn", k, k)
+    perturb = np.eye(3)[..., None] + np.sin(psi) * k + (1.0 - np.cos(psi)) * k2
+    exact = np.einsum("abn,bc->acn", perturb, r_avg)
+    th = _theta_hat(np.pi / 2 - dec, ra)
+    ph = _phi_hat(np.pi / 2 - dec, ra)
+    bh = np.einsum("ban,bn->an", exact, _theta_hat(np.pi / 2 - alt, az))
+    cos_x = np.sum(bh * th, axis=0)
+    sin_x = np.sum(bh * ph, axis=0)
+    return np.array([[cos_x, sin_x], [-sin_x, cos_x]])
+
+
+def rotate_coherency(coh, rot):
+    """C' = R^T C R per source and frequency; core/coords.py:170-173.
+    coh (N, Nf, 2, 2), rot (2, 2, N)."""
+    return np.einsum("ban,nfbc,cdn->nfad", rot, coh, rot)
+
+
+def stokes_to_coherency(i, q, u, v):
+    """0.5 [[I + Q, U - iV], [U + iV, I - Q]] with shape (..., 2, 2)."""
+    i, q, u, v = np.broadcast_arrays(*(np.asarray(x, dtype=np.float64) for x in (i, q, u, v)))
+    c = np.empty(i.shape + (2, 2), dtype=np.complex128)
+    c[..., 0, 0] = 0.5 * (i + q)
+    c[..., 1, 1] = 0.5 * (i - q)
+    c[..., 0, 1] = 0.5 * (u - 1j * v)
+    c[..., 1, 0] = 0.5 * (u + 1j * v)
+    return c

@@ -20,6 +20,13 @@ reference functions return:
   driven in the loop order of ``cpu/cpu.py:247-272``;
 * ``erfa.npz``      -- ``CoordinateRotationERFA._ld / _ab / _bpn / _atioq``
   (``cpu/coords.py:89-181``) on seeded unit vectors and astrom parameters;
+* ``coherency.npz`` -- ``calc_coherency_rotation`` (``coordinates.py:288-330``,
+  with ``vecs2rot``, ``axis_angle_rotation_matrix``,
+  ``spherical_basis_vector_rotation_matrix``, ``theta_hat``, ``phi_hat``) and
+  ``CoordinateRotation._rotate_frame_coherency`` (``core/coords.py:152-175``) on
+  seeded sources, for the rigid LST frame and for the ERFA apparent-place frame;
+  the astropy-derived average rotation ``_calc_average_rotation_matrix`` is
+  replaced by the frame's rigid 3x3 (ICRS -> alt/az cartesian, x north, y east);
 * ``redundancies.npz`` -- ``get_redundancies`` (``cli.py:273-290``) on hexagonal,
   jittered, random and co-located antenna layouts.  ``cli.py`` imports click,
   astropy, line_profiler and pyuvdata at module level, so only that function's
@@ -464,6 +471,73 @@ def make_redundancies():
     _save("redundancies.npz", **out)
 
 
+def make_coherency():
+    coords = ref.coordinates
+    rng = np.random.default_rng(51)
+    lat = np.deg2rad(-30.72)
+    nsrc, nfreq = 400, 3
+    ra = rng.uniform(0, 2 * np.pi, nsrc)
+    dec = np.arcsin(rng.uniform(-1, 1, nsrc))
+    eci = np.asarray(coords.point_source_crd_eq(ra, dec))
+    stokes_i = rng.uniform(0.5, 3.0, (nsrc, nfreq))
+    frac = rng.uniform(0, 0.9, (nsrc, nfreq))
+    direction = rng.normal(size=(3, nsrc, nfreq))
+    direction /= np.linalg.norm(direction, axis=0)
+    q, u, v = stokes_i * frac * direction
+    coh = np.empty((nsrc, nfreq, 2, 2), dtype=complex)
+    coh[..., 0, 0] = 0.5 * (stokes_i + q)
+    coh[..., 1, 1] = 0.5 * (stokes_i - q)
+    coh[..., 0, 1] = 0.5 * (u - 1j * v)
+    coh[..., 1, 0] = 0.5 * (u + 1j * v)
+    enu_to_altaz = np.array([[0.0, 1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+    out = {"ra": ra, "dec": dec, "coherency": coh, "lat": lat}
+    saved = coords._calc_average_rotation_matrix
+
+    class _Self:
+        xp = np
+        telescope_loc = None
+
+    try:
+        for case in ("lst", "erfa"):
+            if case == "lst":
+                lst = 1.234
+                rigid = np.asarray(coords.eci_to_enu_matrix(lst, lat))
+                topo = rigid @ eci
+                out["lst_lst"] = lst
+            else:
+                astrom = seeded_astrom(rng, lat)
+                for k, val in astrom.items():
+                    out[f"erfa_{k}"] = np.asarray(val)
+                rot_cls = ref.cpu_coords.CoordinateRotationERFA
+                p = eci.copy()
+                rot_cls._ld(_Self(), p, astrom["eh"], astrom["em"], 1e-6)
+                rot_cls._ab(_Self(), p, astrom["v"], astrom["em"], astrom["bm1"])
+                rot_cls._bpn(_Self(), p, astrom)
+                topo = p.copy()
+                rot_cls._atioq(_Self(), topo, astrom)
+                # rigid part of the apparent place: BPN then the CIRS -> ENU rotation
+                probe = np.eye(3)
+                rot_cls._atioq(_Self(), probe, astrom)
+                rigid = probe @ np.asarray(astrom["bpn"])
+            r_avg = enu_to_altaz @ rigid
+            coords._calc_average_rotation_matrix = lambda time, location, _r=r_avg: _r
+            az, za = coords.enu_to_az_za(topo[0], topo[1], orientation="astropy")
+            above = np.flatnonzero(topo[2] > 0)
+            alt = np.pi / 2 - za[above]
+            rot = coords.calc_coherency_rotation(ra=ra[above], dec=dec[above], alt=alt, az=az[above], time=None,
+                                                 location=None)
+            rotated = ref.core_coords.CoordinateRotation._rotate_frame_coherency(
+                _Self(), coh[above], ra[above], dec[above], alt, az[above], None)
+            out[f"{case}_topo"] = topo
+            out[f"{case}_rigid"] = rigid
+            out[f"{case}_above"] = above
+            out[f"{case}_rot"] = np.asarray(rot)
+            out[f"{case}_rotated"] = np.asarray(rotated)
+    finally:
+        coords._calc_average_rotation_matrix = saved
+    _save("coherency.npz", **out)
+
+
 if __name__ == "__main__":
     make_matprod()
     make_bilinear()
@@ -473,3 +547,4 @@ if __name__ == "__main__":
     make_pipeline()
     make_erfa()
     make_redundancies()
+    make_coherency()

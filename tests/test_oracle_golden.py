@@ -182,3 +182,36 @@ def test_erfa_steps_match_reference():
         np.testing.assert_allclose(orc.erfa_bcrs(g["eci"], a), g[f"t{t}_bcrs"], rtol=0, atol=2e-15)
         top = orc.erfa_atioq_matrix(a) @ g[f"t{t}_bcrs"]
         np.testing.assert_allclose(top, g[f"t{t}_topo"], rtol=0, atol=2e-15)
+
+
+def test_coherency_rotation_matches_reference():
+    """coordinates.py:288-580 and core/coords.py:152-175 through the reference's
+    own functions; the restatement equals them wherever the reference is finite
+    and is the unperturbed rotation where it divides 0 by 0."""
+    g = golden("coherency")
+    for case in ("lst", "erfa"):
+        topo, ab = g[f"{case}_topo"], g[f"{case}_above"]
+        az, za = orc.enu_to_az_za(topo[0], topo[1], orientation="astropy")
+        rot = orc.coherency_rotation(g["ra"][ab], g["dec"][ab], np.pi / 2 - za[ab], az[ab],
+                                     orc.ENU_TO_ALTAZ @ g[f"{case}_rigid"])
+        ref = g[f"{case}_rot"]
+        finite = ~np.isnan(ref).any(axis=(0, 1))
+        np.testing.assert_allclose(rot[..., finite], ref[..., finite], rtol=0, atol=1e-15)
+        assert np.isfinite(rot).all()
+        np.testing.assert_allclose(rot[0, 0] ** 2 + rot[0, 1] ** 2, 1.0, rtol=0, atol=1e-14)
+        c = orc.rotate_coherency(g["coherency"][ab], rot)
+        fc = ~np.isnan(g[f"{case}_rotated"]).any(axis=(1, 2, 3))
+        np.testing.assert_allclose(c[fc], g[f"{case}_rotated"][fc], rtol=0, atol=1e-15)
+
+
+def test_oracle_unpolarised_coherency_equals_scalar():
+    from matvis_b200 import workloads as wl
+
+    cfg = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=400, nfreq=1, ntimes=2, nant=5, seed=3)
+    beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in cfg["beams"]]
+    kw = dict(ants={i: tuple(p) for i, p in enumerate(cfg["antpos"])}, ra=cfg["ra"], dec=cfg["dec"],
+              freqs=cfg["freqs"], lsts=cfg["lsts"], latitude=cfg["latitude"], beams=beams, polarized=True,
+              beam_idx=cfg["beam_idx"])
+    a = orc.simulate_vis(fluxes=cfg["fluxes"], **kw)
+    b = orc.simulate_vis(fluxes=orc.stokes_to_coherency(cfg["fluxes"], 0, 0, 0), **kw)
+    np.testing.assert_allclose(b, a, rtol=0, atol=1e-12 * np.abs(a).max())
