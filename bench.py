@@ -217,8 +217,10 @@ def cpu_oracle_sample(cfg, nsrc_sample: int, nslices: int = 1):
         terms += len(antpos) ** 2 * n
     dt = time.perf_counter() - t0
     del vis
-    return terms / dt, dt, f"{nslices} (f, t) slice(s), all {len(antpos)} antennas, {nsrc_sample} of " \
-                           f"{len(cfg['ra'])} sources (seeded subset), FP64 numpy/scipy"
+    srcs = (f"all {len(cfg['ra'])} sources" if nsrc_sample >= len(cfg["ra"])
+            else f"{nsrc_sample} of {len(cfg['ra'])} sources (seeded subset)")
+    return terms / dt, dt, f"{nslices} (f, t) slice(s) of the workload, all {len(antpos)} antennas, {srcs}, " \
+                           f"FP64 numpy/scipy oracle"
 
 
 def run_reference(args, rank, world):
@@ -226,8 +228,8 @@ def run_reference(args, rank, world):
         return
     from matvis_b200 import workloads as wl
 
-    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes)
-    nsrc_sample = 49152
+    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes, nside=args.nside)
+    nsrc_sample = len(cfg["ra"])  # one full (f, t) slice per step (a few seconds on the host cores)
     for _ in range(max(args.warmup, 0)):
         cpu_oracle_sample(cfg, nsrc_sample)
     vals, dts = [], []
@@ -335,9 +337,15 @@ def run_b200(args, rank, world, local_rank):
     peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
     achieved = algo_flops / (herk_ms / 1000.0) / 1e12
     tensor_peak = bf16_peak / 2 if args.gemm_mode.startswith("tf32") else bf16_peak
+    # DRAM bytes per launch from an ncu capture (dram__bytes_read/write.sum) of the
+    # nside-64 slice of this workload (K = 49,152, k_chunk 4096: 312.3 MB read, 57.7 MB
+    # written over 12 x 21 work units), scaled by the columns read and the units written
+    n_units = (T * (T + 1) // 2) * -(-kvalid // kc)
+    traffic = 312.251904e6 / 49152 * kvalid + 57.691904e6 / 252 * n_units
     roofline = {
         "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
-        "traffic": None, "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
+        "traffic": traffic, "traffic_source": "ncu dram bytes of the nside-64 slice, scaled by columns and units",
+        "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
         "kernel": f"mvb_herk {args.gemm_mode}: M={M}, K={kvalid}, k_chunk={kc}",
         "herk_ms": herk_ms,
         "algorithmic_flops_per_launch": algo_flops,
@@ -369,7 +377,8 @@ def run_b200(args, rank, world, local_rank):
     }
 
     if rank == 0 and world == 1 and not args.skip_cpu:
-        v, dt, sample = cpu_oracle_sample(cfg, 49152)
+        # three full (f, t) slices: about 10 s of FP64 work on the host cores
+        v, dt, sample = cpu_oracle_sample(cfg, len(cfg["ra"]), nslices=3)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample,
                                 "seconds": dt}
     if rank == 0 and not args.skip_plain:

@@ -186,7 +186,8 @@ int mvb_absmax(const void *z, int z_c128, int64_t n, float *out, void *stream);
  *   K_valid = min(n * kmul, Kcap),  n = *n_dev if n_dev != NULL else n_host,
  * i.e. a source count times the columns per source (nax); the device count
  * comes straight from mvb_horizon_compact, with no host round trip. */
-/* Workspace bytes: one FP32 partial tile (256 x 128 floats) per (k-slice, tile). */
+/* Workspace bytes: one FP32 partial tile (256 x 128 floats) per (k-slice, tile);
+ * the workspace must be 16-byte aligned. */
 size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
 /* Upper-triangle 128 x 128 complex tiles of V = conj(Z) Z^T over K_valid
  * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05

@@ -387,10 +387,10 @@ struct FF {
   __device__ __forceinline__ double value() const { return (double)hi + (double)lo; }
 };
 
-// One CTA (256 threads) per 8 columns of an upper tile: thread (r, h) sums rows
-// r of columns c0 + 4h .. c0 + 4h + 3 (real and imaginary) over the k-slices,
-// so each slice contributes two contiguous 4 KB runs per CTA.  F is a template
-// parameter (no runtime integer division in the index arithmetic).
+// One CTA (8 warps) per 8 columns of an upper tile: warp w sums column c0 + w,
+// lane l rows 4l .. 4l + 3 (a 16-byte load per component per k-slice; a warp
+// reads the column's two contiguous 512-byte runs).  F is a template parameter
+// (no runtime integer division in the index arithmetic).
 template <typename OT, int F>
 __global__ void __launch_bounds__(256)
     herk_reduce_all_kernel(const float *__restrict__ part, int T, int n_tiles, const int32_t *__restrict__ n_dev,
@@ -404,48 +404,43 @@ __global__ void __launch_bounds__(256)
   int64_t kc;
   plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
   const int M = A * F;
-  const int r = threadIdx.x & 127, h = threadIdx.x >> 7;
-  const int c0 = g * 8 + h * 4;
-  const int m = I * 128 + r;
-  if (J * 128 + c0 >= M || I * 128 >= M) return;  // columns (or the whole tile) past M: nothing to write
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = g * 8 + w;
+  const int n = J * 128 + c;
+  const int r0 = 4 * lane;
+  if (n >= M || I * 128 + r0 >= M) return;  // nothing of this thread's to write
   FF are[4], aim[4];
-  const size_t sstride = (size_t)n_tiles * (256 * 128);
-  const float *p0 = part + (size_t)t * (256 * 128) + r;
+  const size_t sstride = (size_t)n_tiles * (256 * 128) / 4;  // in float4
+  const float4 *pre = reinterpret_cast<const float4 *>(part + (size_t)t * (256 * 128) + c * 128 + r0);
+  const float4 *pim = reinterpret_cast<const float4 *>(part + (size_t)t * (256 * 128) + (128 + c) * 128 + r0);
   int s = 0;
-  // four slices per step: 32 independent loads in flight per thread, sums in slice order
+  // four slices per step: 8 independent 16-byte loads in flight, sums in slice order
   for (; s + 4 <= nsplit; s += 4) {
-    float vr[4][4], vi[4][4];
+    float4 vr[4], vi[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 4; ++u) {
+      vr[u] = __ldg(pre + (s + u) * sstride);
+      vi[u] = __ldg(pim + (s + u) * sstride);
+    }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        vr[u][j] = __ldg(p0 + (s + u) * sstride + (c0 + j) * 128);
-        vi[u][j] = __ldg(p0 + (s + u) * sstride + (128 + c0 + j) * 128);
-      }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        are[j].add(vr[u][j]);
-        aim[j].add(vi[u][j]);
-      }
-  }
-  for (; s < nsplit; ++s) {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      are[j].add(__ldg(p0 + s * sstride + (c0 + j) * 128));
-      aim[j].add(__ldg(p0 + s * sstride + (128 + c0 + j) * 128));
+    for (int u = 0; u < 4; ++u) {
+      are[0].add(vr[u].x), are[1].add(vr[u].y), are[2].add(vr[u].z), are[3].add(vr[u].w);
+      aim[0].add(vi[u].x), aim[1].add(vi[u].y), aim[2].add(vi[u].z), aim[3].add(vi[u].w);
     }
   }
-  if (m >= M) return;
+  for (; s < nsplit; ++s) {
+    const float4 vr = __ldg(pre + s * sstride), vi = __ldg(pim + s * sstride);
+    are[0].add(vr.x), are[1].add(vr.y), are[2].add(vr.z), are[3].add(vr.w);
+    aim[0].add(vi.x), aim[1].add(vi.y), aim[2].add(vi.z), aim[3].add(vi.w);
+  }
   const int64_t AF2 = (int64_t)A * F * F;
-  const int i = m / F, q = m % F;  // F is 1 or 2: shifts and masks
+  const int jj = n / F, pp = n % F;  // F is 1 or 2: shifts and masks
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int n = J * 128 + c0 + j;
-    if (n >= M) break;
-    const double re = are[j].value() * vscale, im = aim[j].value() * vscale;
-    const int jj = n / F, pp = n % F;
+  for (int k = 0; k < 4; ++k) {
+    const int m = I * 128 + r0 + k;
+    if (m >= M) break;
+    const double re = are[k].value() * vscale, im = aim[k].value() * vscale;
+    const int i = m / F, q = m % F;
     // direct: rows m -> (i, q), columns n -> (j, p); out[(i*A + j)*F*F + p*F + q]
     store_out<OT>(out, i * AF2 + (int64_t)jj * F * F + pp * F + q, re, im, accumulate);
     // mirror: V[n, m] = conj(V[m, n]) for the off-diagonal tiles (a diagonal tile
@@ -573,6 +568,7 @@ extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, con
   if (!n_dev && n_host * kmul > Kcap) return fail(MVB_ERR_ARG, "mvb_herk: n * kmul exceeds Kcap");
   if (reinterpret_cast<uintptr_t>(z) % 16) return fail(MVB_ERR_ARG, "mvb_herk: panel not 16-byte aligned");
   if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk)) return fail(MVB_ERR_ARG, "mvb_herk: workspace too small");
+  if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "mvb_herk: ws must be 16-byte aligned");
   if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk: panel too large");
   if (drain_ksteps < 0 || drain_ksteps > 2) return fail(MVB_ERR_ARG, "mvb_herk: drain_ksteps must be 0, 1 or 2");
   // default: 6-product mode drains every k-step, 3-product modes every 2
@@ -598,6 +594,7 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
   if (!ws || !out || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || nant <= 0 || (nfeed != 1 && nfeed != 2) ||
       k_chunk <= 0 || kmul <= 0 || (int64_t)nant * nfeed > Mpad || (pairs && npairs < 0))
     return fail(MVB_ERR_ARG, "mvb_herk_reduce: bad arguments");
+  if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "mvb_herk_reduce: ws must be 16-byte aligned");
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
   const int nsm = num_sms();
