@@ -150,6 +150,10 @@ int mvb_exptau(const double *antpos, int A, double freq, const double *crd, int6
  * for tf32): element (m, k) of a plane is at (k / KB) * Mpad * KB + m * KB + k % KB.
  * Mpad is a multiple of 128, Kcap of 64.  Bytes: 2P x Mpad x Kcap x element size. */
 size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap);
+/* sflux[f * N + s] = (float) sqrt(0.5 * flux[s * nf + f]) (cpu/cpu.py:188): the
+ * per-frequency sqrt(0.5 I) rows the Z writers read, from the caller's
+ * (N, nf) float64 Stokes I. */
+int mvb_flux_sqrt_half(const double *flux, int64_t N, int nf, float *sflux, void *stream);
 /* Fused tau + Z: Z[a*F+f, s*X+x] = exptau(a, s) * sflux[j] * beam[bidx[a], f, x, s]
  * with j = sidx[s] (sidx != NULL: sflux is the full per-source sqrt(0.5 I) at
  * this frequency, float32) or j = s (sidx == NULL: sflux already compacted),

@@ -48,6 +48,7 @@ _SIGNATURES = {
     "mvb_rotate": (c_int, [_p, c_int64, _p, _p, _p]),
     "mvb_bcrs": (c_int, [_p, c_int64, _p, _p, _p]),
     "mvb_redundant_pairs": (c_int, [_p, c_int64, c_int, _p, c_int64, _p]),
+    "mvb_flux_sqrt_half": (c_int, [_p, c_int64, c_int, _p, _p]),
     "mvb_coherency_rotation": (c_int, [_p, c_int64, _p, _p, c_int64, _p, c_int64, _p, _p, _p]),
     "mvb_rotate_coherency": (c_int, [_p, _p, _p, _p, c_int64, c_int, _p, c_int64, _p]),
     "mvb_tau_z_pol": (c_int, [_p, c_int, ctypes.c_double, _p, c_int64, _p, c_int64, _p, _p, _p, _p, c_int64, c_int,

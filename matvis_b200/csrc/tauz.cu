@@ -615,3 +615,35 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
 #undef MVB_ZX
   return check_launch("tau_z_kernel(exptau)");
 }
+
+// sqrt(0.5 I) per source and frequency (cpu/cpu.py:188), transposed from the
+// caller's (N, Nf) float64 Stokes I to the (Nf, N) float32 rows the Z writers
+// read; 32 x 32 tiles through shared memory so both sides are coalesced.
+namespace mvb {
+__global__ void flux_sqrt_half_kernel(const double *__restrict__ flux, int64_t N, int nf, float *__restrict__ out) {
+  __shared__ float tile[32][33];
+  const int64_t s0 = (int64_t)blockIdx.x * 32;
+  const int f0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t s = s0 + r;
+    const int f = f0 + threadIdx.x;
+    if (s < N && f < nf) tile[r][threadIdx.x] = (float)sqrt(0.5 * flux[s * nf + f]);
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int f = f0 + r;
+    const int64_t s = s0 + threadIdx.x;
+    if (s < N && f < nf) out[(int64_t)f * N + s] = tile[threadIdx.x][r];
+  }
+}
+}  // namespace mvb
+
+extern "C" int mvb_flux_sqrt_half(const double *flux, int64_t N, int nf, float *sflux, void *stream) {
+  if (N < 0 || nf <= 0 || (N > 0 && (!flux || !sflux))) return fail(MVB_ERR_ARG, "mvb_flux_sqrt_half: bad arguments");
+  if (N == 0) return MVB_OK;
+  if (ceil_div(N, 32) > 0x7fffffff || ceil_div(nf, 32) > 65535)
+    return fail(MVB_ERR_ARG, "mvb_flux_sqrt_half: too many sources or frequencies");
+  dim3 grid((unsigned)ceil_div(N, 32), (unsigned)ceil_div(nf, 32));
+  flux_sqrt_half_kernel<<<grid, dim3(32, 8), 0, as_stream(stream)>>>(flux, N, nf, sflux);
+  return check_launch("flux_sqrt_half_kernel");
+}

@@ -37,9 +37,11 @@ from .getz import ZMatrixCalc
 from .autotune import tune_k_chunk
 from .matprod import B200MatMul, B200VectorDot, choose_k_chunk
 
-#: k-slice of the Hermitian product before autotuning (fastest at the
-#: HERA-350-like slice: 2.37 ms at 2048 vs 2.61 ms at 8192 columns).
-DEFAULT_K_CHUNK = 2048
+#: k-slice of the Hermitian product without autotuning: the tuner's choice for
+#: the HERA-350-like slice in fp16x3 (product + reduction 1.36 ms at 4096
+#: columns; shorter slices mean more partial tiles to reduce).  The number of
+#: slices is still fitted to whole waves of SMs on the device.
+DEFAULT_K_CHUNK = 4096
 
 
 @dataclass
@@ -108,16 +110,16 @@ class VisEngine:
                 [c[..., 0, 0].real, c[..., 1, 1].real, c[..., 0, 1].real, c[..., 0, 1].imag], axis=-1
             ).transpose(1, 0, 2).astype(np.float32))
             trace = np.maximum(c[..., 0, 0].real + c[..., 1, 1].real, 0.0)
-            self.sflux_host = np.ascontiguousarray(np.sqrt(0.5 * trace).T.astype(np.float32))
+            self.flux_host = np.ascontiguousarray(trace)  # Stokes I, for the Z scale bound
             if s.radec is not None:
                 self.radec_host = np.ascontiguousarray(np.asarray(s.radec, dtype=np.float64).reshape(2, self.nsrc))
             else:
                 e = self.eci_host
                 self.radec_host = np.ascontiguousarray(np.stack([np.arctan2(e[1], e[0]), np.arcsin(np.clip(e[2], -1, 1))]))
         else:
-            fl = fl.astype(np.float64)
-            # sqrt(0.5 I) per frequency (cpu/cpu.py:188), frequency-major, float32
-            self.sflux_host = np.ascontiguousarray(np.sqrt(0.5 * fl).T.astype(np.float32))
+            # Stokes I (N, Nf); sqrt(0.5 I) (cpu/cpu.py:188) is formed on the device,
+            # frequency-major float32, by mvb_flux_sqrt_half at upload
+            self.flux_host = np.ascontiguousarray(fl, dtype=np.float64)
         self.method = _norm_matprod(s.matprod)
         self.nchunks = max(1, int(s.nchunks))
         self.chunk_size = int(np.ceil(self.nsrc / self.nchunks)) if self.nsrc else 1
@@ -151,7 +153,8 @@ class VisEngine:
         if self.method == "MatMul" and _lib.GEMM_MODES.get(s.gemm_mode, s.gemm_mode) == _lib.GEMM_F16_3:
             # |Z| <= max sqrt(0.5 I) * max |beam| (bilinear weights are convex, |exptau| = 1); for a
             # polarised sky |sum_x beam_x L_xy| <= sqrt(2) max|beam| sqrt(trace C) = 2 max|beam| sqrt(I / 2)
-            zmax = float(self.sflux_host.max(initial=0.0)) * beam_bound(s.beams) * (2.0 if self.pol_sky else 1.0)
+            smax = float(np.sqrt(0.5 * max(float(self.flux_host.max(initial=0.0)), 0.0)))
+            zmax = smax * beam_bound(s.beams) * (2.0 if self.pol_sky else 1.0)
             self.zscale = _lib.f16_scale(zmax * (1 + 2**-10))
         self._graph = None
         self._allocated = False
@@ -208,13 +211,18 @@ class VisEngine:
             self.allocate()
         self.eci.copy_(torch.from_numpy(self.eci_host), non_blocking=False)
         self.antpos.copy_(torch.from_numpy(self.antpos_host))
-        self.sflux.copy_(torch.from_numpy(self.sflux_host))
+        if self.pol_sky:
+            self.sflux.zero_()  # not read: the polarised writer takes the coherency
+        elif self.nsrc:
+            fl = torch.from_numpy(self.flux_host).to(self.eci.device, non_blocking=False)
+            _lib.check(_lib.lib.mvb_flux_sqrt_half(_lib.ptr(fl), self.nsrc, len(self.freqs), _lib.ptr(self.sflux),
+                                                   _lib.stream_handle()))
         if self.pol_sky:
             self.coh.copy_(torch.from_numpy(self.coh_host))
             self.radec.copy_(torch.from_numpy(self.radec_host))
 
     def h2d_bytes(self) -> int:
-        n = self.eci_host.nbytes + self.antpos_host.nbytes + self.sflux_host.nbytes
+        n = self.eci_host.nbytes + self.antpos_host.nbytes + (0 if self.pol_sky else self.flux_host.nbytes)
         if self.pol_sky:
             n += self.coh_host.nbytes + self.radec_host.nbytes
         return n
@@ -335,12 +343,18 @@ class VisEngine:
         steps: queue.Queue = queue.Queue()
         errors: list[BaseException] = []
 
+        page = 4096 // out.itemsize
+
         def copier():
             try:
                 torch.cuda.set_device(dev)
                 with torch.cuda.stream(side):
                     while (item := steps.get()) is not None:
                         t, done = item
+                        # touch the destination pages while the step still computes, so that
+                        # the copy after it is not held up by first-touch page faults
+                        for f in range(nf):
+                            out[f, t].reshape(-1)[::page] = 0
                         side.wait_event(done)
                         for f in range(nf):
                             host[f, t].copy_(self.vis[f, t])

@@ -274,3 +274,15 @@ def test_herk_accumulation_positive_sums(device, k_chunk, mode):
     rel = np.abs(out.cpu().numpy() - ref) / np.abs(ref)
     print(f"{mode} k_chunk={k_chunk}: max rel {rel.max():.3e}, mean rel {rel.mean():.3e}")
     assert rel.max() < 2e-6
+
+
+@pytest.mark.parametrize("N,nf", [(1, 1), (33, 3), (70001, 64), (1000, 33)])
+def test_flux_sqrt_half_bitexact(device, N, nf):
+    """sqrt(0.5 I) transposed to (Nf, N) float32 (cpu/cpu.py:188): FP64 square root
+    rounded once to float32, as numpy does it."""
+    rng = np.random.default_rng(N + nf)
+    fl = rng.lognormal(0, 2, (N, nf))
+    out = torch.empty((nf, N), dtype=torch.float32, device=DEV)
+    src = torch.as_tensor(fl, device=DEV)
+    _lib.check(_lib.lib.mvb_flux_sqrt_half(_lib.ptr(src), N, nf, _lib.ptr(out), None))
+    np.testing.assert_array_equal(out.cpu().numpy(), np.sqrt(0.5 * fl).T.astype(np.float32))
