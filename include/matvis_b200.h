@@ -197,7 +197,7 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
  * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05
  * tensor cores with TMEM accumulators, fed by TMA (cp.async.bulk.tensor,
  * 32-byte swizzle); mode MVB_GEMM_* selects the split precision.
- * drain_ksteps (1 or 2; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
+ * drain_ksteps (1, 2 or 4; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
  * number of 32-byte k-steps summed in one TMEM block before the block is added
  * to FP32 registers: the tensor core rounds its accumulator toward zero at every
  * instruction, so short blocks bound that drift.

@@ -142,7 +142,7 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
     umma_bf16(d, a, b, idesc, acc);
 }
 
-// KD: k-steps accumulated in one TMEM block before it is drained (1 or 2).
+// KD: k-steps accumulated in one TMEM block before it is drained (1, 2 or 4).
 template <int MODE, int KD>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const __grid_constant__ CUtensorMap zmap, int T, int n_tiles, const int32_t *__restrict__ n_dev,
@@ -439,7 +439,8 @@ __global__ void __launch_bounds__(256)
   for (int k = 0; k < 4; ++k) {
     const int m = I * 128 + r0 + k;
     if (m >= M) break;
-    const double re = are[k].value() * vscale, im = aim[k].value() * vscale;
+    // an autocorrelation of one feed (m == n) is real, as conj(z) z is in the reference
+    const double re = are[k].value() * vscale, im = m == n ? 0.0 : aim[k].value() * vscale;
     const int i = m / F, q = m % F;
     // direct: rows m -> (i, q), columns n -> (j, p); out[(i*A + j)*F*F + p*F + q]
     store_out<OT>(out, i * AF2 + (int64_t)jj * F * F + pp * F + q, re, im, accumulate);
@@ -480,7 +481,8 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
       re.add(__ldg(p0 + c * 128 + r));
       im.add(__ldg(p0 + (128 + c) * 128 + r));
     }
-    store_out<OT>(out, e, re.value() * vscale, (conj ? -im.value() : im.value()) * vscale, accumulate);
+    const double vi = m == n ? 0.0 : (conj ? -im.value() : im.value()) * vscale;  // one-feed autos are real
+    store_out<OT>(out, e, re.value() * vscale, vi, accumulate);
   }
 }
 
@@ -490,9 +492,9 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
 // Raises a kernel's dynamic shared-memory limit once per (device, slot); the
 // attribute is not touched again, in particular not during graph capture.
 int set_smem_once(const void *fn, int bytes, int slot) {
-  static bool done[64][16] = {};
+  static bool done[64][32] = {};
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 16)
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 32)
     return fail(MVB_ERR_CUDA, "set_smem_once: bad device");
   if (done[dev][slot]) return MVB_OK;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -541,7 +543,9 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   const int64_t max_units = (int64_t)n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
   const int grid = (int)std::min<int64_t>(max_units, nsm);
   const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
-  int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE, KD>), (int)smem, 2 * MODE + (KD - 1));
+  // slots 16 + 3 * MODE + {0, 1, 2} for KD = {1, 2, 4}
+  int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE, KD>), (int)smem,
+                         16 + 3 * MODE + (KD == 4 ? 2 : KD - 1));
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
   herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials,
@@ -570,14 +574,16 @@ extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, con
   if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk)) return fail(MVB_ERR_ARG, "mvb_herk: workspace too small");
   if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "mvb_herk: ws must be 16-byte aligned");
   if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk: panel too large");
-  if (drain_ksteps < 0 || drain_ksteps > 2) return fail(MVB_ERR_ARG, "mvb_herk: drain_ksteps must be 0, 1 or 2");
+  if (drain_ksteps < 0 || drain_ksteps > 4 || drain_ksteps == 3)
+    return fail(MVB_ERR_ARG, "mvb_herk: drain_ksteps must be 0, 1, 2 or 4");
   // default: 6-product mode drains every k-step, 3-product modes every 2
   const int kd = drain_ksteps ? drain_ksteps : (mode == MVB_GEMM_BF16_6 ? 1 : 2);
   cudaStream_t s = as_stream(stream);
   float *part = static_cast<float *>(ws);
 #define MVB_HERK(M)                                                                           \
-  return kd == 1 ? launch_herk<M, 1>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
-                 : launch_herk<M, 2>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s)
+  return kd == 1   ? launch_herk<M, 1>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
+         : kd == 2 ? launch_herk<M, 2>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
+                   : launch_herk<M, 4>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s)
   switch (mode) {
     case MVB_GEMM_BF16_3: MVB_HERK(MVB_GEMM_BF16_3);
     case MVB_GEMM_BF16_6: MVB_HERK(MVB_GEMM_BF16_6);

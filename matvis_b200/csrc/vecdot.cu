@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(256)
         }
         if (lane == 0) {
           part[(u * F * F + p * F + q) * 2] = r;
-          part[(u * F * F + p * F + q) * 2 + 1] = i;
+          part[(u * F * F + p * F + q) * 2 + 1] = (ai == aj && p == q) ? 0.0 : i;  // one-feed autos are real
         }
       }
   }

@@ -164,14 +164,17 @@ class VisEngine:
         dev = self.device
         s = self.spec
         A, N = self.nant, self.nsrc
-        self.eci = torch.empty((3, N), dtype=torch.float64, device=dev)
+        # at least one source slot, so that an empty sky still hands the kernels
+        # valid pointers (they read nothing when the source count is 0)
+        Na = max(N, 1)
+        self.eci = torch.zeros((3, Na), dtype=torch.float64, device=dev)
         self.antpos = torch.empty((A, 3), dtype=torch.float64, device=dev)
-        self.sflux = torch.empty((len(self.freqs), N), dtype=torch.float32, device=dev)
-        self.topo = torch.zeros((3, N), dtype=torch.float64, device=dev)
-        self.bcrs = torch.zeros((3, N), dtype=torch.float64, device=dev) if self.bcrs_plan is not None else None
+        self.sflux = torch.zeros((len(self.freqs), Na), dtype=torch.float32, device=dev)
+        self.topo = torch.zeros((3, Na), dtype=torch.float64, device=dev)
+        self.bcrs = torch.zeros((3, Na), dtype=torch.float64, device=dev) if self.bcrs_plan is not None else None
         if self.pol_sky:
-            self.coh = torch.empty((len(self.freqs), N, 4), dtype=torch.float32, device=dev)
-            self.radec = torch.empty((2, N), dtype=torch.float64, device=dev)
+            self.coh = torch.zeros((len(self.freqs), Na, 4), dtype=torch.float32, device=dev)
+            self.radec = torch.zeros((2, Na), dtype=torch.float64, device=dev)
             self.rot2 = torch.zeros((self.cap, 2), dtype=torch.float64, device=dev)
         self.crd = torch.zeros((3, self.cap), dtype=torch.float64, device=dev)
         self.kept = torch.zeros((self.cap,), dtype=torch.int32, device=dev)
@@ -209,17 +212,19 @@ class VisEngine:
         """Host -> device copies of the job inputs (pinned staging when possible)."""
         if not self._allocated:
             self.allocate()
-        self.eci.copy_(torch.from_numpy(self.eci_host), non_blocking=False)
+        N = self.nsrc
+        if N:
+            self.eci[:, :N].copy_(torch.from_numpy(self.eci_host), non_blocking=False)
         self.antpos.copy_(torch.from_numpy(self.antpos_host))
         if self.pol_sky:
             self.sflux.zero_()  # not read: the polarised writer takes the coherency
-        elif self.nsrc:
+        elif N:
             fl = torch.from_numpy(self.flux_host).to(self.eci.device, non_blocking=False)
             _lib.check(_lib.lib.mvb_flux_sqrt_half(_lib.ptr(fl), self.nsrc, len(self.freqs), _lib.ptr(self.sflux),
                                                    _lib.stream_handle()))
-        if self.pol_sky:
-            self.coh.copy_(torch.from_numpy(self.coh_host))
-            self.radec.copy_(torch.from_numpy(self.radec_host))
+        if self.pol_sky and N:
+            self.coh[:, :N].copy_(torch.from_numpy(self.coh_host))
+            self.radec[:, :N].copy_(torch.from_numpy(self.radec_host))
 
     def h2d_bytes(self) -> int:
         n = self.eci_host.nbytes + self.antpos_host.nbytes + (0 if self.pol_sky else self.flux_host.nbytes)
