@@ -429,10 +429,12 @@ def run_serve(args, local_rank):
         spec.gemm_mode = args.gemm_mode
     warm = VisServer(device=dev, max_active=args.serve_max_active)
     warm.serve_stream([(0.0, jobs[0][1])])  # kernel warm-up, not timed
+    warm.close()
     srv = VisServer(device=dev, max_active=args.serve_max_active)
     t0 = time.perf_counter()
     srv.serve_stream(jobs)
     wall = time.perf_counter() - t0
+    srv.close()
     summ = latency_summary(srv.results)
     line = {
         "metric": "served form: job latency p50/p99 and throughput", "impl": "b200", "unit": UNIT,

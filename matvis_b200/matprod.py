@@ -50,7 +50,8 @@ class MatProd(ABC):
         self.device = _lib.require_cuda(device)
         if antpairs is None:
             self.all_pairs = True
-            self.antpairs = np.array([(i, j) for i in range(nant) for j in range(nant)])
+            idx = np.arange(nant)
+            self.antpairs = np.stack(np.meshgrid(idx, idx, indexing="ij"), axis=-1).reshape(-1, 2)  # i slow
         else:
             self.all_pairs = False
             self.antpairs = np.asarray(antpairs)

@@ -9,8 +9,12 @@ Jobs (``JobSpec``) arrive at any time.  The server
   resident on the device, and gives it its own CUDA stream;
 * advances the active jobs one time step at a time, round robin, so their
   kernels overlap on the device;
-* copies each finished job's visibilities to pinned host memory, records its
-  latency (submission to result on the host), and frees its memory.
+* hands each finished job to a copier thread, which waits for the job's last
+  kernel on its own stream, copies the visibilities and the status word to the
+  host (touching the result's pages first), and counts the job's terms, so the
+  scheduling loop never waits on a copy or a host allocation; the job's latency
+  runs from submission to its result on the host, after which its device
+  memory is freed.
 
 Each job's arithmetic is exactly the single-job path (same kernels, same
 deterministic reduction order), so a result is bit-identical alone and in a
@@ -19,6 +23,7 @@ mix.  ``latency_summary`` reports p50 / p99 and the throughput.
 
 from __future__ import annotations
 
+import queue
 import threading
 import time
 from collections import deque
@@ -40,7 +45,8 @@ class _Job:
     stream: torch.cuda.Stream | None = None
     next_t: int = 0
     done_event: torch.cuda.Event | None = None
-    host: torch.Tensor | None = None
+    host: np.ndarray | None = None
+    status_word: int = 0
     footprint: int = 0
     t_admit: float = 0.0
     t_done: float = 0.0
@@ -61,10 +67,18 @@ class JobResult:
 class VisServer:
     """Continuous-batching visibility server on one device."""
 
-    def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 8, steps_per_turn: int = 1):
+    def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 8, steps_per_turn: int = 1,
+                 reserve_fraction: float = 0.5):
         self.device = _lib.require_cuda(device)
         free = torch.cuda.mem_get_info(self.device)[0]
         self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
+        # Device allocations for a newly admitted job would otherwise reach
+        # cudaMalloc, which waits for the kernels of the jobs already running;
+        # a block of the budget taken once and handed back to torch's caching
+        # allocator lets admission carve the job's buffers from the cache.
+        if reserve_fraction > 0:
+            reserve = torch.empty(int(self.budget * min(reserve_fraction, 1.0)), dtype=torch.uint8, device=self.device)
+            del reserve
         self.max_active = max_active
         self.steps_per_turn = steps_per_turn
         self._pending: deque[_Job] = deque()
@@ -76,6 +90,40 @@ class VisServer:
         self.in_use = 0
         self.peak_in_use = 0
         self.max_concurrent = 0
+        self._to_copy: queue.Queue = queue.Queue()
+        self._copied: queue.Queue = queue.Queue()
+        self._copier = threading.Thread(target=self._copy_loop, name="mvb-serve-d2h", daemon=True)
+        self._copier.start()
+
+    def close(self):
+        """Stop the copier thread (the server serves no more jobs after this)."""
+        if self._copier.is_alive():
+            self._to_copy.put(None)
+            self._copier.join()
+
+    def _copy_loop(self):
+        torch.cuda.set_device(self.device)
+        cs = torch.cuda.Stream(device=self.device)
+        status = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        while (job := self._to_copy.get()) is not None:
+            try:
+                eng = job.engine
+                host = np.empty(tuple(eng.vis.shape), dtype=np.complex64 if eng.vis.dtype == torch.complex64
+                                else np.complex128)
+                host.reshape(-1)[:: 4096 // host.itemsize] = 0  # first-touch the pages before the copy
+                with torch.cuda.stream(cs):
+                    cs.wait_event(job.done_event)
+                    torch.from_numpy(host).copy_(eng.vis)  # pageable destination: returns when done
+                    status.copy_(eng.status)
+                    cs.synchronize()
+                job.status_word = int(status[0])
+                job.host = host
+                job.t_done = time.perf_counter()
+                job.terms = float(eng.nant ** 2 * len(eng.freqs)) * self._n_above_total(job)
+            except Exception as exc:  # recorded per job; the server keeps running
+                job.error = f"copy failed: {exc}"
+                job.t_done = time.perf_counter()
+            self._copied.put(job)
 
     # ------------------------------------------------------------------ API
     def submit(self, spec: JobSpec, t_submit: float | None = None) -> int:
@@ -132,40 +180,37 @@ class VisServer:
                     eng.enqueue_time(job.next_t, stream=job.stream)
                     job.next_t += 1
                 if job.next_t >= nt:
-                    job.host = torch.empty(eng.vis.shape, dtype=eng.vis.dtype, pin_memory=True)
-                    job.host.copy_(eng.vis, non_blocking=True)
                     job.done_event = torch.cuda.Event()
                     job.done_event.record(job.stream)
                     self._finishing.append(job)
+                    self._to_copy.put(job)
                     continue
             still.append(job)
         self._active = still
 
     def _retire(self):
-        keep = []
-        for job in self._finishing:
-            if not job.done_event.query():
-                keep.append(job)
-                continue
-            job.t_done = time.perf_counter()
-            eng = job.engine
-            err = None
+        while True:
             try:
-                _lib.check_status_word(eng.status, f"job {job.jid}")
-            except Exception as exc:  # recorded per job; the server keeps running
-                err = str(exc)
-            vis = job.host.numpy()
-            if not job.spec.polarized:
+                job = self._copied.get_nowait()
+            except queue.Empty:
+                break
+            err = job.error
+            if err is None and job.status_word:
+                try:
+                    _lib.check_status_word(torch.tensor([job.status_word], dtype=torch.int32), f"job {job.jid}")
+                except Exception as exc:
+                    err = str(exc)
+            vis = job.host
+            if vis is not None and not job.spec.polarized:
                 vis = vis[..., 0, 0]
-            A = eng.nant
-            terms = float(A * A * len(eng.freqs)) * self._n_above_total(job)
             self._results[job.jid] = JobResult(jid=job.jid, vis=None if err else vis, latency_s=job.t_done - job.t_submit,
-                                               queue_s=job.t_admit - job.t_submit, terms=terms, error=err)
+                                               queue_s=job.t_admit - job.t_submit, terms=job.terms, error=err)
             with self._lock:
                 self.in_use -= job.footprint
+            self._finishing.remove(job)
             job.engine = None
             job.stream = None
-        self._finishing = keep
+            job.host = None
 
     @staticmethod
     def _n_above_total(job: _Job) -> float:
@@ -208,6 +253,8 @@ class VisServer:
                 time.sleep(min(0.001, max(0.0, arrivals[i][0] - now)))
                 continue
             self.poll()
+            if not self._active and self._finishing and not self._pending:
+                time.sleep(0.0002)  # only copies in flight: leave the interpreter to the copier
             if time.perf_counter() - t0 > timeout_s:
                 raise TimeoutError("serve_stream did not finish in time")
         return ids
