@@ -7,14 +7,19 @@ dependencies):
 
 * ``times`` are local sidereal times in radians and ``telescope_loc`` is the
   latitude in radians (or an object with ``.lat``); the rotation is the rigid
-  LST rotation (``coord_method="CoordinateRotationLST"``);
+  LST rotation (``coord_method="CoordinateRotationLST"``), or the ERFA-style
+  apparent place (``coord_method="CoordinateRotationERFA"``) from per-time
+  astrometry parameters given in ``coord_method_params``;
+* ``fluxes`` is Stokes I (NSRCS, NFREQS), or, with ``polarized=True``, a
+  (NSRCS, NFREQS, 2, 2) coherency for a polarised sky;
 * beams are :class:`~matvis_b200.beams.GridBeam` / :class:`~matvis_b200.beams.GaussianBeam`
   or a beamfits beam (:func:`~matvis_b200.beamfits.read_beamfits`), interpolated to
   each frequency;
 * ``skycoords`` is an (ra, dec) pair in radians or an object with ``.ra``/``.dec``.
 
 Both run the batched engine (``engine.VisEngine``): every time and frequency of
-the call is one launch sequence on the GPU, with device-side source counts.
+the call is one launch sequence on the GPU, with device-side source counts, and
+each time step's visibilities are copied to the host while later steps compute.
 """
 
 from __future__ import annotations
