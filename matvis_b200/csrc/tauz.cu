@@ -175,13 +175,24 @@ struct PanelWriter {
   }
 };
 
-constexpr int kTauZThreads = 64;
-constexpr int kTauZSrc = 4;      // consecutive sources per thread (16-byte stores per plane at X = 2)
-constexpr int kTauZAnts = 32;    // antennas per CTA (the CTA's beam block is read once per 32 antennas)
-constexpr int kTauZMaxBFX = 16;  // beams staged in shared memory up to nbeam * F * X = 16, else read from L2
-constexpr int kTauZBlockSrc = kTauZThreads * kTauZSrc;
+// CTA = 128 threads over 32 sources x 64 antennas: thread bits 0..2 pick a group
+// of 4 consecutive sources (16-byte stores per plane at X = 2), bits 3..6 one of
+// 16 antenna lanes, each lane taking every 16th antenna of the block.  A CTA
+// thus writes only 4 k-blocks (X = 2) of 128 rows, so the Z lines it has open at
+// any time fit, summed over the resident CTAs, well inside L2 (a wider k-range
+// per CTA left partially written lines to be evicted); a warp's store writes 16
+// whole 32-byte sectors.  The CTA's beam values (nbeam * F * X x 32 sources)
+// are staged once in shared memory for its 16 antenna lanes.
+constexpr int kTauZThreads = 128;
+constexpr int kTauZSrc = 4;                 // consecutive sources per thread
+constexpr int kTauZGroups = 8;              // source groups per CTA
+constexpr int kTauZAntLanes = kTauZThreads / kTauZGroups;
+constexpr int kTauZAnts = 64;               // antennas per CTA
+constexpr int kTauZBlockSrc = kTauZGroups * kTauZSrc;
+constexpr int kTauZRow = kTauZBlockSrc + 1;  // staged beam values per q, padded
+constexpr int kTauZMaxBFX = 16;              // beam planes staged in shared memory, else read through L1
 
-// grid.x: blocks of kTauZBlockSrc sources, grid.y: antenna blocks (kTauZAnts).
+// grid.x: blocks of kTauZBlockSrc sources, grid.y: blocks of kTauZAnts antennas.
 // EXT = 0: phase from antpos . crd (fused tau); EXT = 1 / 2: phase factor read
 // from a caller exptau (A, e_ld) in complex64 / complex128, multiplied by sflux.
 // POL (EXT = 0, X = 2): polarised sky.  Instead of sqrt(0.5 I) the source
@@ -201,7 +212,8 @@ __global__ void __launch_bounds__(kTauZThreads)
   static_assert(!POL || (X == 2 && EXT == 0), "the polarised sky needs two beam axes and the fused phase");
   const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
   const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
-  const int64_t s0 = ((int64_t)blockIdx.x * kTauZThreads + threadIdx.x) * kTauZSrc;
+  const int64_t s0 = (int64_t)blockIdx.x * kTauZBlockSrc + (threadIdx.x % kTauZGroups) * kTauZSrc;
+  const int alane = threadIdx.x / kTauZGroups;
   if ((int64_t)blockIdx.x * kTauZBlockSrc >= s_end) return;  // uniform per CTA
   const bool write = s0 < s_end;  // s_end is a multiple of kTauZSrc (64 / X)
 
@@ -245,24 +257,28 @@ __global__ void __launch_bounds__(kTauZThreads)
       l00[j] = l10r[j] = l10i[j] = l11[j] = 0.f;
     }
   }
-  // STAGED: the CTA's beam values in shared memory, [q][j][thread] (thread
-  // fastest: the per-antenna reads are conflict-free; each thread reads only its
-  // own entries, so no barrier is needed), q = (beam * F + f) * X + x.
-  // Otherwise (many beams) the values are read from L2 per antenna.
+  // STAGED: the CTA's beam values, shared by its 16 antenna lanes, in shared
+  // memory as [q][j][group] with a row of 33 values per q (q = (beam * F + f) *
+  // X + x): the 8 source groups of a warp read 8 consecutive values, and lanes
+  // with different beams land on different banks.  Otherwise (more than 16 beam
+  // planes) the values are read through L1 per antenna.
   extern __shared__ float2 bsm[];
   if constexpr (STAGED) {
-    const int nbfx = nbeam * F * X;
-    for (int q = 0; q < nbfx; ++q)
-#pragma unroll
-      for (int j = 0; j < kTauZSrc; ++j)
-        bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x] =
-            (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
+    const int nq = nbeam * F * X;
+    for (int e = threadIdx.x; e < nq * kTauZBlockSrc; e += kTauZThreads) {
+      const int q = e / kTauZBlockSrc, sl = e % kTauZBlockSrc;  // sl = group * kTauZSrc + j
+      const int64_t ss = (int64_t)blockIdx.x * kTauZBlockSrc + sl;
+      bsm[q * kTauZRow + (sl % kTauZSrc) * kTauZGroups + sl / kTauZSrc] =
+          ss < n ? __ldg(beam + (int64_t)q * beam_ld + ss) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
   }
+  const int sg = threadIdx.x % kTauZGroups;
   const int a0 = blockIdx.y * kTauZAnts;
   const int a1 = min(a0 + kTauZAnts, A);
   const int64_t plane = Mpad * Kcap;
   {
-    for (int a = a0; a < a1; ++a) {
+    for (int a = a0 + alane; a < a1; a += kTauZAntLanes) {
       const int b = beam_idx ? beam_idx[a] : 0;
       float er[kTauZSrc], ei[kTauZSrc];
       double dx = 0, dy = 0, dz = 0;
@@ -303,9 +319,9 @@ __global__ void __launch_bounds__(kTauZThreads)
             const int q = (b * F + f) * X + x;
             float2 bv;
             if constexpr (STAGED)
-              bv = bsm[(q * kTauZSrc + j) * kTauZThreads + threadIdx.x];
+              bv = bsm[q * kTauZRow + j * kTauZGroups + sg];
             else
-              bv = (s0 + j < n) ? beam[(int64_t)q * beam_ld + s0 + j] : make_float2(0.f, 0.f);
+              bv = (s0 + j < n) ? __ldg(beam + (int64_t)q * beam_ld + s0 + j) : make_float2(0.f, 0.f);
             vr[j * X + x] = er[j] * bv.x - ei[j] * bv.y;
             vi[j * X + x] = er[j] * bv.y + ei[j] * bv.x;
           }
@@ -450,25 +466,25 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
   if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !sflux || (nsrc > 0 && !crd) || (F != 1 && F != 2) ||
       (X != 1 && X != 2) || nbeam <= 0 || beam_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_tau_z: bad arguments");
-  const bool staged = nbeam * F * X <= kTauZMaxBFX;
-  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z");
   if (rc) return rc;
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z: Kcap too small for nsrc * nax");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  const bool staged = nbeam * F * X <= kTauZMaxBFX;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZRow * sizeof(float2) : 0;
   const double foc = freq * kInvC;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_TAUZ(M, XX)                                                                                        \
-  do {                                                                                                         \
-  if (staged)                                                                                                  \
-    tau_z_kernel<M, XX, 0, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
-                                                                bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
-  else                                                                                                         \
-    tau_z_kernel<M, XX, 0, false><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, \
-                                                              bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
+#define MVB_TAUZ(M, XX)                                                                                    \
+  do {                                                                                                       \
+    if (staged)                                                                                              \
+      tau_z_kernel<M, XX, 0, true, false><<<grid, kTauZThreads, smem, s>>>(                                  \
+          antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
+    else                                                                                                     \
+      tau_z_kernel<M, XX, 0, false, false><<<grid, kTauZThreads, 0, s>>>(                                    \
+          antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
   } while (0)
 #define MVB_TAUZ2(M) \
   if (X == 2)        \
@@ -534,26 +550,22 @@ extern "C" int mvb_tau_z_pol(const double *antpos, int A, double freq, const dou
     return fail(MVB_ERR_ARG, "mvb_tau_z_pol: coh and rot must be 16-byte aligned");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
-  const bool staged = nbeam * F * X <= kTauZMaxBFX;
-  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  const bool staged = nbeam * F * X <= kTauZMaxBFX;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZRow * sizeof(float2) : 0;
   const double foc = freq * kInvC;
   const float2 *bm = static_cast<const float2 *>(beam);
   const float4 *c4 = reinterpret_cast<const float4 *>(coh);
   const double2 *r2 = reinterpret_cast<const double2 *>(rot);
   cudaStream_t s = as_stream(stream);
-#define MVB_TZP(M)                                                                                                \
-  do {                                                                                                            \
-    if (staged)                                                                                                   \
-      tau_z_kernel<M, 2, 0, true, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,    \
-                                                                        nullptr, sidx, bm, beam_ld, nbeam,        \
-                                                                        beam_idx, F, zscale, z, Mpad, Kcap,       \
-                                                                        nullptr, 0, c4, r2);                      \
-    else                                                                                                          \
-      tau_z_kernel<M, 2, 0, false, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,      \
-                                                                      nullptr, sidx, bm, beam_ld, nbeam,          \
-                                                                      beam_idx, F, zscale, z, Mpad, Kcap,         \
-                                                                      nullptr, 0, c4, r2);                        \
+#define MVB_TZP(M)                                                                                          \
+  do {                                                                                                             \
+    if (staged)                                                                                                    \
+      tau_z_kernel<M, 2, 0, true, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,      \
+          nullptr, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, nullptr, 0, c4, r2);               \
+    else                                                                                                           \
+      tau_z_kernel<M, 2, 0, false, true><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,        \
+          nullptr, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, nullptr, 0, c4, r2);               \
   } while (0)
   switch (mode) {
     case MVB_GEMM_BF16_3: MVB_TZP(MVB_GEMM_BF16_3); break;
@@ -572,26 +584,24 @@ extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, i
   if (A <= 0 || nsrc < 0 || !exptau || !z || !beam || !sflux || (F != 1 && F != 2) || (X != 1 && X != 2) ||
       nbeam <= 0 || beam_ld < nsrc || e_ld < nsrc)
     return fail(MVB_ERR_ARG, "mvb_z_from_exptau: bad arguments");
-  const bool staged = nbeam * F * X <= kTauZMaxBFX;
-  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZSrc * kTauZThreads * sizeof(float2) : 0;
   int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_z_from_exptau");
   if (rc) return rc;
   if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_z_from_exptau: Kcap too small");
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
   dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  const bool staged = nbeam * F * X <= kTauZMaxBFX;
+  const size_t smem = staged ? (size_t)nbeam * F * X * kTauZRow * sizeof(float2) : 0;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_ZX(M, XX, E)                                                                                       \
-  do {                                                                                                         \
-  if (staged)                                                                                                  \
-    tau_z_kernel<M, XX, E, true><<<grid, kTauZThreads, smem, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux, \
-                                                                nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z, \
-                                                                Mpad, Kcap, exptau, e_ld);                    \
-  else                                                                                                         \
-    tau_z_kernel<M, XX, E, false><<<grid, kTauZThreads, smem, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr, nsrc, sflux,  \
-                                                              nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z,  \
-                                                              Mpad, Kcap, exptau, e_ld);                    \
+#define MVB_ZX(M, XX, E)                                                                                      \
+  do {                                                                                                             \
+    if (staged)                                                                                                    \
+      tau_z_kernel<M, XX, E, true, false><<<grid, kTauZThreads, smem, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr,    \
+          nsrc, sflux, nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, exptau, e_ld);              \
+    else                                                                                                           \
+      tau_z_kernel<M, XX, E, false, false><<<grid, kTauZThreads, 0, s>>>(nullptr, A, 0.0, nullptr, 0, nullptr,      \
+          nsrc, sflux, nullptr, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, exptau, e_ld);              \
   } while (0)
 #define MVB_ZX3(M, E) \
   if (X == 2)         \
