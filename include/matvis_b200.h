@@ -146,7 +146,7 @@ int mvb_exptau(const double *antpos, int A, double freq, const double *crd, int6
                void *exptau, int out_c128, void *stream);
 /* Z panel layout (modes MVB_GEMM_*): 2P planes (plane 2p + c holds split term
  * p of component c, c = 0 real, 1 imaginary), each k-blocked as
- * [Kcap / KB][Mpad][KB] with KB = 32 bytes of elements (16 for bf16 / fp16, 8
+ * [Kcap / KB][Mpad][KB] with KB = 64 bytes of elements (32 for bf16 / fp16, 16
  * for tf32): element (m, k) of a plane is at (k / KB) * Mpad * KB + m * KB + k % KB.
  * Mpad is a multiple of 128, Kcap of 64.  Bytes: 2P x Mpad x Kcap x element size. */
 size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap);

@@ -180,9 +180,9 @@ def zpanel_dtype(mode: int) -> torch.dtype:
 
 
 def zpanel_kblock(mode: int) -> int:
-    """Elements per 32-byte k-block of a split-plane panel (planes are stored
+    """Elements per 64-byte k-block of a split-plane panel (planes are stored
     [Kcap / KB][Mpad][KB])."""
-    return 32 // torch.empty((), dtype=zpanel_dtype(mode)).element_size()
+    return 64 // torch.empty((), dtype=zpanel_dtype(mode)).element_size()
 
 
 def zpanel_planes(mode: int) -> int:

@@ -55,10 +55,11 @@ __host__ __device__ inline int mode_terms(int mode) { return mode == MVB_GEMM_BF
 __host__ __device__ inline int mode_elem_bytes(int mode) { return mode == MVB_GEMM_TF32_3 ? 4 : 2; }
 
 // Split-plane panel layout: each plane is stored k-blocked, [Kcap / KB][Mpad][KB]
-// with KB = 32 bytes of elements (16 bf16 / fp16, 8 tf32), so the 128-row x
-// 32-byte box one k-step of the Hermitian product loads is one contiguous 4 KB
-// run of HBM (a row-major plane would scatter it over 128 DRAM pages).
-constexpr int kKBlockBytes = 32;
+// with KB = 64 bytes of elements (32 bf16 / fp16, 16 tf32), so the 128-row x
+// 64-byte box of one Hermitian-product stage (two k-steps) is one contiguous
+// 8 KB run of HBM (a row-major plane would scatter it over 128 DRAM pages), and
+// each of its rows is one 64-byte request.
+constexpr int kKBlockBytes = 64;
 __host__ __device__ inline int64_t panel_off(int64_t m, int64_t k, int64_t Mpad, int kb) {
   return (k / kb) * (Mpad * kb) + m * kb + (k % kb);
 }
@@ -209,6 +210,18 @@ __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.
 
 // Shared-memory matrix descriptor (tcgen05 / UMMA), K-major, 32-byte swizzle:
 // 8-row core-matrix groups of 8 x 32 B, SBO = 256 B between groups.
+// K-major, 64-byte swizzle: rows of 64 bytes, 8-row core-matrix groups of
+// 512 B (SBO); the second 32-byte k-step of a row is the start address + 32 B.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((smem_addr & 0x3FFFF) >> 4);  // start address  [0, 14)
+  d |= static_cast<uint64_t>(1) << 16;                      // LBO (unused)   [16, 30)
+  d |= static_cast<uint64_t>(512 >> 4) << 32;               // SBO            [32, 46)
+  d |= static_cast<uint64_t>(1) << 46;                      // version = 1    [46, 48)
+  d |= static_cast<uint64_t>(4) << 61;                      // SWIZZLE_64B    [61, 64)
+  return d;
+}
+
 __device__ __forceinline__ uint64_t umma_desc_sw32(uint32_t smem_addr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((smem_addr & 0x3FFFF) >> 4);  // start address  [0, 14)

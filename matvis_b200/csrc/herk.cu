@@ -17,8 +17,8 @@
 //
 // Accuracy.  The tensor core rounds its FP32 accumulator toward zero at every
 // UMMA, so a long in-TMEM sum drifts by about one ulp per instruction (3e-5
-// relative after 2,048 columns).  Each k-step (one 32-byte column block) is
-// therefore accumulated into a FRESH TMEM block, products in ascending order of
+// relative after 2,048 columns).  Each group of KD k-steps (32-byte column
+// blocks) is therefore accumulated into a FRESH TMEM block, products in ascending order of
 // magnitude -- BF16_6 {11, 02, 20, 01, 10, 00}, BF16_3 / TF32_3 {01, 10, 00} -- so
 // only the final hi x hi UMMAs round at full magnitude, and the block is drained
 // by the epilogue warps into FP32 registers with round-to-nearest adds.  One
@@ -29,8 +29,10 @@
 // together read the same Z columns (L2 reuse).  Persistent CTAs (one per SM,
 // 192 KB of shared memory) loop over units.  Warp roles (576 threads):
 //   warp 0 lane 0 : TMA producer, one 4-D box per operand per stage (all 2P
-//                   split/component planes of 128 rows x 32 bytes, one k-block of
-//                   the k-blocked panel, SWIZZLE_32B);
+//                   split/component planes of 128 rows x 64 bytes, one k-block of
+//                   the k-blocked panel = two k-steps, SWIZZLE_64B; 64-byte rows
+//                   halve the TMA row requests per byte against 32-byte ones,
+//                   which bounded the kernel);
 //   warp 1        : TMEM owner (512 columns = two k-step blocks); lane 0 issues
 //                   the UMMAs and tcgen05.commit's the stage / block barriers;
 //   warps 2..17   : epilogue; warp w drains TMEM lane quadrant (w % 4), column
@@ -57,7 +59,7 @@ constexpr int kPlanExtra = 32;  // extra k-slices the split planner may add to f
 constexpr int kHerkThreads = 64 + 32 * kEpiWarps;
 constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s
 constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
-constexpr int kPlaneBytes = 128 * 32;              // one 128-row x 32-byte plane tile
+constexpr int kPlaneBytes = 128 * 64;              // one 128-row x 64-byte plane tile (two k-steps)
 constexpr int kSmemBudget = 192 * 1024;
 
 template <int MODE>
@@ -65,7 +67,8 @@ struct HerkCfg {
   static constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
   static constexpr int ES = MODE == MVB_GEMM_TF32_3 ? 4 : 2;
   static constexpr int KSTEP = 32 / ES;  // elements per 32-byte k-step (= UMMA K)
-  static_assert(KSTEP * ES == kKBlockBytes, "one k-step is one k-block of the panel");
+  static constexpr int KB = 64 / ES;     // elements per 64-byte k-block: one stage, two k-steps
+  static_assert(KB * ES == kKBlockBytes, "one stage is one k-block of the panel");
   static constexpr int OPER_BYTES = 2 * P * kPlaneBytes;
   static constexpr int STAGE_BYTES = 2 * OPER_BYTES;
   static constexpr int STAGES = kSmemBudget / STAGE_BYTES;
@@ -201,10 +204,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       decode_tile(t, T, I, J);
       const int64_t k0 = (int64_t)s * kc;
       const int64_t klen = min(kc, kvalid - k0);
-      const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
+      const int nkb = (int)((klen + C::KB - 1) / C::KB);
       const bool diag = I == J;
       const uint32_t bytes = diag ? C::OPER_BYTES : 2 * C::OPER_BYTES;
-      for (int ks = 0; ks < nks; ++ks) {
+      for (int kbi = 0; kbi < nkb; ++kbi) {
         if (!mbar_wait(&empty_bar[st], ph ^ 1, kWaitLimitNs)) {
           atomicOr(status, MVB_DEV_TIMEOUT);
           abort_flag = 1;
@@ -212,8 +215,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         }
         mbar_arrive_expect_tx(&full_bar[st], bytes);
         uint8_t *a = smem + (size_t)st * C::STAGE_BYTES;
-        // k-block index: k0 is a multiple of 64 and each k-step is one 32-byte block
-        const int kb = (int)((k0 + (int64_t)ks * C::KSTEP) / C::KSTEP);
+        // k-block index: k0 is a multiple of 64 elements, a k-block 64 bytes
+        const int kb = (int)((k0 + (int64_t)kbi * C::KB) / C::KB);
         tma_load_4d(a, &zmap, &full_bar[st], 0, I * 128, kb, 0);
         if (!diag) tma_load_4d(a + C::OPER_BYTES, &zmap, &full_bar[st], 0, J * 128, kb, 0);
         ++issued;
@@ -235,45 +238,51 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
       bool ok = true;
-      for (int g0 = 0; g0 < nks && ok; g0 += KD) {
-        // one TMEM block per group of KD k-steps
-        if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, kWaitLimitNs)) {
-          ok = false;
-          break;
+      // k-steps in order; a TMEM block holds KD of them, a stage (one 64-byte
+      // k-block) two: the block and stage boundaries are independent
+      for (int ks = 0; ks < nks; ++ks) {
+        if (ks % KD == 0) {  // a fresh TMEM block
+          if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, kWaitLimitNs)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
         }
-        tc_fence_after();
-        const uint32_t d = tbase + buf * 256;
-        const int gl = min(KD, nks - g0);
-        for (int kk = 0; kk < gl; ++kk) {
+        if ((ks & 1) == 0) {  // a new stage
           if (!mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a_base = smem_u32(smem + (size_t)st * C::STAGE_BYTES);
-          const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
+        }
+        const uint32_t d = tbase + buf * 256;
+        const uint32_t koff = (uint32_t)(ks & 1) * 32;  // the k-step's 32 bytes within the 64-byte rows
+        const uint32_t a_base = smem_u32(smem + (size_t)st * C::STAGE_BYTES) + koff;
+        const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
 #pragma unroll
-          for (int q = 0; q < C::NPROD; ++q) {
-            uint32_t pa, pb;
-            product_terms(C::NPROD, q, pa, pb);
-            const uint64_t a_re = umma_desc_sw32(a_base + (2 * pa) * kPlaneBytes);
-            const uint64_t a_im = umma_desc_sw32(a_base + (2 * pa + 1) * kPlaneBytes);
-            const uint64_t b_re = umma_desc_sw32(b_base + (2 * pb) * kPlaneBytes);
-            const uint64_t b_im = umma_desc_sw32(b_base + (2 * pb + 1) * kPlaneBytes);
-            umma<MODE>(d, a_re, b_re, C::ID256, (kk > 0 || q > 0) ? 1u : 0u);
-            umma<MODE>(d, a_im, b_im, C::ID128, 1u);
-            umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
-          }
+        for (int q = 0; q < C::NPROD; ++q) {
+          uint32_t pa, pb;
+          product_terms(C::NPROD, q, pa, pb);
+          const uint64_t a_re = umma_desc_sw64(a_base + (2 * pa) * kPlaneBytes);
+          const uint64_t a_im = umma_desc_sw64(a_base + (2 * pa + 1) * kPlaneBytes);
+          const uint64_t b_re = umma_desc_sw64(b_base + (2 * pb) * kPlaneBytes);
+          const uint64_t b_im = umma_desc_sw64(b_base + (2 * pb + 1) * kPlaneBytes);
+          umma<MODE>(d, a_re, b_re, C::ID256, (ks % KD != 0 || q > 0) ? 1u : 0u);
+          umma<MODE>(d, a_im, b_im, C::ID128, 1u);
+          umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+        }
+        if ((ks & 1) == 1 || ks == nks - 1) {  // the stage is consumed
           tc_commit(&empty_bar[st]);
           if (++st == C::STAGES) {
             st = 0;
             ph ^= 1;
           }
         }
-        if (!ok) break;
-        tc_commit(&dfull_bar[buf]);
-        dph ^= 1u << buf;
-        buf ^= 1u;
+        if (ks % KD == KD - 1 || ks == nks - 1) {  // the block is complete
+          tc_commit(&dfull_bar[buf]);
+          dph ^= 1u << buf;
+          buf ^= 1u;
+        }
       }
       if (!ok) {
         atomicOr(status, MVB_DEV_TIMEOUT);
@@ -523,19 +532,19 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   auto enc = tensor_map_encoder();
   if (!enc) return fail(MVB_ERR_UNSUPPORTED, "mvb_herk: cuTensorMapEncodeTiled unavailable");
   CUtensorMap map;
-  // k-blocked planes [2P][Kcap / KSTEP][Mpad][KSTEP]: one k-step of 128 rows is a
-  // contiguous 4 KB run per plane; the box lands in shared memory as
-  // [plane][row][32 bytes], the layout of the row-major map it replaces.
-  cuuint64_t dims[4] = {(cuuint64_t)C::KSTEP, (cuuint64_t)Mpad, (cuuint64_t)(Kcap / C::KSTEP), (cuuint64_t)(2 * C::P)};
+  // k-blocked planes [2P][Kcap / KB][Mpad][KB]: one stage of 128 rows is a
+  // contiguous 8 KB run per plane; the box lands in shared memory as
+  // [plane][row][64 bytes], 64-byte swizzled (the UMMA descriptors' layout).
+  cuuint64_t dims[4] = {(cuuint64_t)C::KB, (cuuint64_t)Mpad, (cuuint64_t)(Kcap / C::KB), (cuuint64_t)(2 * C::P)};
   cuuint64_t strides[3] = {(cuuint64_t)kKBlockBytes, (cuuint64_t)Mpad * kKBlockBytes, (cuuint64_t)Mpad * Kcap * C::ES};
-  cuuint32_t box[4] = {(cuuint32_t)C::KSTEP, 128u, 1u, (cuuint32_t)(2 * C::P)};
+  cuuint32_t box[4] = {(cuuint32_t)C::KB, 128u, 1u, (cuuint32_t)(2 * C::P)};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUtensorMapDataType dt = MODE == MVB_GEMM_TF32_3  ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : MODE == MVB_GEMM_F16_3 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                           : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   CUresult r = enc(&map, dt, 4,
                    const_cast<void *>(z), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(MVB_ERR_CUDA, "mvb_herk: cuTensorMapEncodeTiled failed (%d)", (int)r);
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;

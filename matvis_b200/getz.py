@@ -19,8 +19,9 @@ class ZPanel:
     """Device Z in split-plane (or plain complex64) layout.
 
     ``data``: (planes, Kcap / KB, Mpad, KB) for the tensor-core modes -- each
-    plane k-blocked in 32-byte blocks of KB elements, so that one k-step of 128
-    rows is contiguous in HBM -- and (M, Kcap) complex64 for the plain mode.
+    plane k-blocked in 64-byte blocks of KB elements, so that one stage of the
+    Hermitian product (128 rows, two k-steps) is contiguous in HBM -- and
+    (M, Kcap) complex64 for the plain mode.
     ``n_dev`` / ``n_host`` give the valid source count; the valid K extent is
     that count times ``nax``.
     """

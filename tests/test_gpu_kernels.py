@@ -18,6 +18,7 @@ torch = pytest.importorskip("torch")
 
 import matvis_b200 as mv  # noqa: E402
 from matvis_b200 import _lib  # noqa: E402
+from matvis_b200 import workloads  # noqa: E402
 from oracle import oracle as orc  # noqa: E402
 
 from .conftest import golden  # noqa: E402
@@ -103,7 +104,7 @@ def test_bilinear_wrong_dtype(device):
 
 def test_beam_interpolator_enu_matches_oracle(device):
     rng = np.random.default_rng(3)
-    beams = mv.workloads.dipole_beams(rng, 2, dgrid_deg=2.0)
+    beams = workloads.dipole_beams(rng, 2, dgrid_deg=2.0)
     n = 5000
     e = rng.uniform(-0.7, 0.7, n)
     nn = rng.uniform(-0.7, 0.7, n)
