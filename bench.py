@@ -338,10 +338,10 @@ def run_b200(args, rank, world, local_rank):
     achieved = algo_flops / (herk_ms / 1000.0) / 1e12
     tensor_peak = bf16_peak / 2 if args.gemm_mode.startswith("tf32") else bf16_peak
     # DRAM bytes per launch from an ncu capture (dram__bytes_read/write.sum) of the
-    # nside-64 slice of this workload (K = 49,152, k_chunk 4096: 312.3 MB read, 57.7 MB
+    # nside-64 slice of this workload (K = 49,152, k_chunk 4096: 305.8 MB read, 24.4 MB
     # written over 12 x 21 work units), scaled by the columns read and the units written
     n_units = (T * (T + 1) // 2) * -(-kvalid // kc)
-    traffic = 312.251904e6 / 49152 * kvalid + 57.691904e6 / 252 * n_units
+    traffic = 305.779968e6 / 49152 * kvalid + 24.417536e6 / 252 * n_units
     roofline = {
         "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
         "traffic": traffic, "traffic_source": "ncu dram bytes of the nside-64 slice, scaled by columns and units",

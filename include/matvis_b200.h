@@ -196,7 +196,7 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
 /* Upper-triangle 128 x 128 complex tiles of V = conj(Z) Z^T over K_valid
  * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05
  * tensor cores with TMEM accumulators, fed by TMA (cp.async.bulk.tensor,
- * 32-byte swizzle); mode MVB_GEMM_* selects the split precision.
+ * 64-byte swizzle over the 64-byte k-blocks); mode MVB_GEMM_* selects the split precision.
  * drain_ksteps (1, 2 or 4; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
  * number of 32-byte k-steps summed in one TMEM block before the block is added
  * to FP32 registers: the tensor core rounds its accumulator toward zero at every
