@@ -2,6 +2,12 @@
 """Headline benchmark: antenna-pair x source terms/s on the HERA-350-like workload.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+                    [--config 2|3|4 [--sparse] [--nsrc N --nfreq F --ntimes T]]
+
+--config 3 is the precision form (1,000,000 isotropic power-law sources, one
+slice per job by default; --sparse times its 5,000 seeded pairs on the
+VectorDot path), --config 4 the batched form (500,000 sources, 256 frequencies
+x 64 LSTs over 6 h).  Without --config:
 
 Workload (one "step"): the whole config-2 job -- 350 antennas (320 on a 14.6 m
 hexagon + 30 outriggers), 196,608 sources (nside = 128 equal-area centres,
@@ -61,9 +67,13 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--gemm-mode", default="fp16x3", choices=sorted(GEMM_PRECISION))
     ap.add_argument("--k-chunk", type=int, default=None)
-    ap.add_argument("--nfreq", type=int, default=64)
-    ap.add_argument("--ntimes", type=int, default=16)
-    ap.add_argument("--nside", type=int, default=128, help="sky pixelisation (128: 196,608 sources)")
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
+                    help="2: HERA-350-like job (default); 3: 1e6 power-law sources; 4: 500k sources, 256 f x 64 LST")
+    ap.add_argument("--sparse", action="store_true", help="config 3: the 5,000 seeded pairs on the VectorDot path")
+    ap.add_argument("--nsrc", type=int, default=None, help="source count (configs 3 and 4)")
+    ap.add_argument("--nfreq", type=int, default=None, help="default 64 (config 2), 1 (config 3), 256 (config 4)")
+    ap.add_argument("--ntimes", type=int, default=None, help="default 16 (config 2), 1 (config 3), 64 (config 4)")
+    ap.add_argument("--nside", type=int, default=128, help="config-2 sky pixelisation (128: 196,608 sources)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
@@ -124,8 +134,34 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def load_config(args) -> tuple[dict, str]:
+    """The workload named by --config, with its description."""
+    from matvis_b200 import workloads as wl
+
+    if args.config == 2:
+        cfg = wl.config2(nfreq=args.nfreq or 64, ntimes=args.ntimes or 16, nside=args.nside)
+        desc = (f"config2 HERA-350-like: 350 ant x {len(cfg['ra'])} src x {len(cfg['freqs'])} freq x "
+                f"{len(cfg['lsts'])} LST, polarised 2x2, 4 gridded beams + beam_idx; one job per step")
+    elif args.config == 3:
+        cfg = wl.config3(nsrc=args.nsrc or 1_000_000, nfreq=args.nfreq or 1, ntimes=args.ntimes or 1)
+        if not args.sparse:
+            cfg["antpairs"] = None
+        desc = (f"config3: 350 ant x {len(cfg['ra'])} isotropic power-law src x {len(cfg['freqs'])} freq x "
+                f"{len(cfg['lsts'])} LST, polarised 2x2, 4 gridded beams; "
+                + (f"{len(cfg['antpairs'])} seeded pairs on the VectorDot path" if args.sparse else "all pairs")
+                + "; one job per step")
+    else:
+        cfg = wl.config4(nsrc=args.nsrc or 500_000, nfreq=args.nfreq or 256, ntimes=args.ntimes or 64)
+        desc = (f"config4: 350 ant x {len(cfg['ra'])} isotropic power-law src x {len(cfg['freqs'])} freq x "
+                f"{len(cfg['lsts'])} LST over 6 h, polarised 2x2, 4 gridded beams; one job per step")
+    if args.sparse and args.config != 3:
+        raise SystemExit("--sparse applies to config 3")
+    return cfg, desc
+
+
 def terms_per_job(cfg) -> tuple[float, np.ndarray]:
-    """Nant^2 * sum_t n_t * Nf, with n_t from the same FP64 fixed-order rotation as the kernels."""
+    """Npairs * sum_t n_t * Nf (Npairs = Nant^2, or the listed pairs), with n_t from
+    the same FP64 fixed-order rotation as the kernels."""
     from matvis_b200.coordinates import eci_to_enu_matrix, point_source_crd_eq
 
     eci = point_source_crd_eq(cfg["ra"], cfg["dec"])
@@ -135,7 +171,8 @@ def terms_per_job(cfg) -> tuple[float, np.ndarray]:
         z = (R[2, 0] * eci[0] + R[2, 1] * eci[1]) + R[2, 2] * eci[2]
         counts.append(int((z > 0).sum()))
     nant = len(cfg["antpos"])
-    return float(nant * nant * sum(counts) * len(cfg["freqs"])), np.array(counts)
+    npairs = nant * nant if cfg.get("antpairs") is None else len(cfg["antpairs"])
+    return float(npairs * sum(counts) * len(cfg["freqs"])), np.array(counts)
 
 
 # ----------------------------------------------------------------------------- plain GPU path
@@ -143,7 +180,8 @@ def plain_gpu_sample(cfg, nslices: int = 6):
     """Complex64 torch restatement of the reference GPU driver (gpu/gpu.py:197-254) on
     `nslices` (f, t) slices: FP32 rotation, horizon gather with a host count,
     bilinear beam via grid_sample, FP32 phase, per-antenna Z loop, full complex64
-    matmul (TF32 off), device->host copy of the full matrix per slice."""
+    matmul (TF32 off) or, for a pair list, one matmul per pair (GPUVectorDot,
+    gpu/matprod.py:66-98), device->host copy of the result per slice."""
     import torch
     import torch.nn.functional as Fnn
 
@@ -157,6 +195,8 @@ def plain_gpu_sample(cfg, nslices: int = 6):
     grids = torch.as_tensor(np.stack([b.data for b in beams]), dtype=torch.complex64, device=dev)  # B,X,F,za,az
     bidx = np.asarray(cfg["beam_idx"])
     nant = len(cfg["antpos"])
+    pairs = None if cfg.get("antpairs") is None else [(int(i), int(j)) for i, j in cfg["antpairs"]]
+    npairs = nant * nant if pairs is None else len(pairs)
     nb, X, F, nza, naz = grids.shape
     flux = torch.as_tensor(np.sqrt(0.5 * cfg["fluxes"]), dtype=torch.float32, device=dev)
     terms = 0.0
@@ -186,13 +226,17 @@ def plain_gpu_sample(cfg, nslices: int = 6):
         for a in range(nant):  # per-antenna loop of core/getz.py:95-96
             z[a] *= beam[int(bidx[a])]
         z = z.reshape(nant * F, X * n)
-        v = z.conj() @ z.T
+        if pairs is None:
+            v = z.conj() @ z.T
+        else:
+            zz = z.view(nant, F, X * n)
+            v = torch.stack([zz[aj] @ zz[ai].conj().T for ai, aj in pairs])
         _ = v.cpu()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if k > 0:  # first slice is warm-up
             times.append(dt)
-            terms += nant * nant * n
+            terms += npairs * n
     return {"value": terms / sum(times), "unit": UNIT, "slices": nslices,
             "sample": f"{nslices} (f, t) slices of the workload, complex64, TF32 off"}
 
@@ -205,6 +249,7 @@ def cpu_oracle_sample(cfg, nsrc_sample: int, nslices: int = 1):
     from matvis_b200 import workloads as wl
 
     sub = wl.subset(cfg, nsrc=nsrc_sample, nfreq=1, ntimes=1, seed=11)
+    sub["antpairs"] = None  # the oracle computes all pairs; the count below uses all of them
     beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in sub["beams"]]
     antpos = np.asarray(sub["antpos"])
     terms = 0.0
@@ -228,8 +273,10 @@ def run_reference(args, rank, world):
         return
     from matvis_b200 import workloads as wl
 
-    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes, nside=args.nside)
-    nsrc_sample = len(cfg["ra"])  # one full (f, t) slice per step (a few seconds on the host cores)
+    cfg, desc = load_config(args)
+    # one (f, t) slice per step: all sources of config 2 (a few seconds on the host
+    # cores), a 196,608-source seeded subset of the larger skies
+    nsrc_sample = min(len(cfg["ra"]), 196_608)
     for _ in range(max(args.warmup, 0)):
         cpu_oracle_sample(cfg, nsrc_sample)
     vals, dts = [], []
@@ -243,14 +290,108 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.median(dts)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "config2 HERA-350-like (350 ant, 196608 src, 64 f x 16 LST, polarised, 4 beams)",
-                   "sample": sample},
+        "config": {"workload": desc, "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference package not importable here (astropy, pyuvdata absent); its CPU algorithm is timed "
                 "through the FP64 oracle restatement (oracle/oracle.py), pinned to fixtures from the reference code",
     }
     print(json.dumps(line), flush=True)
+
+
+def herk_roofline(eng, args, dev) -> dict:
+    """mvb_herk on the engine's last panel: algorithmic flops 4 M (M+1) K per launch."""
+    import torch
+
+    from matvis_b200 import _lib
+
+    panel = eng.zcalc.z
+    M = eng.nant * eng.nfeed
+    nlast = int(eng.n_above.item())
+    kvalid = nlast * eng.nax
+    kc = eng.k_chunk
+    reps = 10
+    hs = torch.cuda.Stream(device=dev)
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ws = eng.matprod.workspace(panel, kc)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(hs):
+        for r in range(reps + 2):
+            if r == 2:
+                h0.record(hs)
+            _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), eng.matprod.mode, panel.Mpad, panel.Kcap,
+                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, 0, _lib.ptr(ws), ws.numel(),
+                                         _lib.ptr(eng.status), _lib.stream_handle(hs)))
+        h1.record(hs)
+    torch.cuda.synchronize()
+    herk_ms = h0.elapsed_time(h1) / reps
+    algo_flops = 4.0 * M * (M + 1) * kvalid
+    T = panel.Mpad // 128
+    nprod = _lib.GEMM_PRODUCTS[_lib.GEMM_MODES[args.gemm_mode]]
+    exec_flops = 8.0 * (T * (T + 1) // 2) * 128 * 128 * kvalid * nprod
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
+    achieved = algo_flops / (herk_ms / 1000.0) / 1e12
+    tensor_peak = bf16_peak / 2 if args.gemm_mode.startswith("tf32") else bf16_peak
+    # DRAM bytes per launch from an ncu capture (dram__bytes_read/write.sum) of the
+    # nside-64 slice of this workload (K = 49,152, k_chunk 4096: 305.8 MB read, 24.4 MB
+    # written over 12 x 21 work units), scaled by the columns read and the units written
+    # (fp16x3: 4 planes x 2 B per row and column; other modes scale the panel read by their plane bytes)
+    n_units = (T * (T + 1) // 2) * -(-kvalid // kc)
+    plane_bytes = 2 * (3 if args.gemm_mode == "bf16x6" else 2) * (4 if args.gemm_mode.startswith("tf32") else 2)
+    traffic = 305.779968e6 / 49152 * kvalid * plane_bytes / 8 + 24.417536e6 / 252 * n_units
+    roofline = {
+        "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
+        "traffic": traffic,
+        "traffic_source": "ncu dram bytes of the nside-64 fp16x3 slice, scaled by columns, units and plane bytes",
+        "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
+        "kernel": f"mvb_herk {args.gemm_mode}: M={M}, K={kvalid}, k_chunk={kc}",
+        "herk_ms": herk_ms,
+        "algorithmic_flops_per_launch": algo_flops,
+        "executed_tensor_tflops": exec_flops / (herk_ms / 1000.0) / 1e12,
+        "executed_tensor_frac": exec_flops / (herk_ms / 1000.0) / 1e12 / tensor_peak,
+    }
+    return roofline
+
+
+def vecdot_roofline(eng, dev) -> dict:
+    """mvb_vecdot (+ its slice reduction) on the engine's last panel.  Algorithmic
+    bytes per launch: the Z rows of the antennas in the pair list read once
+    (F rows x K x 8 B each) plus the FP64 slice partials written and read."""
+    import torch
+
+    from matvis_b200 import _lib
+
+    panel = eng.zcalc.z
+    mp = eng.matprod
+    kvalid = int(eng.n_above.item()) * eng.nax
+    reps = 10
+    out = torch.empty_like(eng.vis[0, 0])
+    hs = torch.cuda.Stream(device=dev)
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(hs):
+        for r in range(reps + 2):
+            if r == 2:
+                h0.record(hs)
+            mp.enqueue(panel, out, accumulate=False, stream=hs)
+        h1.record(hs)
+    torch.cuda.synchronize()
+    ms = h0.elapsed_time(h1) / reps
+    pairs = np.asarray(mp.antpairs)
+    nrows = len(np.unique(pairs)) * eng.nfeed
+    nsplit = -(-kvalid // mp.k_chunk)
+    algo_bytes = nrows * kvalid * 8.0 + 2 * nsplit * len(pairs) * eng.nfeed ** 2 * 16.0
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo_bytes / (ms / 1000.0) / 1e9
+    return {
+        "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+        "peak_source": ("measured" if "hbm_gbs" in peaks else "fallback") + " HBM copy (MEASURED_PEAKS.json)",
+        "kernel": f"mvb_vecdot: {len(pairs)} pairs, F={eng.nfeed}, K={kvalid}, k_chunk={mp.k_chunk}",
+        "vecdot_ms": ms, "algorithmic_bytes_per_launch": algo_bytes,
+    }
 
 
 # ----------------------------------------------------------------------------- B200 arm
@@ -268,11 +409,13 @@ def run_b200(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
 
-    cfg = wl.config2(nfreq=args.nfreq, ntimes=args.ntimes, nside=args.nside)
+    cfg, desc = load_config(args)
     terms, counts = terms_per_job(cfg)
+    matprod = "VectorDot" if args.sparse else "MatMul"
     spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
                            lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
-                           polarized=True, precision=1, gemm_mode=args.gemm_mode, k_chunk=args.k_chunk)
+                           polarized=True, precision=1, gemm_mode=args.gemm_mode, k_chunk=args.k_chunk,
+                           antpairs=cfg["antpairs"], matprod=matprod)
     eng = VisEngine(spec, device=dev)
     eng.upload()
     eng.run()  # uncaptured run: checks status, warms caches
@@ -307,69 +450,36 @@ def run_b200(args, rank, world, local_rank):
     ms_max = float(ms_t.item())
     value = world * terms / (ms_max / 1000.0)
 
-    # ---- roofline of the dominant kernel: mvb_herk on the last slice's panel
-    panel = eng.zcalc.z
-    M = eng.nant * eng.nfeed
-    nlast = int(eng.n_above.item())
-    kvalid = nlast * eng.nax
-    kc = eng.k_chunk
-    reps = 10
-    hs = torch.cuda.Stream(device=dev)
-    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ws = eng.matprod.workspace(panel, kc)
-    torch.cuda.synchronize()
-    with torch.cuda.stream(hs):
-        for r in range(reps + 2):
-            if r == 2:
-                h0.record(hs)
-            _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), eng.matprod.mode, panel.Mpad, panel.Kcap,
-                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, 0, _lib.ptr(ws), ws.numel(),
-                                         _lib.ptr(eng.status), _lib.stream_handle(hs)))
-        h1.record(hs)
-    torch.cuda.synchronize()
-    herk_ms = h0.elapsed_time(h1) / reps
-    algo_flops = 4.0 * M * (M + 1) * kvalid
-    T = panel.Mpad // 128
-    nprod = _lib.GEMM_PRODUCTS[_lib.GEMM_MODES[args.gemm_mode]]
-    exec_flops = 8.0 * (T * (T + 1) // 2) * 128 * 128 * kvalid * nprod
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    bf16_peak = peaks.get("bf16_tflops", 1590.0)
-    peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
-    achieved = algo_flops / (herk_ms / 1000.0) / 1e12
-    tensor_peak = bf16_peak / 2 if args.gemm_mode.startswith("tf32") else bf16_peak
-    # DRAM bytes per launch from an ncu capture (dram__bytes_read/write.sum) of the
-    # nside-64 slice of this workload (K = 49,152, k_chunk 4096: 305.8 MB read, 24.4 MB
-    # written over 12 x 21 work units), scaled by the columns read and the units written
-    n_units = (T * (T + 1) // 2) * -(-kvalid // kc)
-    traffic = 305.779968e6 / 49152 * kvalid + 24.417536e6 / 252 * n_units
-    roofline = {
-        "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
-        "traffic": traffic, "traffic_source": "ncu dram bytes of the nside-64 slice, scaled by columns and units",
-        "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
-        "kernel": f"mvb_herk {args.gemm_mode}: M={M}, K={kvalid}, k_chunk={kc}",
-        "herk_ms": herk_ms,
-        "algorithmic_flops_per_launch": algo_flops,
-        "executed_tensor_tflops": exec_flops / (herk_ms / 1000.0) / 1e12,
-        "executed_tensor_frac": exec_flops / (herk_ms / 1000.0) / 1e12 / tensor_peak,
-    }
+    # ---- roofline of the dominant kernel, timed on its own stream over the last slice's panel
+    roofline = vecdot_roofline(eng, dev) if args.sparse else herk_roofline(eng, args, dev)
 
+    panel = eng.zcalc.z
+    kvalid = int(eng.n_above.item()) * eng.nax
+    if args.sparse:
+        dtype, kc = "f32", eng.matprod.k_chunk
+        product = ("complex64 Z, FP32 per-pair sums (mvb_vecdot), FP64 warp and slice sums")
+    else:
+        dtype = {"fp16x3": "fp16", "bf16x6": "bf16", "bf16x3": "bf16", "tf32x3": "tf32"}[args.gemm_mode]
+        kc = eng.k_chunk
+        product = (GEMM_PRECISION[args.gemm_mode] + " tcgen05 Hermitian product, FP32 register sums per drained "
+                   "TMEM block, FP64 slice sums")
+    sky = ("HEALPix nside=%d centres, lognormal flux" % args.nside if args.config == 2
+           else "isotropic sources, power-law flux")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"fp16x3": "fp16", "bf16x6": "bf16", "bf16x3": "bf16", "tf32x3": "tf32"}[args.gemm_mode],
-        "data": "synthetic (seeded; HEALPix nside=128 centres, HERA-350-like array, dipole-like beams)",
+        "dtype": dtype,
+        "data": f"synthetic (seeded; {sky}, HERA-350-like array, dipole-like beams)",
         "config": {
-            "workload": f"config2 HERA-350-like: 350 ant x {len(cfg['ra'])} src x {len(cfg['freqs'])} freq x "
-                        f"{len(cfg['lsts'])} LST, polarised 2x2, 4 gridded beams + beam_idx; one job per step",
-            "gemm_mode": args.gemm_mode, "k_chunk": kc, "terms_per_job": terms,
+            "workload": desc,
+            "matprod": matprod, "gemm_mode": None if args.sparse else args.gemm_mode, "k_chunk": kc,
+            "terms_per_job": terms,
             "above_horizon_per_time": [int(c) for c in counts],
             "l2": "inputs larger than L2 (Z panel ~%.1f GB per slice)" % (panel.data.numel() *
                                                                           panel.data.element_size() / 1e9 * kvalid /
                                                                           panel.Kcap),
             "parallelism": "replicas (one job per GPU)" if world > 1 else "1 GPU",
-            "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, "
-                         + GEMM_PRECISION[args.gemm_mode]
-                         + " tcgen05 Hermitian product, FP32 register sums per drained TMEM block, FP64 slice sums",
+            "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, " + product,
         },
         "roofline": roofline,
         "gpu_launches": eng.launches_per_run() * args.steps,
@@ -377,8 +487,9 @@ def run_b200(args, rank, world, local_rank):
     }
 
     if rank == 0 and world == 1 and not args.skip_cpu:
-        # three full (f, t) slices: about 10 s of FP64 work on the host cores
-        v, dt, sample = cpu_oracle_sample(cfg, len(cfg["ra"]), nslices=3)
+        # three (f, t) slices: about 10 s of FP64 work on the host cores (all sources of
+        # config 2, a 196,608-source seeded subset of the larger skies)
+        v, dt, sample = cpu_oracle_sample(cfg, min(len(cfg["ra"]), 196_608), nslices=3)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample,
                                 "seconds": dt}
     if rank == 0 and not args.skip_plain:
@@ -391,7 +502,7 @@ def run_b200(args, rank, world, local_rank):
     if not args.skip_e2e:
         ants = {i: tuple(p) for i, p in enumerate(cfg["antpos"])}
         kw = dict(polarized=True, precision=1, beam_idx=cfg["beam_idx"], gemm_mode=args.gemm_mode,
-                  k_chunk=args.k_chunk, device=dev)
+                  k_chunk=args.k_chunk, device=dev, antpairs=cfg["antpairs"], matprod_method=matprod)
         mv.simulate_vis(ants, cfg["fluxes"], cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
                         cfg["latitude"], **kw)
         barrier()
