@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
                     help="2: HERA-350-like job (default); 3: 1e6 power-law sources; 4: 500k sources, 256 f x 64 LST")
     ap.add_argument("--sparse", action="store_true", help="config 3: the 5,000 seeded pairs on the VectorDot path")
+    ap.add_argument("--pair-kernel", default="auto", choices=["auto", "vecdot", "herk"],
+                    help="--sparse: per-pair sums, the Hermitian product with a pair gather, or the cost model's choice")
     ap.add_argument("--nsrc", type=int, default=None, help="source count (configs 3 and 4)")
     ap.add_argument("--nfreq", type=int, default=None, help="default 64 (config 2), 1 (config 3), 256 (config 4)")
     ap.add_argument("--ntimes", type=int, default=None, help="default 16 (config 2), 1 (config 3), 64 (config 4)")
@@ -415,7 +417,7 @@ def run_b200(args, rank, world, local_rank):
     spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
                            lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
                            polarized=True, precision=1, gemm_mode=args.gemm_mode, k_chunk=args.k_chunk,
-                           antpairs=cfg["antpairs"], matprod=matprod)
+                           antpairs=cfg["antpairs"], matprod=matprod, pair_product=args.pair_kernel)
     eng = VisEngine(spec, device=dev)
     eng.upload()
     eng.run()  # uncaptured run: checks status, warms caches
@@ -451,11 +453,11 @@ def run_b200(args, rank, world, local_rank):
     value = world * terms / (ms_max / 1000.0)
 
     # ---- roofline of the dominant kernel, timed on its own stream over the last slice's panel
-    roofline = vecdot_roofline(eng, dev) if args.sparse else herk_roofline(eng, args, dev)
+    roofline = vecdot_roofline(eng, dev) if eng.method == "VectorDot" else herk_roofline(eng, args, dev)
 
     panel = eng.zcalc.z
     kvalid = int(eng.n_above.item()) * eng.nax
-    if args.sparse:
+    if eng.method == "VectorDot":
         dtype, kc = "f32", eng.matprod.k_chunk
         product = ("complex64 Z, FP32 per-pair sums (mvb_vecdot), FP64 warp and slice sums")
     else:
@@ -472,7 +474,8 @@ def run_b200(args, rank, world, local_rank):
         "data": f"synthetic (seeded; {sky}, HERA-350-like array, dipole-like beams)",
         "config": {
             "workload": desc,
-            "matprod": matprod, "gemm_mode": None if args.sparse else args.gemm_mode, "k_chunk": kc,
+            "matprod": matprod, "pair_kernel": eng.pair_kernel,
+            "gemm_mode": None if eng.method == "VectorDot" else args.gemm_mode, "k_chunk": kc,
             "terms_per_job": terms,
             "above_horizon_per_time": [int(c) for c in counts],
             "l2": "inputs larger than L2 (Z panel ~%.1f GB per slice)" % (panel.data.numel() *
@@ -502,7 +505,8 @@ def run_b200(args, rank, world, local_rank):
     if not args.skip_e2e:
         ants = {i: tuple(p) for i, p in enumerate(cfg["antpos"])}
         kw = dict(polarized=True, precision=1, beam_idx=cfg["beam_idx"], gemm_mode=args.gemm_mode,
-                  k_chunk=args.k_chunk, device=dev, antpairs=cfg["antpairs"], matprod_method=matprod)
+                  k_chunk=args.k_chunk, device=dev, antpairs=cfg["antpairs"], matprod_method=matprod,
+                  pair_product=args.pair_kernel)
         mv.simulate_vis(ants, cfg["fluxes"], cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
                         cfg["latitude"], **kw)
         barrier()

@@ -35,7 +35,7 @@ from .coordinates import (
 )
 from .getz import ZMatrixCalc
 from .autotune import tune_k_chunk
-from .matprod import B200MatMul, B200VectorDot, choose_k_chunk
+from .matprod import B200MatMul, B200VectorDot, choose_k_chunk, pair_product
 
 #: k-slice of the Hermitian product without autotuning: the tuner's choice for
 #: the HERA-350-like slice in fp16x3 (product + reduction 1.36 ms at 4096
@@ -59,6 +59,8 @@ class JobSpec:
     precision: int = 1
     gemm_mode: str = "fp16x3"
     matprod: str = "MatMul"  # or "VectorDot"
+    #: kernel for a VectorDot pair list: "auto" (measured cost model), "vecdot" or "herk"
+    pair_product: str = "auto"
     k_chunk: int | None = None
     source_buffer: float = 1.0
     nchunks: int = 1
@@ -80,6 +82,24 @@ def _norm_matprod(name: str) -> str:
     if n in ("VectorDot", "VectorLoop"):
         return "VectorDot"
     raise ValueError(f"unknown matprod_method {name!r}")
+
+
+def _resolve_product(spec: JobSpec) -> tuple[str, str | None]:
+    """(kernel family, pair kernel): a VectorDot request runs on the Hermitian
+    product with a pair gather when ``pair_product`` says so (or, on "auto", when
+    the measured cost model predicts it faster); the output is the same."""
+    method = _norm_matprod(spec.matprod)
+    if method != "VectorDot":
+        return method, None
+    choice = str(spec.pair_product)
+    if choice not in ("auto", "vecdot", "herk"):
+        raise ValueError(f"pair_product must be 'auto', 'vecdot' or 'herk', not {choice!r}")
+    nant = len(spec.antpos)
+    nfeed = 2 if spec.polarized else 1
+    npairs = nant * nant if spec.antpairs is None else len(spec.antpairs)
+    if choice == "auto":
+        choice = pair_product(nant, nfeed, npairs, spec.gemm_mode)
+    return ("MatMul" if choice == "herk" else "VectorDot"), choice
 
 
 class VisEngine:
@@ -120,7 +140,7 @@ class VisEngine:
             # Stokes I (N, Nf); sqrt(0.5 I) (cpu/cpu.py:188) is formed on the device,
             # frequency-major float32, by mvb_flux_sqrt_half at upload
             self.flux_host = np.ascontiguousarray(fl, dtype=np.float64)
-        self.method = _norm_matprod(s.matprod)
+        self.method, self.pair_kernel = _resolve_product(s)
         self.nchunks = max(1, int(s.nchunks))
         self.chunk_size = int(np.ceil(self.nsrc / self.nchunks)) if self.nsrc else 1
         if not 0 < s.source_buffer <= 1:
@@ -437,7 +457,7 @@ def estimate_device_bytes(spec: JobSpec) -> int:
     cap = max(1, int(chunk * spec.source_buffer) if chunk > 1000 else chunk)
     npairs = len(spec.antpairs) if spec.antpairs is not None else A * A
     csize = 8 if spec.precision == 1 else 16
-    method = _norm_matprod(spec.matprod)
+    method, _ = _resolve_product(spec)
     if method == "MatMul":
         mode = _lib.GEMM_MODES[spec.gemm_mode] if isinstance(spec.gemm_mode, str) else int(spec.gemm_mode)
     else:

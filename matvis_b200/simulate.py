@@ -15,7 +15,11 @@ dependencies):
 * beams are :class:`~matvis_b200.beams.GridBeam` / :class:`~matvis_b200.beams.GaussianBeam`
   or a beamfits beam (:func:`~matvis_b200.beamfits.read_beamfits`), interpolated to
   each frequency;
-* ``skycoords`` is an (ra, dec) pair in radians or an object with ``.ra``/``.dec``.
+* ``skycoords`` is an (ra, dec) pair in radians or an object with ``.ra``/``.dec``;
+* ``matprod_method="VectorDot"`` with a pair list runs the per-pair kernel or,
+  where a measured cost model predicts it faster, the tensor-core Hermitian
+  product with a pair gather (same output); ``pair_product`` ("auto", "vecdot",
+  "herk") overrides the choice.
 
 Both run the batched engine (``engine.VisEngine``): every time and frequency of
 the call is one launch sequence on the GPU, with device-side source counts, and
@@ -97,6 +101,7 @@ def simulate(
     beam_spline_opts=None,
     max_progress_reports: int = 100,
     matprod_method: str = "B200MatMul",
+    pair_product: str = "auto",
     coord_method: str = "CoordinateRotationLST",
     max_memory=np.inf,
     min_chunks: int = 1,
@@ -127,7 +132,7 @@ def simulate(
         lsts=lsts, latitude=latitude_of(telescope_loc), beams=_beams_at(beam_list, freq), beam_idx=beam_idx,
         polarized=polarized,
         antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
-        k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks, **rot_kw,
+        pair_product=pair_product, k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks, **rot_kw,
     )
     eng = VisEngine(spec, device=dev)
     out = eng.run_to_host()[0]
@@ -154,6 +159,7 @@ def simulate_vis(
     coord_method: str = "CoordinateRotationLST",
     coord_method_params=None,
     matprod_method: str = "MatMul",
+    pair_product: str = "auto",
     gemm_mode: str = "fp16x3",
     k_chunk: int | None = None,
     min_chunks: int = 1,
@@ -181,7 +187,7 @@ def simulate_vis(
         antpos=antpos, eci=point_source_crd_eq(ra, dec), radec=np.stack([ra, dec]), lsts=lsts_of(times),
         latitude=latitude_of(telescope_loc),
         beam_idx=beam_idx, polarized=polarized, antpairs=antpairs, precision=precision, gemm_mode=gemm_mode,
-        matprod=_norm_matprod(matprod_method), k_chunk=k_chunk, source_buffer=source_buffer,
+        matprod=_norm_matprod(matprod_method), pair_product=pair_product, k_chunk=k_chunk, source_buffer=source_buffer,
         nchunks=max(1, int(min_chunks)), **rot_kw,
     )
     if _chromatic(beams):

@@ -64,12 +64,13 @@ def test_times_with_no_source_above_horizon(device):
         assert np.all(_sim(cfg, matprod_method=matprod) == 0)
 
 
-@pytest.mark.parametrize("matprod", ["MatMul", "VectorDot"])
-def test_pairs_in_both_orders(device, matprod):
-    """antpairs with i < j, i > j and i == j (cpu/matprod.py:21-30 gathers [i, j] as given)."""
+@pytest.mark.parametrize("matprod,kernel", [("MatMul", "auto"), ("VectorDot", "vecdot"), ("VectorDot", "herk")])
+def test_pairs_in_both_orders(device, matprod, kernel):
+    """antpairs with i < j, i > j and i == j (cpu/matprod.py:21-30 gathers [i, j] as given),
+    a VectorDot request on either pair kernel."""
     cfg = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=3000, nfreq=1, ntimes=2, nant=20, seed=21)
     pairs = np.array([(0, 5), (5, 0), (3, 3), (19, 2), (2, 19), (7, 12), (12, 7), (0, 19)])
-    vis = _sim(cfg, antpairs=pairs, matprod_method=matprod)
+    vis = _sim(cfg, antpairs=pairs, matprod_method=matprod, pair_product=kernel)
     ref = _ref(cfg, antpairs=pairs, matprod="VectorDot")
     scale = np.abs(_ref(cfg)).max()
     np.testing.assert_allclose(vis, ref, rtol=0, atol=1e-6 * scale)

@@ -64,9 +64,11 @@ def test_config4_chunking_invariant(device, c4_small):
 
 
 def test_config3_sparse_matmul_vs_vectordot(device):
+    """The per-pair kernel (pinned: the cost model sends 5,000 pairs to the
+    Hermitian product) against the tensor-core product's pair gather."""
     c = wl.config3(nsrc=1_000_000, npairs=5000)
     vm = _run(c, matprod="MatMul")
-    vd = _run(c, matprod="VectorDot")
+    vd = _run(c, matprod="VectorDot", pair_product="vecdot")
     full = _run(dict(c, antpairs=np.array([(i, i) for i in range(len(c["antpos"]))])))
     scale = np.abs(full).max()
     assert vm.shape == vd.shape == (1, 1, 5000, 2, 2)

@@ -8,8 +8,8 @@ import numpy as np
 import pytest
 
 from matvis_b200 import _utils, sharding, workloads
-from matvis_b200.engine import JobSpec, _norm_matprod
-from matvis_b200.matprod import choose_k_chunk
+from matvis_b200.engine import JobSpec, _norm_matprod, _resolve_product
+from matvis_b200.matprod import choose_k_chunk, pair_product
 from oracle import oracle as orc
 
 from .conftest import golden
@@ -43,6 +43,38 @@ def test_matprod_names():
         assert _norm_matprod(n) == "VectorDot"
     with pytest.raises(ValueError):
         _norm_matprod("Einsum")
+
+
+def test_pair_product_cost_model():
+    """Measured break-even of the per-pair kernel against the Hermitian product
+    with a pair gather: ~2,750 pairs for 350 two-feed antennas (21 tiles)."""
+    assert pair_product(350, 2, 5000) == "herk"
+    assert pair_product(350, 2, 2000) == "vecdot"
+    assert pair_product(350, 2, 350 * 351 // 2) == "herk"
+    assert pair_product(37, 1, 63) == "vecdot"  # redundant-baseline representatives of a 37-element hexagon
+    # TF32 operands and six split products double the product's cost
+    assert pair_product(350, 2, 5000, "tf32x3") == "vecdot"
+    assert pair_product(350, 2, 5000, "bf16x6") == "vecdot"
+    assert pair_product(350, 2, 12000, "bf16x6") == "herk"
+
+
+def test_resolve_product():
+    def spec(**kw):
+        base = dict(antpos=np.zeros((350, 3)), eci=np.zeros((3, 1)), fluxes=np.ones((1, 1)), freqs=np.ones(1),
+                    lsts=np.zeros(1), latitude=0.0, beams=[], polarized=True)
+        return JobSpec(**{**base, **kw})
+
+    pairs = np.stack(np.triu_indices(350, 1), axis=1)
+    assert _resolve_product(spec()) == ("MatMul", None)
+    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:5000])) == ("MatMul", "herk")
+    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:500])) == ("VectorDot", "vecdot")
+    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:5000], pair_product="vecdot")) == \
+        ("VectorDot", "vecdot")
+    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:50], pair_product="herk")) == \
+        ("MatMul", "herk")
+    assert _resolve_product(spec(matprod="VectorDot")) == ("MatMul", "herk")  # all 350^2 pairs
+    with pytest.raises(ValueError):
+        _resolve_product(spec(matprod="VectorDot", pair_product="dense"))
 
 
 def test_choose_k_chunk():
