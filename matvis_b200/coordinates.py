@@ -7,14 +7,47 @@ kernels consume.  Per-source work per time step runs on the GPU.
 
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
+
+#: below this many sources one numpy pass beats handing the work to threads
+_PAR_MIN = 1 << 17
+#: chunk granule (elements): a multiple of every SIMD width, so each chunk is
+#: split into vector body and tail exactly as the whole array would be
+_PAR_GRANULE = 8192
 
 
 def point_source_crd_eq(ra, dec):
-    """ECI unit vectors, shape (3, N); coordinates.py:174-200."""
+    """ECI unit vectors, shape (3, N); coordinates.py:174-200.
+
+    Large skies are cut into granule-aligned chunks evaluated by the same numpy
+    ufuncs on host threads (numpy releases the GIL inside them), so every
+    element is bit-identical to the single-pass result; the kernels' horizon
+    selection depends on that.
+    """
     ra = np.asarray(ra, dtype=np.float64)
     dec = np.asarray(dec, dtype=np.float64)
-    return np.asarray([np.cos(ra) * np.cos(dec), np.cos(dec) * np.sin(ra), np.sin(dec)])
+    nthreads = min(os.cpu_count() or 1, 16)
+    if ra.shape != dec.shape or ra.size < _PAR_MIN or nthreads < 2:
+        return np.asarray([np.cos(ra) * np.cos(dec), np.cos(dec) * np.sin(ra), np.sin(dec)])
+    r, d = ra.reshape(-1), dec.reshape(-1)
+    n = r.size
+    out = np.empty((3, n), dtype=np.float64)
+    step = -(-n // nthreads)
+    step = -(-step // _PAR_GRANULE) * _PAR_GRANULE
+
+    def work(lo):
+        sl = slice(lo, min(lo + step, n))
+        cd = np.cos(d[sl])
+        np.multiply(np.cos(r[sl]), cd, out=out[0, sl])
+        np.multiply(cd, np.sin(r[sl]), out=out[1, sl])
+        np.sin(d[sl], out=out[2, sl])
+
+    with ThreadPoolExecutor(nthreads) as ex:
+        list(ex.map(work, range(0, n, step)))
+    return out.reshape((3,) + ra.shape)
 
 
 def eci_to_enu_matrix(ha, lat):

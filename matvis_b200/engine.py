@@ -16,8 +16,10 @@ whole job can be captured once as a CUDA graph and replayed.
 
 from __future__ import annotations
 
+import os
 import queue
 import threading
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -82,6 +84,26 @@ def _norm_matprod(name: str) -> str:
     if n in ("VectorDot", "VectorLoop"):
         return "VectorDot"
     raise ValueError(f"unknown matprod_method {name!r}")
+
+
+def _pinned(src: np.ndarray) -> torch.Tensor:
+    """A page-locked host copy of ``src`` for an asynchronous upload (filled by
+    host threads when large; torch's pinned-block cache keeps the block until the
+    copy that reads it has run).  Pageable when the host refuses to pin."""
+    src = np.ascontiguousarray(src)
+    try:
+        t = torch.empty(src.shape, dtype=torch.from_numpy(src[:0]).dtype, pin_memory=True)
+    except RuntimeError:
+        return torch.from_numpy(src)
+    d, s_ = t.numpy().reshape(-1), src.reshape(-1)
+    nthreads = min(os.cpu_count() or 1, 8)
+    if src.nbytes < (8 << 20) or nthreads < 2:
+        np.copyto(d, s_)
+        return t
+    step = -(-s_.size // nthreads)
+    with ThreadPoolExecutor(nthreads) as ex:
+        list(ex.map(lambda lo: np.copyto(d[lo:lo + step], s_[lo:lo + step]), range(0, s_.size, step)))
+    return t
 
 
 def _resolve_product(spec: JobSpec) -> tuple[str, str | None]:
@@ -233,18 +255,20 @@ class VisEngine:
         if not self._allocated:
             self.allocate()
         N = self.nsrc
+        # every copy is asynchronous on the current stream, from page-locked staging
         if N:
-            self.eci[:, :N].copy_(torch.from_numpy(self.eci_host), non_blocking=False)
-        self.antpos.copy_(torch.from_numpy(self.antpos_host))
+            self.eci[:, :N].copy_(_pinned(self.eci_host), non_blocking=True)
+        self.antpos.copy_(_pinned(self.antpos_host), non_blocking=True)
         if self.pol_sky:
             self.sflux.zero_()  # not read: the polarised writer takes the coherency
         elif N:
-            fl = torch.from_numpy(self.flux_host).to(self.eci.device, non_blocking=False)
+            fl = torch.empty(self.flux_host.shape, dtype=torch.float64, device=self.eci.device)
+            fl.copy_(_pinned(self.flux_host), non_blocking=True)
             _lib.check(_lib.lib.mvb_flux_sqrt_half(_lib.ptr(fl), self.nsrc, len(self.freqs), _lib.ptr(self.sflux),
                                                    _lib.stream_handle()))
         if self.pol_sky and N:
-            self.coh[:, :N].copy_(torch.from_numpy(self.coh_host))
-            self.radec[:, :N].copy_(torch.from_numpy(self.radec_host))
+            self.coh[:, :N].copy_(_pinned(self.coh_host), non_blocking=True)
+            self.radec[:, :N].copy_(_pinned(self.radec_host), non_blocking=True)
 
     def h2d_bytes(self) -> int:
         n = self.eci_host.nbytes + self.antpos_host.nbytes + (0 if self.pol_sky else self.flux_host.nbytes)

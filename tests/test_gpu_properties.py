@@ -87,3 +87,26 @@ def test_config3_subset_vs_oracle(device):
     autos = _run(dict(c, antpairs=np.array([(i, i) for i in range(len(c["antpos"]))])))
     scale = np.abs(autos).max()
     assert np.abs(vm - ref).max() <= 1e-6 * scale
+
+
+@pytest.fixture(scope="module")
+def c3_dense_ref():
+    """A 30,000-source seeded subset of config 3, all 350 antennas and pairs, and its FP64 oracle."""
+    c = wl.subset(wl.config3(nsrc=1_000_000, npairs=5000), nsrc=30000, seed=5)
+    c["antpairs"] = None
+    beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in c["beams"]]
+    ants = {i: tuple(p) for i, p in enumerate(c["antpos"])}
+    ref = orc.simulate_vis(ants=ants, fluxes=c["fluxes"], ra=c["ra"], dec=c["dec"], freqs=c["freqs"], lsts=c["lsts"],
+                           latitude=c["latitude"], beams=beams, polarized=True, beam_idx=c["beam_idx"])
+    return c, ref
+
+
+@pytest.mark.parametrize("mode,tol", [("fp16x3", 1e-6), ("bf16x6", 1e-6), ("tf32x3", 1e-6), ("bf16x3", 3e-5)])
+def test_config3_split_modes_vs_oracle(device, c3_dense_ref, mode, tol):
+    """Per split mode, max |dV| / sqrt(|V_ii| |V_jj|) over every output of the
+    config-3 subset (complex128 output, so the product's error is what is seen)."""
+    c, ref = c3_dense_ref
+    vis = _run(c, precision=2, gemm_mode=mode)
+    err = orc.cosine_error_metric(vis, ref, 2)
+    print(f"config3 subset {mode}: max normalised error {err:.3e}")
+    assert err <= tol, err

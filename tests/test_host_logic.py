@@ -77,6 +77,19 @@ def test_resolve_product():
         _resolve_product(spec(matprod="VectorDot", pair_product="dense"))
 
 
+@pytest.mark.parametrize("n", [1_000_000, 300_001, 131_072, 5])
+def test_point_source_crd_eq_threads_bit_identical(n):
+    """The threaded unit vectors equal the single numpy pass bit for bit (the
+    horizon selection downstream is bit-exact against the oracle)."""
+    from matvis_b200.coordinates import point_source_crd_eq
+
+    rng = np.random.default_rng(n)
+    ra, dec = rng.uniform(0, 2 * np.pi, n), np.arcsin(rng.uniform(-1, 1, n))
+    one = np.asarray([np.cos(ra) * np.cos(dec), np.cos(dec) * np.sin(ra), np.sin(dec)])
+    np.testing.assert_array_equal(point_source_crd_eq(ra, dec), one)
+    np.testing.assert_array_equal(point_source_crd_eq(ra.reshape(-1, 1), dec.reshape(-1, 1)), one[:, :, None])
+
+
 def test_choose_k_chunk():
     kc = choose_k_chunk(21, 196608, 148)
     assert kc % 64 == 0 and 1024 <= kc <= 8192
