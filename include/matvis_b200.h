@@ -145,9 +145,13 @@ int mvb_beam_gaussian(const double *sigmas, int nbeam, const double *crd, int64_
 int mvb_exptau(const double *antpos, int A, double freq, const double *crd, int64_t ld, int64_t nsrc,
                void *exptau, int out_c128, void *stream);
 /* Z panel layout (modes MVB_GEMM_*): 2P planes (plane 2p + c holds split term
- * p of component c, c = 0 real, 1 imaginary), each k-blocked as
- * [Kcap / KB][Mpad][KB] with KB = 64 bytes of elements (32 for bf16 / fp16, 16
- * for tf32): element (m, k) of a plane is at (k / KB) * Mpad * KB + m * KB + k % KB.
+ * p of component c, c = 0 real, 1 imaginary), stored as the Hermitian product's
+ * shared-memory image [Kcap / KB][Mpad / 128][2P][128][KB] with KB = 64 bytes
+ * of elements (32 for bf16 / fp16, 16 for tf32), the four 16-byte chunks of
+ * each 64-byte row in 64-byte swizzled order: element (m, k) of plane pl is at
+ *   ((k / KB) * (Mpad / 128) + m / 128) * 2P * 128 * KB + pl * 128 * KB
+ *   + (m % 128) * KB + ((c / E) ^ ((m % 128 / 2) % 4)) * E + c % E,
+ * c = k % KB, E = KB / 4 elements per chunk.
  * Mpad is a multiple of 128, Kcap of 64.  Bytes: 2P x Mpad x Kcap x element size. */
 size_t mvb_zpanel_bytes(int mode, int64_t Mpad, int64_t Kcap);
 /* sflux[f * N + s] = (float) sqrt(0.5 * flux[s * nf + f]) (cpu/cpu.py:188): the
@@ -195,8 +199,9 @@ int mvb_absmax(const void *z, int z_c128, int64_t n, float *out, void *stream);
 size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
 /* Upper-triangle 128 x 128 complex tiles of V = conj(Z) Z^T over K_valid
  * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05
- * tensor cores with TMEM accumulators, fed by TMA (cp.async.bulk.tensor,
- * 64-byte swizzle over the 64-byte k-blocks); mode MVB_GEMM_* selects the split precision.
+ * tensor cores with TMEM accumulators, fed by one bulk copy (cp.async.bulk) per
+ * operand and stage from the panel's stored shared-memory image; mode
+ * MVB_GEMM_* selects the split precision.
  * drain_ksteps (1, 2 or 4; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
  * number of 32-byte k-steps summed in one TMEM block before the block is added
  * to FP32 registers: the tensor core rounds its accumulator toward zero at every

@@ -54,15 +54,23 @@ constexpr int kTile = 128;
 __host__ __device__ inline int mode_terms(int mode) { return mode == MVB_GEMM_BF16_6 ? 3 : 2; }
 __host__ __device__ inline int mode_elem_bytes(int mode) { return mode == MVB_GEMM_TF32_3 ? 4 : 2; }
 
-// Split-plane panel layout: each plane is stored k-blocked, [Kcap / KB][Mpad][KB]
-// with KB = 64 bytes of elements (32 bf16 / fp16, 16 tf32), so the 128-row x
-// 64-byte box of one Hermitian-product stage (two k-steps) is one contiguous
-// 8 KB run of HBM (a row-major plane would scatter it over 128 DRAM pages), and
-// each of its rows is one 64-byte request.
+// Split-plane panel layout: the Hermitian product's shared-memory image, stored.
+// For k-block kb (KB = 64 bytes of elements: 32 bf16 / fp16, 16 tf32) and row
+// block I (128 rows), the npl = 2P planes follow each other as 128 rows x 64
+// bytes, [Kcap / KB][Mpad / 128][npl][128][KB], and inside each 64-byte row the
+// four 16-byte chunks are permuted by the 64-byte swizzle (chunk c of row r is
+// stored at chunk c ^ ((r >> 1) & 3), the pattern the UMMA shared-memory
+// descriptors read).  One operand of one product stage (two k-steps, all planes)
+// is then one contiguous run of npl x 8 KB, fetched with a single bulk copy.
+// panel_off gives plane 0's element; plane p is 128 * KB elements further.
 constexpr int kKBlockBytes = 64;
-__host__ __device__ inline int64_t panel_off(int64_t m, int64_t k, int64_t Mpad, int kb) {
-  return (k / kb) * (Mpad * kb) + m * kb + (k % kb);
+__host__ __device__ inline int64_t panel_off(int64_t m, int64_t k, int64_t Mpad, int kb, int npl) {
+  const int64_t blk = ((k / kb) * (Mpad / 128) + m / 128) * npl;
+  const int r = (int)(m % 128), c = (int)(k % kb);
+  const int epc = kb / 4;  // elements per 16-byte chunk
+  return blk * (128 * kb) + (int64_t)r * kb + ((c / epc) ^ ((r >> 1) & 3)) * epc + c % epc;
 }
+__host__ __device__ constexpr int64_t panel_plane_stride(int kb) { return 128 * (int64_t)kb; }
 
 // ---------------------------------------------------------------------------
 // device helpers
@@ -138,6 +146,15 @@ __device__ __forceinline__ void tma_load_4d(void *smem_dst, const void *map, uin
       " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(smem_dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, no multicast (both
+// addresses 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void bulk_load(void *smem_dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(smem_dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 
 // ---- tcgen05 --------------------------------------------------------------

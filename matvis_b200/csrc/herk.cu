@@ -28,11 +28,14 @@
 // Schedule.  Work unit u = (k-slice s, tile t), t fastest so the CTAs that run
 // together read the same Z columns (L2 reuse).  Persistent CTAs (one per SM,
 // 192 KB of shared memory) loop over units.  Warp roles (576 threads):
-//   warp 0 lane 0 : TMA producer, one 4-D box per operand per stage (all 2P
-//                   split/component planes of 128 rows x 64 bytes, one k-block of
-//                   the k-blocked panel = two k-steps, SWIZZLE_64B; 64-byte rows
-//                   halve the TMA row requests per byte against 32-byte ones,
-//                   which bounded the kernel);
+//   warp 0 lane 0 : producer, one 1-D bulk copy per operand per stage: the
+//                   panel stores each (k-block, row block) as the stage's
+//                   shared-memory image (all 2P split/component planes of 128
+//                   rows x 64 bytes, 64-byte swizzled; two k-steps), so an
+//                   operand is one contiguous 2P x 8 KB run.  A bulk copy of it
+//                   completes in about half the time of the same bytes as tiled
+//                   TMA boxes of 64-byte rows, and the three stages in flight no
+//                   longer leave the MMA waiting;
 //   warp 1        : TMEM owner (512 columns = two k-step blocks); lane 0 issues
 //                   the UMMAs and tcgen05.commit's the stage / block barriers;
 //   warps 2..17   : epilogue; warp w drains TMEM lane quadrant (w % 4), column
@@ -46,9 +49,6 @@
 // MVB_DEV_TIMEOUT in the status word, stops issuing work, drains the copies and
 // MMAs it issued, frees TMEM and returns.
 #include <algorithm>
-#include <mutex>
-
-#include <cudaTypedefs.h>
 
 #include "common.cuh"
 
@@ -148,7 +148,7 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
 // KD: k-steps accumulated in one TMEM block before it is drained (1, 2 or 4).
 template <int MODE, int KD>
 __global__ void __launch_bounds__(kHerkThreads, 1)
-    herk_kernel(const __grid_constant__ CUtensorMap zmap, int T, int n_tiles, const int32_t *__restrict__ n_dev,
+    herk_kernel(const uint8_t *__restrict__ zpanel, int T, int n_tiles, const int32_t *__restrict__ n_dev,
                 int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, float *__restrict__ partials,
                 int32_t *__restrict__ status) {
   using C = HerkCfg<MODE>;
@@ -183,7 +183,6 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     mbar_init(&drain_bar, 1);
     abort_flag = 0;
     fence_mbar_init();
-    tma_prefetch_desc(&zmap);
   }
   if (warp == 1) {
     tmem_alloc(&tmem_base_sh, 512);
@@ -215,10 +214,12 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         }
         mbar_arrive_expect_tx(&full_bar[st], bytes);
         uint8_t *a = smem + (size_t)st * C::STAGE_BYTES;
-        // k-block index: k0 is a multiple of 64 elements, a k-block 64 bytes
-        const int kb = (int)((k0 + (int64_t)kbi * C::KB) / C::KB);
-        tma_load_4d(a, &zmap, &full_bar[st], 0, I * 128, kb, 0);
-        if (!diag) tma_load_4d(a + C::OPER_BYTES, &zmap, &full_bar[st], 0, J * 128, kb, 0);
+        // k-block index: k0 is a multiple of 64 elements, a k-block 64 bytes;
+        // operand (kb, R) starts at ((kb T + R) 2P) planes of 8 KB
+        const int64_t kb = (k0 + (int64_t)kbi * C::KB) / C::KB;
+        bulk_load(a, zpanel + (kb * T + I) * (int64_t)C::OPER_BYTES, C::OPER_BYTES, &full_bar[st]);
+        if (!diag)
+          bulk_load(a + C::OPER_BYTES, zpanel + (kb * T + J) * (int64_t)C::OPER_BYTES, C::OPER_BYTES, &full_bar[st]);
         ++issued;
         if (++st == C::STAGES) {
           st = 0;
@@ -512,40 +513,10 @@ int set_smem_once(const void *fn, int bytes, int slot) {
   return MVB_OK;
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  });
-  return fn;
-}
-
 template <int MODE, int KD>
 static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
                        int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
   using C = HerkCfg<MODE>;
-  auto enc = tensor_map_encoder();
-  if (!enc) return fail(MVB_ERR_UNSUPPORTED, "mvb_herk: cuTensorMapEncodeTiled unavailable");
-  CUtensorMap map;
-  // k-blocked planes [2P][Kcap / KB][Mpad][KB]: one stage of 128 rows is a
-  // contiguous 8 KB run per plane; the box lands in shared memory as
-  // [plane][row][64 bytes], 64-byte swizzled (the UMMA descriptors' layout).
-  cuuint64_t dims[4] = {(cuuint64_t)C::KB, (cuuint64_t)Mpad, (cuuint64_t)(Kcap / C::KB), (cuuint64_t)(2 * C::P)};
-  cuuint64_t strides[3] = {(cuuint64_t)kKBlockBytes, (cuuint64_t)Mpad * kKBlockBytes, (cuuint64_t)Mpad * Kcap * C::ES};
-  cuuint32_t box[4] = {(cuuint32_t)C::KB, 128u, 1u, (cuuint32_t)(2 * C::P)};
-  cuuint32_t estr[4] = {1, 1, 1, 1};
-  const CUtensorMapDataType dt = MODE == MVB_GEMM_TF32_3  ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                                 : MODE == MVB_GEMM_F16_3 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                                          : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  CUresult r = enc(&map, dt, 4,
-                   const_cast<void *>(z), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(MVB_ERR_CUDA, "mvb_herk: cuTensorMapEncodeTiled failed (%d)", (int)r);
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
   const int nsm = num_sms();
@@ -557,8 +528,8 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
                          16 + 3 * MODE + (KD == 4 ? 2 : KD - 1));
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
-  herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(map, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials,
-                                                     status);
+  herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), T, n_tiles, n_dev, n_host,
+                                                         kmul, Kcap, k_chunk, nsm, partials, status);
   return check_launch("herk_kernel");
 }
 

@@ -58,10 +58,13 @@ __device__ __forceinline__ void store_words(void *p, const uint32_t *w) {
 
 // Writes NV consecutive real values of one component (c = 0 real, 1 imaginary)
 // as the P split terms into planes [2p + c] of a panel row, with vector stores:
-// NV = 4 or 8 values: 8- or 16-byte stores of bf16 / fp16, 16- or 32-byte of float32.
+// NV = 4 or 8 values: 8- or 16-byte stores of bf16 / fp16 (inside one 16-byte
+// chunk of the swizzled row, at off), 16 bytes of float32 at off, or 2 x 16
+// bytes of float32 at off (values 0..3) and off2 (values 4..7: the next chunk,
+// which the swizzle may place anywhere in the row).
 template <int MODE, int NV>
-__device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t off, int comp, const float *v,
-                                          float zscale) {
+__device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t off, int64_t off2, int comp,
+                                          const float *v, float zscale) {
   if constexpr (MODE == MVB_GEMM_F16_3) {
     // one paired conversion per two values for each term (cvt.rn.f16x2.f32)
     uint32_t whi[NV / 2], wlo[NV / 2];
@@ -93,8 +96,15 @@ __device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t
       whi[i] = __float_as_uint(hi[i]);
       wlo[i] = __float_as_uint(lo[i]);
     }
-    store_words<NV>(p0, whi);
-    store_words<NV>(p1, wlo);
+    if constexpr (NV == 8) {
+      store_words<4>(p0, whi);
+      store_words<4>(p1, wlo);
+      store_words<4>(static_cast<float *>(z) + off2 + (int64_t)(0 + comp) * plane_stride, whi + 4);
+      store_words<4>(static_cast<float *>(z) + off2 + (int64_t)(2 + comp) * plane_stride, wlo + 4);
+    } else {
+      store_words<NV>(p0, whi);
+      store_words<NV>(p1, wlo);
+    }
   } else {
     constexpr int P = MODE == MVB_GEMM_BF16_6 ? 3 : 2;
     float r[NV];
@@ -276,7 +286,6 @@ __global__ void __launch_bounds__(kTauZThreads)
   const int sg = threadIdx.x % kTauZGroups;
   const int a0 = blockIdx.y * kTauZAnts;
   const int a1 = min(a0 + kTauZAnts, A);
-  const int64_t plane = Mpad * Kcap;
   {
     for (int a = a0 + alane; a < a1; a += kTauZAntLanes) {
       const int b = beam_idx ? beam_idx[a] : 0;
@@ -345,9 +354,12 @@ __global__ void __launch_bounds__(kTauZThreads)
             *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
         } else {
           // kTauZSrc * X consecutive k from a multiple of kTauZSrc * X: inside one k-block
-          const int64_t off = panel_off(m, s0 * X, Mpad, kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2));
-          put_split<MODE, kTauZSrc * X>(z, plane, off, 0, vr, zscale);
-          put_split<MODE, kTauZSrc * X>(z, plane, off, 1, vi, zscale);
+          constexpr int KB = kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2);
+          constexpr int NPL = MODE == MVB_GEMM_BF16_6 ? 6 : 4;
+          const int64_t off = panel_off(m, s0 * X, Mpad, KB, NPL);
+          const int64_t off2 = panel_off(m, s0 * X + kTauZSrc * X / 2, Mpad, KB, NPL);
+          put_split<MODE, kTauZSrc * X>(z, panel_plane_stride(KB), off, off2, 0, vr, zscale);
+          put_split<MODE, kTauZSrc * X>(z, panel_plane_stride(KB), off, off2, 1, vi, zscale);
         }
       }
     }
@@ -381,7 +393,6 @@ __global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, i
   const int64_t kend = round_up(K, kKAlign);
   const int64_t half = kend / 2;
   const int64_t total = M * half;
-  const int64_t plane = Mpad * Kcap;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t m = i / half, k = (i % half) * 2;
     float vr[2], vi[2];
@@ -397,10 +408,12 @@ __global__ void z_pack_kernel(const CT *__restrict__ zs, int64_t M, int64_t K, i
     if constexpr (MODE == MVB_Z_C64) {
       *reinterpret_cast<float4 *>(static_cast<float2 *>(z) + m * Kcap + k) = make_float4(vr[0], vi[0], vr[1], vi[1]);
     } else {
-      // (k, k + 1), k even: inside one k-block
-      const int64_t off = panel_off(m, k, Mpad, kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2));
-      PanelWriter<MODE>::put(z, plane, off, 0, vr, 2, zscale);
-      PanelWriter<MODE>::put(z, plane, off, 1, vi, 2, zscale);
+      // (k, k + 1), k even: inside one 16-byte chunk of one k-block row
+      constexpr int KB = kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2);
+      constexpr int NPL = MODE == MVB_GEMM_BF16_6 ? 6 : 4;
+      const int64_t off = panel_off(m, k, Mpad, KB, NPL);
+      PanelWriter<MODE>::put(z, panel_plane_stride(KB), off, 0, vr, 2, zscale);
+      PanelWriter<MODE>::put(z, panel_plane_stride(KB), off, 1, vi, 2, zscale);
     }
   }
 }

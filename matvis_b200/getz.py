@@ -18,9 +18,10 @@ from ._lib import check, ptr, stream_handle
 class ZPanel:
     """Device Z in split-plane (or plain complex64) layout.
 
-    ``data``: (planes, Kcap / KB, Mpad, KB) for the tensor-core modes -- each
-    plane k-blocked in 64-byte blocks of KB elements, so that one stage of the
-    Hermitian product (128 rows, two k-steps) is contiguous in HBM -- and
+    ``data``: (Kcap / KB, Mpad / 128, planes, 128, KB) for the tensor-core modes
+    -- the Hermitian product's shared-memory image of each (64-byte k-block,
+    128-row block), the 16-byte chunks of every row in 64-byte swizzled order,
+    so that one operand of a product stage is one contiguous bulk copy -- and
     (M, Kcap) complex64 for the plain mode.
     ``n_dev`` / ``n_host`` give the valid source count; the valid K extent is
     that count times ``nax``.
@@ -38,7 +39,8 @@ class ZPanel:
             self.data = torch.zeros((self.M, self.Kcap), dtype=dt, device=device)
         else:
             kb = _lib.zpanel_kblock(mode)
-            self.data = torch.zeros((planes, self.Kcap // kb, self.Mpad, kb), dtype=dt, device=device)
+            self.data = torch.zeros((self.Kcap // kb, self.Mpad // _lib.TILE, planes, _lib.TILE, kb), dtype=dt,
+                                    device=device)
         self.n_dev = None
         self.n_host = 0
         #: power-of-two factor the panel holds Z multiplied by (fp16x3 mode)
@@ -54,8 +56,14 @@ class ZPanel:
         k = n * self.nax
         if self.mode == _lib.Z_C64:
             return self.data[:, :k].to(torch.complex128)
-        p, nkb, mpad, kb = self.data.shape
-        d = self.data.permute(0, 2, 1, 3).reshape(p, mpad, nkb * kb)[:, : self.M, :k].to(torch.float64)
+        nkb, nblk, p, rows, kb = self.data.shape
+        # undo the 64-byte swizzle: chunk c of row r sits at chunk c ^ ((r >> 1) & 3)
+        r = torch.arange(rows, device=self.data.device)[:, None]
+        c = torch.arange(kb, device=self.data.device)[None, :]
+        epc = kb // 4
+        idx = (((c // epc) ^ ((r >> 1) & 3)) * epc + c % epc).expand(nkb, nblk, p, rows, kb)
+        d = torch.gather(self.data, 4, idx).permute(2, 1, 3, 0, 4).reshape(p, nblk * rows, nkb * kb)
+        d = d[:, : self.M, :k].to(torch.float64)
         re = d[0::2].sum(0) / self.scale
         im = d[1::2].sum(0) / self.scale
         return torch.complex(re, im)

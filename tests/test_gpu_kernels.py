@@ -198,7 +198,9 @@ def test_vectordot_arange_known_answer(device):
 
 
 @pytest.mark.parametrize("mode,tol", [("bf16x6", 1e-6), ("tf32x3", 1e-6), ("fp16x3", 1e-6), ("bf16x3", 3e-5)])
-@pytest.mark.parametrize("nant,nfeed,K,k_chunk", [(350, 2, 20000, 2048), (64, 1, 777, 64), (129, 2, 4096, 1024)])
+# row counts whose last 128-row block holds 60 (700 rows), 64, 2, 72 and 128 rows
+@pytest.mark.parametrize("nant,nfeed,K,k_chunk", [(350, 2, 20000, 2048), (64, 1, 777, 64), (129, 2, 4096, 1024),
+                                                  (96, 2, 3000, 1024), (100, 2, 3000, 1024), (128, 1, 2000, 512)])
 def test_matmul_random_vs_oracle(device, mode, tol, nant, nfeed, K, k_chunk):
     rng = np.random.default_rng(nant + K)
     M = nant * nfeed

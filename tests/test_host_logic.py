@@ -90,6 +90,35 @@ def test_point_source_crd_eq_threads_bit_identical(n):
     np.testing.assert_array_equal(point_source_crd_eq(ra.reshape(-1, 1), dec.reshape(-1, 1)), one[:, :, None])
 
 
+@pytest.mark.parametrize("mode", ["fp16x3", "bf16x6", "tf32x3"])
+def test_panel_layout_round_trip(mode):
+    """Z written element by element at the documented panel offsets (the
+    product's swizzled shared-memory image) reads back through ZPanel.to_complex."""
+    import torch
+
+    from matvis_b200 import _lib
+    from matvis_b200.getz import ZPanel
+
+    m_, nax, nsrc = 200, 2, 150
+    md = _lib.GEMM_MODES[mode]
+    mpad, kcap = _lib.zpanel_shape(md, m_, nax * nsrc)
+    kb, npl = _lib.zpanel_kblock(md), _lib.zpanel_planes(md)
+    rng = np.random.default_rng(1)
+    z = (rng.integers(-8, 8, (m_, nax * nsrc)) + 1j * rng.integers(-8, 8, (m_, nax * nsrc))).astype(np.complex128)
+    flat = np.zeros(npl * mpad * kcap)
+    e = kb // 4
+    for m in range(m_):
+        for k in range(nax * nsrc):
+            c, r = k % kb, m % 128
+            base = ((k // kb) * (mpad // 128) + m // 128) * npl * 128 * kb + r * kb + ((c // e) ^ ((r // 2) % 4)) * e + c % e
+            flat[base] = z[m, k].real  # split term 0 carries the value, the others stay 0
+            flat[base + 128 * kb] = z[m, k].imag
+    panel = ZPanel.__new__(ZPanel)
+    panel.mode, panel.M, panel.nax, panel.n_host, panel.n_dev, panel.scale = md, m_, nax, nsrc, None, 1.0
+    panel.data = torch.as_tensor(flat.reshape(kcap // kb, mpad // 128, npl, 128, kb))
+    np.testing.assert_array_equal(panel.to_complex().numpy(), z)
+
+
 def test_choose_k_chunk():
     kc = choose_k_chunk(21, 196608, 148)
     assert kc % 64 == 0 and 1024 <= kc <= 8192
