@@ -119,6 +119,15 @@ def test_panel_layout_round_trip(mode):
     np.testing.assert_array_equal(panel.to_complex().numpy(), z)
 
 
+def test_engine_interface():
+    """The engine's public methods (the served form, simulate and bench call them)."""
+    from matvis_b200.engine import VisEngine
+
+    for name in ("allocate", "upload", "h2d_bytes", "enqueue", "enqueue_time", "run", "run_to_host", "capture",
+                 "result", "device_bytes", "launches_per_run"):
+        assert callable(getattr(VisEngine, name, None)), name
+
+
 def test_choose_k_chunk():
     kc = choose_k_chunk(21, 196608, 148)
     assert kc % 64 == 0 and 1024 <= kc <= 8192
