@@ -70,6 +70,10 @@ def parse():
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
                     help="2: HERA-350-like job (default); 3: 1e6 power-law sources; 4: 500k sources, 256 f x 64 LST")
     ap.add_argument("--sparse", action="store_true", help="config 3: the 5,000 seeded pairs on the VectorDot path")
+    ap.add_argument("--sky", default="stokes", choices=["stokes", "pol"],
+                    help="pol: a seeded polarised sky (coherency fluxes) instead of Stokes I")
+    ap.add_argument("--rotation", default="lst", choices=["lst", "erfa"],
+                    help="erfa: the apparent-place rotation from per-time astrometry parameters (refreshed every step)")
     ap.add_argument("--pair-kernel", default="auto", choices=["auto", "vecdot", "herk"],
                     help="--sparse: per-pair sums, the Hermitian product with a pair gather, or the cost model's choice")
     ap.add_argument("--nsrc", type=int, default=None, help="source count (configs 3 and 4)")
@@ -161,15 +165,18 @@ def load_config(args) -> tuple[dict, str]:
     return cfg, desc
 
 
-def terms_per_job(cfg) -> tuple[float, np.ndarray]:
+def terms_per_job(cfg, astrom=None) -> tuple[float, np.ndarray]:
     """Npairs * sum_t n_t * Nf (Npairs = Nant^2, or the listed pairs), with n_t from
-    the same FP64 fixed-order rotation as the kernels."""
-    from matvis_b200.coordinates import eci_to_enu_matrix, point_source_crd_eq
+    the same FP64 fixed-order rotation as the kernels (for the ERFA rotation its
+    rigid part, BPN then CIRS -> ENU: aberration and light deflection, ~1e-4 rad,
+    change the count by ~1e-5)."""
+    from matvis_b200.coordinates import atioq_matrix, eci_to_enu_matrix, point_source_crd_eq
 
     eci = point_source_crd_eq(cfg["ra"], cfg["dec"])
     counts = []
-    for lst in cfg["lsts"]:
-        R = eci_to_enu_matrix(lst, cfg["latitude"])
+    for t, lst in enumerate(cfg["lsts"]):
+        R = (eci_to_enu_matrix(lst, cfg["latitude"]) if astrom is None
+             else atioq_matrix(astrom[t]) @ np.asarray(astrom[t]["bpn"]).reshape(3, 3))
         z = (R[2, 0] * eci[0] + R[2, 1] * eci[1]) + R[2, 2] * eci[2]
         counts.append(int((z > 0).sum()))
     nant = len(cfg["antpos"])
@@ -412,12 +419,23 @@ def run_b200(args, rank, world, local_rank):
         import torch.distributed as dist
 
     cfg, desc = load_config(args)
-    terms, counts = terms_per_job(cfg)
+    fluxes, rot_kw, sim_kw = cfg["fluxes"], {}, {}
+    if args.sky == "pol":
+        fluxes = wl.polarised_sky(cfg)
+        desc += "; polarised sky (seeded Q, U, V; coherency fluxes)"
+    if args.rotation == "erfa":
+        time_s = 600.0 * np.arange(len(cfg["lsts"]))
+        rot_kw = dict(astrom=wl.synthetic_astrom(cfg["lsts"], cfg["latitude"]), time_s=time_s, update_bcrs_every=0.0)
+        sim_kw = dict(coord_method="CoordinateRotationERFA", coord_method_params=rot_kw)
+        desc += "; ERFA apparent-place rotation from seeded astrometry parameters, refreshed every time step"
+    if args.sky != "stokes" or args.rotation != "lst":
+        args.skip_cpu = args.skip_plain = True  # the samplers restate the Stokes-I, LST-rotation path
+    terms, counts = terms_per_job(cfg, rot_kw.get("astrom"))
     matprod = "VectorDot" if args.sparse else "MatMul"
-    spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
+    spec = job_from_arrays(ants=cfg["antpos"], fluxes=fluxes, ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
                            lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
                            polarized=True, precision=1, gemm_mode=args.gemm_mode, k_chunk=args.k_chunk,
-                           antpairs=cfg["antpairs"], matprod=matprod, pair_product=args.pair_kernel)
+                           antpairs=cfg["antpairs"], matprod=matprod, pair_product=args.pair_kernel, **rot_kw)
     eng = VisEngine(spec, device=dev)
     eng.upload()
     eng.run()  # uncaptured run: checks status, warms caches
@@ -507,15 +525,15 @@ def run_b200(args, rank, world, local_rank):
         kw = dict(polarized=True, precision=1, beam_idx=cfg["beam_idx"], gemm_mode=args.gemm_mode,
                   k_chunk=args.k_chunk, device=dev, antpairs=cfg["antpairs"], matprod_method=matprod,
                   pair_product=args.pair_kernel)
-        mv.simulate_vis(ants, cfg["fluxes"], cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
-                        cfg["latitude"], **kw)
+        mv.simulate_vis(ants, fluxes, cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
+                        cfg["latitude"], **kw, **sim_kw)
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         nb_out = 0
         for _ in range(args.e2e_steps):
-            out = mv.simulate_vis(ants, cfg["fluxes"], cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
-                                  cfg["latitude"], **kw)
+            out = mv.simulate_vis(ants, fluxes, cfg["ra"], cfg["dec"], cfg["freqs"], cfg["lsts"], cfg["beams"],
+                                  cfg["latitude"], **kw, **sim_kw)
             nb_out = out.nbytes
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / args.e2e_steps

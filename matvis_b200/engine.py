@@ -106,6 +106,35 @@ def _pinned(src: np.ndarray) -> torch.Tensor:
     return t
 
 
+def _repack_coherency(c: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """(N, Nf, 2, 2) complex coherency -> (Nf, N, 4) float32 [C00, C11, Re C01,
+    Im C01] and the (N, Nf) float64 trace max(C00 + C11, 0); source chunks on
+    host threads (plain copies and one addition: the values do not depend on
+    the split)."""
+    n, nf = c.shape[:2]
+    coh = np.empty((nf, n, 4), dtype=np.float32)
+    trace = np.empty((n, nf), dtype=np.float64)
+
+    def work(lo):
+        hi = min(lo + step, n)
+        cb = c[lo:hi]
+        coh[:, lo:hi, 0] = cb[..., 0, 0].real.T
+        coh[:, lo:hi, 1] = cb[..., 1, 1].real.T
+        coh[:, lo:hi, 2] = cb[..., 0, 1].real.T
+        coh[:, lo:hi, 3] = cb[..., 0, 1].imag.T
+        np.maximum(cb[..., 0, 0].real + cb[..., 1, 1].real, 0.0, out=trace[lo:hi])
+
+    nthreads = min(os.cpu_count() or 1, 16)
+    step = max(-(-n // nthreads), 1)
+    if n * nf < (1 << 16) or nthreads < 2:
+        step = max(n, 1)
+        work(0)
+    else:
+        with ThreadPoolExecutor(nthreads) as ex:
+            list(ex.map(work, range(0, n, step)))
+    return coh, trace
+
+
 def _resolve_product(spec: JobSpec) -> tuple[str, str | None]:
     """(kernel family, pair kernel): a VectorDot request runs on the Hermitian
     product with a pair gather when ``pair_product`` says so (or, on "auto", when
@@ -146,13 +175,9 @@ class VisEngine:
         if self.pol_sky:
             if not s.polarized:
                 raise ValueError("a polarised sky (coherency fluxes) needs polarized=True")
-            # per frequency and source: C00, C11, Re C01, Im C01 (float32, 16 bytes)
-            c = np.asarray(fl, dtype=np.complex128)
-            self.coh_host = np.ascontiguousarray(np.stack(
-                [c[..., 0, 0].real, c[..., 1, 1].real, c[..., 0, 1].real, c[..., 0, 1].imag], axis=-1
-            ).transpose(1, 0, 2).astype(np.float32))
-            trace = np.maximum(c[..., 0, 0].real + c[..., 1, 1].real, 0.0)
-            self.flux_host = np.ascontiguousarray(trace)  # Stokes I, for the Z scale bound
+            # per frequency and source: C00, C11, Re C01, Im C01 (float32, 16 bytes);
+            # Stokes I = trace C for the Z scale bound
+            self.coh_host, self.flux_host = _repack_coherency(np.asarray(fl, dtype=np.complex128))
             if s.radec is not None:
                 self.radec_host = np.ascontiguousarray(np.asarray(s.radec, dtype=np.float64).reshape(2, self.nsrc))
             else:

@@ -198,6 +198,47 @@ def config4(nsrc: int = 500_000, nfreq: int = 256, ntimes: int = 64):
     )
 
 
+def polarised_sky(cfg: dict, seed: int = 2, max_frac: float = 0.8) -> np.ndarray:
+    """A polarised version of a workload's sky: seeded Q, U, V of random direction
+    and polarised fraction uniform in [0, max_frac) of Stokes I, returned as the
+    (N, Nf, 2, 2) coherency 0.5 [[I + Q, U - iV], [U + iV, I - Q]] (the
+    reference's coherency convention for a polarised sky)."""
+    rng = np.random.default_rng(seed)
+    i = np.asarray(cfg["fluxes"], dtype=np.float64)
+    frac = rng.uniform(0, max_frac, i.shape)
+    d = rng.normal(size=(3,) + i.shape)
+    d /= np.linalg.norm(d, axis=0)
+    q, u, v = i * frac * d
+    c = np.empty(i.shape + (2, 2), dtype=np.complex128)
+    c[..., 0, 0] = 0.5 * (i + q)
+    c[..., 1, 1] = 0.5 * (i - q)
+    c[..., 0, 1] = 0.5 * (u - 1j * v)
+    c[..., 1, 0] = 0.5 * (u + 1j * v)
+    return c
+
+
+def synthetic_astrom(lsts, latitude: float, seed: int = 3) -> list[dict]:
+    """Seeded astrometry parameters of the ERFA apparent-place step, one dict per
+    time (the fields of ERFA's ASTROM structure that the rotation uses): Earth's
+    heliocentric direction eh at 1 AU (em), its barycentric velocity v (|v| = 1e-4
+    c, perpendicular to eh) with bm1 = sqrt(1 - v^2), a bias-precession-nutation
+    matrix bpn 0.35 deg from the identity (about 25 years of precession), polar
+    motion of 1 microradian, the Earth rotation angle eral = the LST, and the
+    site latitude.  Stand-ins for the caller's astropy-derived values, for timing."""
+    rng = np.random.default_rng(seed)
+    lam, eps = rng.uniform(0, 2 * np.pi), np.deg2rad(23.44)
+    eh = np.array([np.cos(lam), np.sin(lam) * np.cos(eps), np.sin(lam) * np.sin(eps)])
+    v = 1e-4 * np.array([-np.sin(lam), np.cos(lam) * np.cos(eps), np.cos(lam) * np.sin(eps)])
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    ang = np.deg2rad(0.35)
+    k = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    bpn = np.eye(3) + np.sin(ang) * k + (1 - np.cos(ang)) * (k @ k)
+    base = dict(eh=eh, em=1.0, v=v, bm1=float(np.sqrt(1 - v @ v)), bpn=bpn, xpl=1e-6, ypl=-1e-6,
+                sphi=float(np.sin(latitude)), cphi=float(np.cos(latitude)))
+    return [dict(base, eral=float(l)) for l in np.asarray(lsts, dtype=np.float64)]
+
+
 def subset(cfg: dict, nsrc: int | None = None, nfreq: int | None = None, ntimes: int | None = None,
            nant: int | None = None, seed: int = 0) -> dict:
     """A smaller seeded slice of a configuration (for oracle-checkable tests)."""

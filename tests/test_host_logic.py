@@ -119,6 +119,20 @@ def test_panel_layout_round_trip(mode):
     np.testing.assert_array_equal(panel.to_complex().numpy(), z)
 
 
+@pytest.mark.parametrize("n,nf", [(70001, 3), (5, 2), (0, 4)])
+def test_repack_coherency(n, nf):
+    """The threaded coherency repack equals the single-pass expressions exactly."""
+    from matvis_b200.engine import _repack_coherency
+
+    rng = np.random.default_rng(n)
+    c = rng.normal(size=(n, nf, 2, 2)) + 1j * rng.normal(size=(n, nf, 2, 2))
+    coh, trace = _repack_coherency(c)
+    ref = np.stack([c[..., 0, 0].real, c[..., 1, 1].real, c[..., 0, 1].real, c[..., 0, 1].imag],
+                   axis=-1).transpose(1, 0, 2).astype(np.float32)
+    np.testing.assert_array_equal(coh, ref)
+    np.testing.assert_array_equal(trace, np.maximum(c[..., 0, 0].real + c[..., 1, 1].real, 0.0))
+
+
 def test_engine_interface():
     """The engine's public methods (the served form, simulate and bench call them)."""
     from matvis_b200.engine import VisEngine
