@@ -182,6 +182,17 @@ class BeamInterpolator(ABC):
         return self.interpolated_beam
 
 
+def is_chromatic(beams) -> bool:
+    """True when a beam carries several frequencies (a beamfits beam)."""
+    return any(hasattr(b, "at_frequency") for b in beams)
+
+
+def beams_at_frequency(beams, freq: float) -> list:
+    """Beams at one frequency: beamfits beams are interpolated to ``freq`` and
+    re-gridded (core/beams.py:82-93); grid and analytic beams pass unchanged."""
+    return [b.to_grid_beam(freq) if hasattr(b, "at_frequency") else b for b in beams]
+
+
 class B200BeamInterpolator(BeamInterpolator):
     """Beam interpolation on the B200 (``mvb_beam_interp`` / ``mvb_beam_gaussian``).
 

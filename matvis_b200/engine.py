@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .beams import B200BeamInterpolator, GaussianBeam, GridBeam
+from .beams import B200BeamInterpolator, GaussianBeam, GridBeam, beams_at_frequency, is_chromatic
 from .coordinates import (
     ENU_TO_ALTAZ,
     atioq_matrix,
@@ -216,12 +216,18 @@ class VisEngine:
             else:
                 rigid = list(self.rot)
             self.ravg = [np.ascontiguousarray(ENU_TO_ALTAZ @ r) for r in rigid]
+        # a beamfits beam is interpolated to every frequency of the job on the host
+        # (re-gridded per frequency, core/beams.py:82-93) and on the device per slice
+        self.chromatic = is_chromatic(s.beams)
+        self.beams_per_freq = ([beams_at_frequency(s.beams, f) for f in self.freqs] if self.chromatic
+                               else [list(s.beams)])
         self.zscale = 1.0
         if self.method == "MatMul" and _lib.GEMM_MODES.get(s.gemm_mode, s.gemm_mode) == _lib.GEMM_F16_3:
             # |Z| <= max sqrt(0.5 I) * max |beam| (bilinear weights are convex, |exptau| = 1); for a
             # polarised sky |sum_x beam_x L_xy| <= sqrt(2) max|beam| sqrt(trace C) = 2 max|beam| sqrt(I / 2)
             smax = float(np.sqrt(0.5 * max(float(self.flux_host.max(initial=0.0)), 0.0)))
-            zmax = smax * beam_bound(s.beams) * (2.0 if self.pol_sky else 1.0)
+            bmax = max((beam_bound(b) for b in self.beams_per_freq), default=1.0)
+            zmax = smax * bmax * (2.0 if self.pol_sky else 1.0)
             self.zscale = _lib.f16_scale(zmax * (1 + 2**-10))
         self._graph = None
         self._allocated = False
@@ -248,11 +254,17 @@ class VisEngine:
         self.n_above = torch.zeros(1, dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.ws_compact = torch.empty(_lib.lib.mvb_horizon_ws_bytes(self.chunk_size), dtype=torch.uint8, device=dev)
-        self.bmfunc = B200BeamInterpolator(
-            beam_list=s.beams, beam_idx=s.beam_idx, polarized=s.polarized, nant=A, freq=float(self.freqs[0]) if len(self.freqs) else 0.0,
-            nsrc=self.cap, precision=1, device=dev,
-        )
-        self.bmfunc.setup()
+        # one interpolator per frequency for a beamfits beam, all writing one beam buffer
+        self.bmfuncs = []
+        for i, bl in enumerate(self.beams_per_freq):
+            bf = B200BeamInterpolator(beam_list=bl, beam_idx=s.beam_idx, polarized=s.polarized, nant=A,
+                                      freq=float(self.freqs[i]) if len(self.freqs) else 0.0, nsrc=self.cap,
+                                      precision=1, device=dev)
+            bf.setup()
+            if self.bmfuncs:
+                bf.interpolated_beam = self.bmfuncs[0].interpolated_beam
+            self.bmfuncs.append(bf)
+        self.bmfunc = self.bmfuncs[0]
         if self.method == "MatMul":
             self.matprod = B200MatMul(1, self.nfeed, A, s.antpairs, precision=s.precision, gemm_mode=s.gemm_mode,
                                       k_chunk=s.k_chunk, device=dev)
@@ -330,15 +342,18 @@ class VisEngine:
                 _lib.ptr(self.topo), self.nsrc, c0, c1, None, _lib.ptr(self.crd), _lib.ptr(self.kept), None,
                 _lib.ptr(self.n_above), self.cap, _lib.ptr(self.status), _lib.ptr(self.ws_compact),
                 self.ws_compact.numel(), sh))
-            self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, self.bmfunc.interpolated_beam,
-                               stream=stream, status=self.status)
             beam = self.bmfunc.interpolated_beam
+            if not self.chromatic:  # time-only: once for all frequencies
+                self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, beam, stream=stream, status=self.status)
             if self.pol_sky:
                 chk(L.mvb_coherency_rotation(
                     _lib.ptr(self.radec), self.nsrc, _lib.ptr(self.kept), _lib.ptr(self.crd), self.cap,
                     _lib.ptr(self.n_above), self.cap, self.ravg[t].ctypes.data_as(_lib.c_void_p), _lib.ptr(self.rot2),
                     sh))
             for f in range(len(self.freqs)):
+                if self.chromatic:
+                    self.bmfuncs[f].launch(self.crd, self.cap, self.n_above, self.cap, beam, stream=stream,
+                                           status=self.status)
                 if self.pol_sky:
                     chk(L.mvb_tau_z_pol(
                         _lib.ptr(self.antpos), A, float(self.freqs[f]), _lib.ptr(self.crd), self.cap,
@@ -373,7 +388,8 @@ class VisEngine:
 
     def launches_per_run(self) -> int:
         per_f = 3 if self.method == "MatMul" else 2
-        per_chunk = 3 + per_f * len(self.freqs) + int(self.pol_sky)  # count + scatter + beam (+ frame), per frequency
+        # count + scatter + beam (+ frame), per frequency (+ its beam for a beamfits beam)
+        per_chunk = 2 + int(not self.chromatic) + (per_f + int(self.chromatic)) * len(self.freqs) + int(self.pol_sky)
         n = len(self.lsts) * (1 + self.nchunks * per_chunk)
         return n + (sum(self.bcrs_plan) if self.bcrs_plan is not None else 0)
 

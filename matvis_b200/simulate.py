@@ -35,18 +35,10 @@ import torch
 
 from . import _lib
 from ._utils import get_desired_chunks
+from .beams import beams_at_frequency
 from .coordinates import latitude_of, lsts_of, point_source_crd_eq, radec_of
 from .engine import JobSpec, VisEngine, _norm_matprod
 
-
-def _chromatic(beams) -> bool:
-    return any(hasattr(b, "at_frequency") for b in beams)
-
-
-def _beams_at(beams, freq: float) -> list:
-    """Beams at one frequency: beamfits beams (``BeamFits``) are interpolated to
-    ``freq`` and re-gridded (core/beams.py:82-93), grid / analytic beams pass."""
-    return [b.to_grid_beam(freq) if hasattr(b, "at_frequency") else b for b in beams]
 
 logger = logging.getLogger(__name__)
 
@@ -129,7 +121,7 @@ def simulate(
                                     precision, source_buffer=source_buffer, memory_buffer=memory_buffer)
     spec = JobSpec(
         antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=I_sky[:, None], freqs=np.array([float(freq)]),
-        lsts=lsts, latitude=latitude_of(telescope_loc), beams=_beams_at(beam_list, freq), beam_idx=beam_idx,
+        lsts=lsts, latitude=latitude_of(telescope_loc), beams=beams_at_frequency(beam_list, freq), beam_idx=beam_idx,
         polarized=polarized,
         antpairs=antpairs, precision=precision, gemm_mode=gemm_mode, matprod=_norm_matprod(matprod_method),
         pair_product=pair_product, k_chunk=k_chunk, source_buffer=source_buffer, nchunks=nchunks, **rot_kw,
@@ -190,11 +182,7 @@ def simulate_vis(
         matprod=_norm_matprod(matprod_method), pair_product=pair_product, k_chunk=k_chunk, source_buffer=source_buffer,
         nchunks=max(1, int(min_chunks)), **rot_kw,
     )
-    if _chromatic(beams):
-        # frequency-dependent beams: one job per frequency (wrapper.py:180-199)
-        parts = [VisEngine(JobSpec(fluxes=fluxes[:, i : i + 1], freqs=freqs[i : i + 1], beams=_beams_at(beams, f),
-                                   **common), device=device).run_to_host() for i, f in enumerate(freqs)]
-        vis = np.concatenate(parts, axis=0)
-    else:
-        vis = VisEngine(JobSpec(fluxes=fluxes, freqs=freqs, beams=list(beams), **common), device=device).run_to_host()
+    # frequency-dependent (beamfits) beams are interpolated per frequency inside the
+    # one batched job (the reference re-interpolates per frequency, wrapper.py:180-199)
+    vis = VisEngine(JobSpec(fluxes=fluxes, freqs=freqs, beams=list(beams), **common), device=device).run_to_host()
     return vis if polarized else vis[..., 0, 0]
