@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
                     help="2: HERA-350-like job (default); 3: 1e6 power-law sources; 4: 500k sources, 256 f x 64 LST")
     ap.add_argument("--sparse", action="store_true", help="config 3: the 5,000 seeded pairs on the VectorDot path")
+    ap.add_argument("--pairs", default="all", choices=["all", "redundant"],
+                    help="redundant: one pair per redundant baseline group (get_redundancies) on the VectorDot path")
     ap.add_argument("--sky", default="stokes", choices=["stokes", "pol"],
                     help="pol: a seeded polarised sky (coherency fluxes) instead of Stokes I")
     ap.add_argument("--rotation", default="lst", choices=["lst", "erfa"],
@@ -165,6 +167,11 @@ def load_config(args) -> tuple[dict, str]:
                 f"{len(cfg['lsts'])} LST over 6 h, polarised 2x2, 4 gridded beams; one job per step")
     if args.sparse and args.config != 3:
         raise SystemExit("--sparse applies to config 3")
+    if args.pairs == "redundant":
+        from matvis_b200.pairs import redundant_antpairs
+
+        cfg["antpairs"] = redundant_antpairs(cfg["antpos"])
+        desc += f"; {len(cfg['antpairs'])} redundant-baseline pairs on the VectorDot path"
     return cfg, desc
 
 
@@ -434,7 +441,7 @@ def run_b200(args, rank, world, local_rank):
     if args.sky != "stokes" or args.rotation != "lst":
         args.skip_cpu = args.skip_plain = True  # the samplers restate the Stokes-I, LST-rotation path
     terms, counts = terms_per_job(cfg, rot_kw.get("astrom"))
-    matprod = "VectorDot" if args.sparse else "MatMul"
+    matprod = "VectorDot" if args.sparse or args.pairs != "all" else "MatMul"
     spec = job_from_arrays(ants=cfg["antpos"], fluxes=fluxes, ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
                            lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
                            polarized=True, precision=1, gemm_mode=args.gemm_mode, k_chunk=args.k_chunk,
