@@ -1,5 +1,5 @@
 // Shared helpers for the sm_100a kernels: status handling, PTX wrappers for
-// mbarriers, TMA (cp.async.bulk.tensor) and tcgen05 (TMEM, UMMA).
+// mbarriers, bulk copies (cp.async.bulk) and tcgen05 (TMEM, UMMA).
 #pragma once
 
 #include <cuda.h>
@@ -124,30 +124,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64
   }
 }
 
-// ---- TMA ------------------------------------------------------------------
-__device__ __forceinline__ void tma_prefetch_desc(const void *map) {
-  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
-}
-
-// 3-D tiled load, no multicast, into this CTA's shared memory.
-__device__ __forceinline__ void tma_load_3d(void *smem_dst, const void *map, uint64_t *bar, int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(smem_dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// 4-D tiled load, no multicast, into this CTA's shared memory.
-__device__ __forceinline__ void tma_load_4d(void *smem_dst, const void *map, uint64_t *bar, int c0, int c1, int c2,
-                                            int c3) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(smem_dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-      : "memory");
-}
-
+// ---- bulk copies ----------------------------------------------------------
 // 1-D bulk copy global -> this CTA's shared memory, no multicast (both
 // addresses 16-byte aligned, bytes a multiple of 16).
 __device__ __forceinline__ void bulk_load(void *smem_dst, const void *src, uint32_t bytes, uint64_t *bar) {
@@ -225,10 +202,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Shared-memory matrix descriptor (tcgen05 / UMMA), K-major, 32-byte swizzle:
-// 8-row core-matrix groups of 8 x 32 B, SBO = 256 B between groups.
-// K-major, 64-byte swizzle: rows of 64 bytes, 8-row core-matrix groups of
-// 512 B (SBO); the second 32-byte k-step of a row is the start address + 32 B.
+// Shared-memory matrix descriptor (tcgen05 / UMMA), K-major, 64-byte swizzle:
+// rows of 64 bytes, 8-row core-matrix groups of 512 B (SBO); the second
+// 32-byte k-step of a row is the start address + 32 B.
 __device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((smem_addr & 0x3FFFF) >> 4);  // start address  [0, 14)
@@ -236,16 +212,6 @@ __device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
   d |= static_cast<uint64_t>(512 >> 4) << 32;               // SBO            [32, 46)
   d |= static_cast<uint64_t>(1) << 46;                      // version = 1    [46, 48)
   d |= static_cast<uint64_t>(4) << 61;                      // SWIZZLE_64B    [61, 64)
-  return d;
-}
-
-__device__ __forceinline__ uint64_t umma_desc_sw32(uint32_t smem_addr) {
-  uint64_t d = 0;
-  d |= static_cast<uint64_t>((smem_addr & 0x3FFFF) >> 4);  // start address  [0, 14)
-  d |= static_cast<uint64_t>(1) << 16;                      // LBO (unused)   [16, 30)
-  d |= static_cast<uint64_t>(256 >> 4) << 32;               // SBO            [32, 46)
-  d |= static_cast<uint64_t>(1) << 46;                      // version = 1    [46, 48)
-  d |= static_cast<uint64_t>(6) << 61;                      // SWIZZLE_32B    [61, 64)
   return d;
 }
 

@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 
   uint64_t issued = 0;  // producer: stages issued
   if (warp == 0 && lane == 0) {
-    // ---------------- TMA producer ----------------
+    // ---------------- bulk-copy producer ----------------
     uint32_t st = 0, ph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
       const int s = u / n_tiles, t = u % n_tiles;
