@@ -387,7 +387,8 @@ class VisEngine:
         return n + (ws.numel() if ws is not None else 0)
 
     def launches_per_run(self) -> int:
-        per_f = 3 if self.method == "MatMul" else 2
+        # per frequency: tau/Z, then mvb_herk + mvb_herk_reduce or vecdot_kernel + its slice reduction
+        per_f = 3
         # count + scatter + beam (+ frame), per frequency (+ its beam for a beamfits beam)
         per_chunk = 2 + int(not self.chromatic) + (per_f + int(self.chromatic)) * len(self.freqs) + int(self.pol_sky)
         n = len(self.lsts) * (1 + self.nchunks * per_chunk)
