@@ -6,10 +6,11 @@ and chunk with a device synchronisation after each stage (cpu/cpu.py:247-272,
 gpu/gpu.py:197-254).  Here one job is one stream of launches:
 
     for t:      mvb_rotate -> (per chunk) mvb_horizon_compact -> mvb_beam_*
-      for f:    mvb_tau_z -> mvb_herk + mvb_herk_reduce   (or mvb_vecdot)
+      for f:    [mvb_beam_* for a beamfits beam] -> mvb_tau_z -> mvb_herk + mvb_herk_reduce
+                (or mvb_vecdot for a short pair list)
 
-Rotation, selection and beam interpolation depend on time only and are done once
-per time for all frequencies.  The above-horizon count never leaves the device:
+Rotation, selection and (for an achromatic beam) beam interpolation depend on
+time only and are done once per time for all frequencies.  The above-horizon count never leaves the device:
 every later kernel reads it from ``n_above`` and sizes its work from it, so the
 whole job can be captured once as a CUDA graph and replayed.
 """
