@@ -232,6 +232,7 @@ class VisEngine:
             self.zscale = _lib.f16_scale(zmax * (1 + 2**-10))
         self._graph = None
         self._allocated = False
+        self._uploaded = False
 
     # ------------------------------------------------------------------ setup
     def allocate(self):
@@ -307,6 +308,7 @@ class VisEngine:
         if self.pol_sky and N:
             self.coh[:, :N].copy_(_pinned(self.coh_host), non_blocking=True)
             self.radec[:, :N].copy_(_pinned(self.radec_host), non_blocking=True)
+        self._uploaded = True
 
     def h2d_bytes(self) -> int:
         n = self.eci_host.nbytes + self.antpos_host.nbytes + (0 if self.pol_sky else self.flux_host.nbytes)
@@ -397,7 +399,7 @@ class VisEngine:
 
     def run(self, check: bool = True) -> torch.Tensor:
         """Run the job on the current stream; returns the device visibilities."""
-        if not self._allocated:
+        if not self._uploaded:
             self.upload()
         self.status.zero_()
         if self._graph is not None:
@@ -418,7 +420,7 @@ class VisEngine:
         allocated host pages (slower than the copy itself), overlap the compute
         of the later time steps.
         """
-        if not self._allocated:
+        if not self._uploaded:
             self.upload()
         shape = tuple(self.vis.shape)
         dtype = np.complex64 if self.ctype == torch.complex64 else np.complex128
@@ -474,7 +476,7 @@ class VisEngine:
 
     def capture(self):
         """Capture the launch sequence as one CUDA graph (run once uncaptured first)."""
-        if not self._allocated:
+        if not self._uploaded:
             self.upload()
         self.enqueue()  # warm-up: function attributes, lazy module loading
         torch.cuda.synchronize()

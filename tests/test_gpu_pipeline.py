@@ -283,3 +283,18 @@ def test_one_beam_per_antenna(device):
     for mode in ("fp16x3", "bf16x6"):
         vis = _engine(cfg, precision=2, gemm_mode=mode).run().cpu().numpy()
         assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6, mode
+
+
+def test_allocate_then_run_uploads_inputs(device):
+    """An engine allocated explicitly still uploads its inputs before the first run."""
+    cfg = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=2000, nfreq=1, ntimes=1, nant=10, seed=9)
+    spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
+                           lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
+                           polarized=True, precision=2)
+    e1 = VisEngine(spec)
+    e1.allocate()
+    v1 = e1.run().cpu().numpy()
+    v2 = VisEngine(spec).run().cpu().numpy()
+    assert np.abs(v1).max() > 0
+    np.testing.assert_array_equal(v1, v2)
+
