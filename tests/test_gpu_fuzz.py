@@ -3,7 +3,8 @@ FP64 oracle, drawn across the shapes the kernels branch on -- antenna counts on
 both sides of the 64- and 128-row block boundaries, one or two feeds, empty and
 non-empty skies, every split mode, both products (MatMul, VectorDot with a
 random pair list on either pair kernel), source chunking, complex64 and
-complex128 output, gridded and Gaussian beams.
+complex128 output, gridded and Gaussian beams, Stokes-I and polarised
+(coherency) skies, the LST rotation and the ERFA-style apparent place.
 
 Tolerance: max |dV| / sqrt(|V_ii| |V_jj|) <= 1e-6 (3e-5 for the bf16x3 split,
 which is not held to 1e-6 anywhere).
@@ -20,7 +21,7 @@ from oracle import oracle as orc  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-CASES = 24
+CASES = 48
 
 
 def _case(seed):
@@ -45,13 +46,20 @@ def _case(seed):
         beam_idx = rng.integers(0, 2, nant)
     else:
         beams, beam_idx = [mv.GaussianBeam(sigma=float(rng.uniform(0.15, 0.4)))], None
+    if polarized and rng.integers(0, 2):
+        fluxes = wl.polarised_sky({"fluxes": fluxes}, seed=seed)
+    rotation = {}
+    if rng.integers(0, 2):
+        time_s = np.sort(rng.uniform(0, 3600, ntimes))
+        rotation = dict(astrom=wl.synthetic_astrom(lsts, -0.536, seed=seed), time_s=time_s,
+                        update_bcrs_every=float(rng.choice([0.0, 300.0])))
     pairs = None
     if use_pairs:
         npairs = int(rng.integers(1, max(2, nant * nant // 3)))
         pairs = np.column_stack([rng.integers(0, nant, npairs), rng.integers(0, nant, npairs)])
     return dict(antpos=antpos, ra=ra, dec=dec, freqs=freqs, fluxes=fluxes, lsts=lsts, beams=beams, beam_idx=beam_idx,
                 polarized=polarized, mode=mode, matprod=matprod, pair_kernel=pair_kernel, pairs=pairs,
-                nchunks=nchunks, precision=precision)
+                nchunks=nchunks, precision=precision, rotation=rotation)
 
 
 def _oracle_beams(beams):
@@ -64,14 +72,17 @@ def test_random_job_vs_oracle(device, seed):
     c = _case(seed)
     ants = {i: tuple(p) for i, p in enumerate(c["antpos"])}
     latitude = -0.536
+    rot_kw = {}
+    if c["rotation"]:
+        rot_kw = dict(coord_method="CoordinateRotationERFA", coord_method_params=c["rotation"])
     vis = mv.simulate_vis(ants, c["fluxes"], c["ra"], c["dec"], c["freqs"], c["lsts"], c["beams"], latitude,
                           polarized=c["polarized"], precision=c["precision"], beam_idx=c["beam_idx"],
                           antpairs=c["pairs"], matprod_method=c["matprod"], pair_product=c["pair_kernel"],
-                          gemm_mode=c["mode"], min_chunks=c["nchunks"])
+                          gemm_mode=c["mode"], min_chunks=c["nchunks"], **rot_kw)
     ref = orc.simulate_vis(ants=ants, fluxes=c["fluxes"], ra=c["ra"], dec=c["dec"], freqs=c["freqs"], lsts=c["lsts"],
                            latitude=latitude, beams=_oracle_beams(c["beams"]), polarized=c["polarized"],
                            beam_idx=c["beam_idx"], antpairs=c["pairs"], matprod="VectorDot" if c["pairs"] is not None
-                           else "MatMul")
+                           else "MatMul", **c["rotation"])
     assert vis.shape == ref.shape, (vis.shape, ref.shape)
     if len(c["ra"]) == 0:
         assert np.all(vis == 0)
@@ -79,7 +90,7 @@ def test_random_job_vs_oracle(device, seed):
     # the metric normalises by the autocorrelations: take them from an all-pairs oracle run
     full = ref if c["pairs"] is None else orc.simulate_vis(
         ants=ants, fluxes=c["fluxes"], ra=c["ra"], dec=c["dec"], freqs=c["freqs"], lsts=c["lsts"], latitude=latitude,
-        beams=_oracle_beams(c["beams"]), polarized=c["polarized"], beam_idx=c["beam_idx"])
+        beams=_oracle_beams(c["beams"]), polarized=c["polarized"], beam_idx=c["beam_idx"], **c["rotation"])
     nfeed = 2 if c["polarized"] else 1
     nant = len(c["antpos"])
     v4 = vis if c["polarized"] else vis[..., None, None]
@@ -96,4 +107,5 @@ def test_random_job_vs_oracle(device, seed):
     worst = float(np.max(np.where(norm > 0, err / scale, err)))
     tol = 3e-5 if c["mode"] == "bf16x3" else 1e-6
     assert worst <= tol, (seed, worst, {k: v for k, v in c.items() if k in ("mode", "matprod", "pair_kernel",
-                                                                            "nchunks", "precision", "polarized")})
+                                                                            "nchunks", "precision", "polarized")},
+                          "erfa" if c["rotation"] else "lst", np.ndim(c["fluxes"]))
