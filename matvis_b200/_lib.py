@@ -8,7 +8,7 @@ Device buffers are torch tensors; only their raw pointers cross the boundary.
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
+from ctypes import c_double, c_float, c_int, c_int64, c_size_t, c_void_p
 from pathlib import Path
 
 import torch

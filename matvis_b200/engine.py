@@ -27,7 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .beams import B200BeamInterpolator, GaussianBeam, GridBeam, beams_at_frequency, is_chromatic
+from .beams import B200BeamInterpolator, GridBeam, beams_at_frequency, is_chromatic
 from .coordinates import (
     ENU_TO_ALTAZ,
     atioq_matrix,

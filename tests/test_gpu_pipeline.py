@@ -14,7 +14,7 @@ torch = pytest.importorskip("torch")
 
 import matvis_b200 as mv  # noqa: E402
 from matvis_b200 import workloads as wl  # noqa: E402
-from matvis_b200.engine import JobSpec, VisEngine, job_from_arrays  # noqa: E402
+from matvis_b200.engine import VisEngine, job_from_arrays  # noqa: E402
 from oracle import oracle as orc  # noqa: E402
 
 from .conftest import golden  # noqa: E402
