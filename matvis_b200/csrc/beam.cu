@@ -153,7 +153,7 @@ static int beam_interp_impl(bool azza, const void *grids, int grid_kind, int nbe
                             int64_t nsrc, void *out, int out_c128, int64_t nout, int32_t *status, void *stream) {
   if (!grids || !params || !out || (nsrc > 0 && !crd) || nbeam <= 0 || nax <= 0 || nfeed <= 0 || nza < 1 || naz < 1 ||
       (grid_kind != 0 && grid_kind != 1) || nout < nsrc || nsrc < 0)
-    return fail(MVB_ERR_ARG, "mvb_beam_interp: bad arguments");
+    return fail(MVB_ERR_ARG, azza ? "mvb_beam_interp_azza: bad arguments" : "mvb_beam_interp: bad arguments");
   if (nout == 0) return MVB_OK;
   const int ncomp = grid_kind == 0 ? 2 : 1;
   const int nplanes = nbeam * nax * nfeed * ncomp;

@@ -59,3 +59,35 @@ def test_argument_errors_are_reported_without_gpu():
     assert b"mvb_herk" in _lib.lib.mvb_last_error()
     with pytest.raises(ValueError):
         _lib.check(rc)
+
+
+def _null_call(name, size):
+    """Every argument null or ``size``: pointers None, integers size, reals 1.0."""
+    import ctypes as ct
+
+    from matvis_b200 import _lib
+
+    args = _lib._SIGNATURES[name][1]
+    vals = [1.0 if a in (ct.c_double, ct.c_float) else None if a in (ct.c_void_p, ct.c_char_p) else size for a in args]
+    return getattr(_lib.lib, name)(*vals)
+
+
+def _status_entry_points():
+    import ctypes as ct
+
+    from matvis_b200 import _lib
+
+    return [n for n, (res, _) in _lib._SIGNATURES.items() if res is ct.c_int and n not in ("mvb_version",
+                                                                                          "mvb_device_info")]
+
+
+@pytest.mark.parametrize("name", _status_entry_points())
+def test_every_entry_point_rejects_null_buffers(name):
+    """With non-zero sizes and null buffers every entry point returns
+    MVB_ERR_ARG and names itself in mvb_last_error -- on the host, before any
+    CUDA call (this runs without a GPU)."""
+    from matvis_b200 import _lib
+
+    assert _null_call(name, 1) == _lib.MVB_ERR_ARG
+    assert _lib.lib.mvb_last_error().decode().startswith(name + ":")
+
