@@ -180,8 +180,8 @@ def zpanel_dtype(mode: int) -> torch.dtype:
 
 
 def zpanel_kblock(mode: int) -> int:
-    """Elements per 64-byte k-block of a split-plane panel (planes are stored
-    [Kcap / KB][Mpad][KB])."""
+    """Elements per 64-byte k-block of a split-plane panel (stored
+    [Kcap / KB][Mpad / 128][planes][128][KB], 16-byte chunks swizzled per row)."""
     return 64 // torch.empty((), dtype=zpanel_dtype(mode)).element_size()
 
 

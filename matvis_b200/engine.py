@@ -21,7 +21,7 @@ import os
 import queue
 import threading
 from concurrent.futures import ThreadPoolExecutor
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 import torch
@@ -544,6 +544,41 @@ def estimate_device_bytes(spec: JobSpec) -> int:
     extra = (16 * Nf * N + 16 * N + 16 * cap) if pol_sky else 0  # coherency, ra/dec, frame rotations
     return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + 8 * nbeam * F * X * cap + panel + ws
                + Nf * Nt * npairs * F * F * csize + extra)
+
+
+def plan_job(spec: JobSpec, budget: float, max_chunks: int = 100) -> tuple[int, int]:
+    """(frequencies per batch, source chunks) for ``spec`` to fit ``budget`` bytes of HBM.
+
+    The output and the per-frequency fluxes grow with the number of frequencies,
+    so a job larger than the budget runs as contiguous frequency batches of equal
+    size, as few as fit (the reference runs one frequency per ``simulate`` call,
+    wrapper.py:180-199, each sized to the free memory, gpu/gpu.py:99-110).  If a
+    single frequency still does not fit, its sources are split into more chunks,
+    up to ``max_chunks`` (the reference's cap, _utils.py:124-209); past that the
+    plan is returned as is and the allocation itself reports the shortfall.
+    """
+    nf = len(spec.freqs)
+    ch0 = max(1, int(spec.nchunks))
+    fl = np.asarray(spec.fluxes)
+
+    def fits(nfb: int, ch: int) -> bool:
+        sub = replace(spec, freqs=np.asarray(spec.freqs)[:nfb], fluxes=fl[:, :nfb], nchunks=ch)
+        return estimate_device_bytes(sub) <= budget
+
+    if nf == 0 or not np.isfinite(budget) or fits(nf, ch0):
+        return max(nf, 1), ch0
+    if fits(1, ch0):
+        lo, hi = 1, nf  # fits(lo) and not fits(hi): the largest batch that fits
+        while hi - lo > 1:
+            mid = (lo + hi) // 2
+            lo, hi = (mid, hi) if fits(mid, ch0) else (lo, mid)
+        nbatch = -(-nf // lo)
+        return -(-nf // nbatch), ch0
+    top = max(ch0, min(int(max_chunks), max(np.asarray(spec.eci).shape[1], 1)))
+    for ch in range(ch0 + 1, top + 1):
+        if fits(1, ch):
+            return 1, ch
+    return 1, top
 
 
 def beam_bound(beams) -> float:

@@ -29,6 +29,7 @@ each time step's visibilities are copied to the host while later steps compute.
 from __future__ import annotations
 
 import logging
+from dataclasses import replace
 
 import numpy as np
 import torch
@@ -37,7 +38,7 @@ from . import _lib
 from ._utils import get_desired_chunks
 from .beams import beams_at_frequency
 from .coordinates import latitude_of, lsts_of, point_source_crd_eq, radec_of
-from .engine import JobSpec, VisEngine, _norm_matprod
+from .engine import JobSpec, VisEngine, _norm_matprod, plan_job
 
 
 logger = logging.getLogger(__name__)
@@ -155,6 +156,8 @@ def simulate_vis(
     gemm_mode: str = "fp16x3",
     k_chunk: int | None = None,
     min_chunks: int = 1,
+    max_memory=np.inf,
+    memory_buffer: float = 0.9,
     device=None,
     **backend_kwargs,
 ):
@@ -162,7 +165,19 @@ def simulate_vis(
 
     ``ants``: {index: (x, y, z)} in metres; ``fluxes``: (NSRCS, NFREQS);
     ``ra``/``dec`` radians; ``freqs`` Hz; ``times`` LSTs (radians).
+
+    The job is sized against ``memory_buffer`` x min(``max_memory``, the device's
+    free memory): one batched job when it fits, else contiguous frequency batches
+    (and, if one frequency does not fit, more source chunks), each written into
+    its slice of one host array (``engine.plan_job``).  ``beam_spline_opts`` and
+    ``max_progress_reports`` are accepted for the reference's keyword set and
+    have no effect; any other keyword is an error, as in the reference.
     """
+    unknown = set(backend_kwargs) - {"max_progress_reports"}
+    if unknown:
+        raise TypeError(f"simulate_vis() got unexpected keyword arguments {sorted(unknown)}")
+    if not 0 < memory_buffer <= 1:
+        raise ValueError("memory_buffer must satisfy 0 < memory_buffer <= 1")
     if not use_gpu:
         raise ValueError("matvis_b200 runs on the GPU only (use_gpu=False has no CPU path here)")
     rot_kw = _check_coord_method(coord_method, coord_method_params)
@@ -184,5 +199,23 @@ def simulate_vis(
     )
     # frequency-dependent (beamfits) beams are interpolated per frequency inside the
     # one batched job (the reference re-interpolates per frequency, wrapper.py:180-199)
-    vis = VisEngine(JobSpec(fluxes=fluxes, freqs=freqs, beams=list(beams), **common), device=device).run_to_host()
+    spec = JobSpec(fluxes=fluxes, freqs=freqs, beams=list(beams), **common)
+    dev = _lib.require_cuda(device)
+    # memory the caching allocator holds but does not use is free for this job too
+    free = torch.cuda.mem_get_info(dev)[0] + torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
+    nfb, nchunks = plan_job(spec, min(max_memory, free) * memory_buffer)
+    if nfb >= freqs.size and nchunks == spec.nchunks:
+        vis = VisEngine(spec, device=dev).run_to_host()
+        return vis if polarized else vis[..., 0, 0]
+    logger.info("simulate_vis: %d frequencies in batches of %d, %d source chunks", freqs.size, nfb, nchunks)
+    vis = None
+    for f0 in range(0, freqs.size, nfb):
+        sub = replace(spec, fluxes=fluxes[:, f0 : f0 + nfb], freqs=freqs[f0 : f0 + nfb], nchunks=nchunks)
+        eng = VisEngine(sub, device=dev)
+        eng.allocate()
+        if vis is None:
+            vis = np.empty((freqs.size,) + tuple(eng.vis.shape[1:]),
+                           dtype=np.complex64 if precision == 1 else np.complex128)
+        eng.run_to_host(out=vis[f0 : f0 + len(sub.freqs)])
+        del eng
     return vis if polarized else vis[..., 0, 0]

@@ -77,6 +77,72 @@ def test_resolve_product():
         _resolve_product(spec(matprod="VectorDot", pair_product="dense"))
 
 
+
+def _plan_spec(nf=24, nsrc=200_000, nant=64, polarized=True, pol_sky=False):
+    fl = np.ones((nsrc, nf, 2, 2)) if pol_sky else np.ones((nsrc, nf))
+    return JobSpec(antpos=np.zeros((nant, 3)), eci=np.zeros((3, nsrc)), fluxes=fl, freqs=np.linspace(1e8, 2e8, nf),
+                   lsts=np.zeros(6), latitude=0.0, beams=[], polarized=polarized)
+
+
+@pytest.mark.parametrize("pol_sky", [False, True])
+def test_plan_job_frequency_batches(pol_sky):
+    """A job over the memory budget runs as the fewest equal frequency batches that fit."""
+    from dataclasses import replace
+
+    from matvis_b200.engine import estimate_device_bytes, plan_job
+
+    spec = _plan_spec(pol_sky=pol_sky)
+    full = estimate_device_bytes(spec)
+    assert plan_job(spec, np.inf) == (24, 1)
+    assert plan_job(spec, full) == (24, 1)
+
+    def size(nfb, ch=1):
+        return estimate_device_bytes(replace(spec, freqs=spec.freqs[:nfb], fluxes=spec.fluxes[:, :nfb], nchunks=ch))
+
+    for frac in (0.999, 0.4, 0.1, 0.0):
+        budget = size(1) + frac * (full - size(1))
+        nfb, ch = plan_job(spec, budget)
+        nbatch = -(-24 // nfb)
+        assert ch == 1 and nfb < 24 and size(nfb) <= budget
+        assert nfb == -(-24 // nbatch)  # batches as equal as the count allows
+        assert size(-(-24 // (nbatch - 1))) > budget  # one batch fewer would not fit
+
+
+def test_plan_job_source_chunks():
+    """When one frequency alone does not fit, the sources are split into more chunks."""
+    from dataclasses import replace
+
+    from matvis_b200.engine import estimate_device_bytes, plan_job
+
+    spec = _plan_spec(nf=3)
+    one = replace(spec, freqs=spec.freqs[:1], fluxes=spec.fluxes[:, :1])
+    budget = estimate_device_bytes(replace(one, nchunks=4))
+    nfb, ch = plan_job(spec, budget)
+    assert nfb == 1 and 1 < ch <= 4
+    assert estimate_device_bytes(replace(one, nchunks=ch)) <= budget
+    assert estimate_device_bytes(replace(one, nchunks=ch - 1)) > budget
+    assert plan_job(spec, 1.0) == (1, 100)  # past the cap the plan stands and allocation reports it
+    assert plan_job(_plan_spec(nf=3, nsrc=10), 1.0) == (1, 10)  # no more chunks than sources
+    assert plan_job(replace(spec, nchunks=7), np.inf) == (3, 7)
+
+
+def test_simulate_vis_keywords():
+    """Reference keywords are accepted; an unknown keyword is a TypeError, as in the reference."""
+    import inspect
+
+    from matvis_b200.simulate import simulate_vis
+
+    params = inspect.signature(simulate_vis).parameters
+    for name in ("max_memory", "memory_buffer", "min_chunks", "source_buffer", "beam_spline_opts", "coord_method",
+                 "coord_method_params", "matprod_method"):
+        assert name in params, name
+    with pytest.raises(TypeError, match="bogus"):
+        simulate_vis({0: (0, 0, 0)}, np.ones((1, 1)), np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), [], 0.0,
+                     bogus=1)
+    with pytest.raises(ValueError, match="memory_buffer"):
+        simulate_vis({0: (0, 0, 0)}, np.ones((1, 1)), np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), [], 0.0,
+                     memory_buffer=1.5)
+
 @pytest.mark.parametrize("n", [1_000_000, 300_001, 131_072, 5])
 def test_point_source_crd_eq_threads_bit_identical(n):
     """The threaded unit vectors equal the single numpy pass bit for bit (the
