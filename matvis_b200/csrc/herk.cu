@@ -55,7 +55,7 @@
 namespace mvb {
 
 constexpr int kEpiWarps = 16;
-constexpr int kPlanExtra = 32;  // extra k-slices the split planner may add to fill the SMs
+constexpr int kPlanExtra = 31;  // extra k-slices the split planner may add to fill the SMs (one per lane)
 constexpr int kHerkThreads = 64 + 32 * kEpiWarps;
 constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s
 constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
@@ -93,31 +93,39 @@ __device__ __forceinline__ void product_terms(int nprod, int q, uint32_t &pa, ui
 // Splits K_valid into nsplit equal slices of kc columns (a multiple of 64, at
 // most kmax), choosing nsplit in [ceil(K/kmax), +kPlanExtra] so that
 // n_tiles * nsplit work units fill whole waves of nsm SMs as evenly as possible
-// (ties: fewer slices).  Used identically by the product and its reduction.
-__host__ __device__ inline void plan_splits(int64_t kvalid, int n_tiles, int kmax, int nsm, int &nsplit, int64_t &kc) {
-  if (kvalid <= 0) {
+// (a candidate replaces the best so far only when 1e-3 more efficient, so ties
+// keep fewer slices; the scan stops at the first candidate of 64 columns).
+// Each lane of a warp evaluates one candidate and the scan runs over the
+// shuffled efficiencies, so every warp reaches the same plan in one candidate's
+// arithmetic; every lane of the warp must call it.  Used identically by the
+// product and its reductions.
+__device__ __forceinline__ void plan_splits(int64_t kvalid, int n_tiles, int kmax, int nsm, int &nsplit, int64_t &kc) {
+  if (kvalid <= 0) {  // kvalid is uniform over the grid
     nsplit = 0;
     kc = kmax;
     return;
   }
   const int64_t nmin = (kvalid + kmax - 1) / kmax;
-  double best_eff = -1.0;
-  nsplit = (int)nmin;
-  kc = kmax;
-  for (int64_t n = nmin; n <= nmin + kPlanExtra; ++n) {
-    int64_t c = (kvalid + n - 1) / n;
-    c = ((c + 63) / 64) * 64;
-    const int64_t ne = (kvalid + c - 1) / c;
-    const int64_t units = (int64_t)n_tiles * ne;
-    const int64_t waves = (units + nsm - 1) / nsm;
-    const double eff = (double)units / (double)(waves * nsm);
-    if (eff > best_eff + 1e-3) {
-      best_eff = eff;
-      nsplit = (int)ne;
-      kc = c;
+  const int64_t n = nmin + (threadIdx.x & 31);
+  int64_t c = (kvalid + n - 1) / n;
+  c = ((c + 63) / 64) * 64;
+  const int64_t ne = (kvalid + c - 1) / c;
+  const int64_t units = (int64_t)n_tiles * ne;
+  const int64_t waves = (units + nsm - 1) / nsm;
+  const double eff = (double)units / (double)(waves * nsm);
+  const unsigned stop = __ballot_sync(0xffffffffu, c <= 64);
+  double best = -1.0;
+  int win = 0;
+  for (int l = 0; l <= kPlanExtra; ++l) {
+    const double e = __shfl_sync(0xffffffffu, eff, l);
+    if (e > best + 1e-3) {
+      best = e;
+      win = l;
     }
-    if (c <= 64) break;
+    if ((stop >> l) & 1u) break;
   }
+  nsplit = (int)__shfl_sync(0xffffffffu, ne, win);
+  kc = __shfl_sync(0xffffffffu, c, win);
 }
 
 // Valid K columns: (source count) x (columns per source), clamped to the panel.
@@ -424,16 +432,16 @@ __global__ void __launch_bounds__(256)
   const float4 *pre = reinterpret_cast<const float4 *>(part + (size_t)t * (256 * 128) + c * 128 + r0);
   const float4 *pim = reinterpret_cast<const float4 *>(part + (size_t)t * (256 * 128) + (128 + c) * 128 + r0);
   int s = 0;
-  // four slices per step: 8 independent 16-byte loads in flight, sums in slice order
-  for (; s + 4 <= nsplit; s += 4) {
-    float4 vr[4], vi[4];
+  // eight slices per step: 16 independent 16-byte loads in flight, sums in slice order
+  for (; s + 8 <= nsplit; s += 8) {
+    float4 vr[8], vi[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       vr[u] = __ldg(pre + (s + u) * sstride);
       vi[u] = __ldg(pim + (s + u) * sstride);
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       are[0].add(vr[u].x), are[1].add(vr[u].y), are[2].add(vr[u].z), are[3].add(vr[u].w);
       aim[0].add(vi[u].x), aim[1].add(vi[u].y), aim[2].add(vi[u].z), aim[3].add(vi[u].w);
     }
