@@ -411,3 +411,30 @@ def test_redundant_pairs_errors_and_capacity():
                                       1, ctypes.byref(n))
     assert rc == _lib.MVB_ERR_OVERFLOW and n.value == 3 and out.tolist() == [[0, 1]]
     assert get_redundancies(np.zeros((0, 0, 2))) == []
+
+
+def test_config5_job_stream_ranges():
+    """The served-form stream: Poisson arrivals and per-job sizes in their stated ranges."""
+    jobs = workloads.config5_jobs(njobs=300, rate_hz=20.0, nsrc_max=5000)
+    t = np.array([a for a, _ in jobs])
+    assert np.all(np.diff(t) > 0) and abs(np.mean(np.diff(t)) - 1 / 20.0) < 0.2 / 20.0
+    for _, spec in jobs:
+        nant, nsrc = len(spec.antpos), spec.eci.shape[1]
+        assert 16 <= nant <= 512 and 1000 <= nsrc <= 5000
+        assert 1 <= len(spec.freqs) <= 32 and 1 <= len(spec.lsts) <= 16
+        assert spec.fluxes.shape == (nsrc, len(spec.freqs)) and np.all(np.diff(spec.freqs) >= 0)
+        assert np.all(np.hypot(spec.antpos[:, 0], spec.antpos[:, 1]) <= 300.0)
+        assert (len(spec.beams) == 1) and (spec.polarized == (not hasattr(spec.beams[0], "sigma")))
+    assert 0 < sum(s.polarized for _, s in jobs) < len(jobs)
+
+
+def test_latency_summary():
+    from matvis_b200.serve import JobResult, latency_summary
+
+    res = {i: JobResult(jid=i, vis=None, latency_s=0.1 * (i + 1), queue_s=0.01 * i, terms=1e9) for i in range(10)}
+    res[10] = JobResult(jid=10, vis=None, latency_s=9.0, queue_s=0.0, terms=5e9, error="boom")
+    s = latency_summary(res)
+    assert s["jobs"] == 10 and s["errors"] == 1 and s["terms"] == 1e10
+    assert s["p50_s"] == pytest.approx(0.55) and s["p99_s"] == pytest.approx(np.percentile(np.arange(1, 11) / 10, 99))
+    assert s["mean_queue_s"] == pytest.approx(0.045)
+    assert latency_summary({}) == {"jobs": 0}
