@@ -438,3 +438,23 @@ def test_latency_summary():
     assert s["p50_s"] == pytest.approx(0.55) and s["p99_s"] == pytest.approx(np.percentile(np.arange(1, 11) / 10, 99))
     assert s["mean_queue_s"] == pytest.approx(0.045)
     assert latency_summary({}) == {"jobs": 0}
+
+
+def test_public_api_and_rotation_registry():
+    """Every exported name resolves; rotation plugins register by class name
+    (core/coords.py:32-38), including subclasses defined by a caller."""
+    import matvis_b200 as mv
+    from matvis_b200.coords import CoordinateRotation
+
+    for name in mv.__all__:
+        assert getattr(mv, name, None) is not None, name
+    assert CoordinateRotation._methods["CoordinateRotationLST"] is mv.CoordinateRotationLST
+    assert CoordinateRotation._methods["CoordinateRotationERFA"] is mv.CoordinateRotationERFA
+
+    class CallerRotation(mv.CoordinateRotationLST):
+        pass
+
+    try:
+        assert CoordinateRotation._methods["CallerRotation"] is CallerRotation
+    finally:
+        del CoordinateRotation._methods["CallerRotation"]
