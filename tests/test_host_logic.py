@@ -25,6 +25,25 @@ def test_chunk_planning_matches_reference_table():
         _utils.get_required_chunks(1, 1, 1, 1, 1, 1, 1, 1, 1.0, 0.0)
 
 
+
+_CHUNK_KW = dict(freemem=10 * 1024**3, nax=2, nfeed=2, nant=4, nsrc=100, nbeam=2, nbeampix=0, precision=1)
+
+
+def test_required_chunks_properties():
+    """The properties the reference's own utils tests check (tests/test_utils.py:38-82)."""
+    assert _utils.get_required_chunks(**_CHUNK_KW) >= 1
+    assert _utils.get_required_chunks(**_CHUNK_KW, memory_buffer=0.1) >= \
+        _utils.get_required_chunks(**_CHUNK_KW, memory_buffer=0.9)
+    assert _utils.get_required_chunks(**{**_CHUNK_KW, "freemem": 10**18}, memory_buffer=1.0) == 1
+    assert _utils.get_required_chunks(**_CHUNK_KW, memory_buffer=1.0) >= 1
+    for bad in (1.1, 0.0, -0.5):
+        with pytest.raises(ValueError, match="memory_buffer"):
+            _utils.get_required_chunks(**_CHUNK_KW, memory_buffer=bad)
+    # less memory never needs fewer chunks; the count stops at 100
+    counts = [_utils.get_required_chunks(**{**_CHUNK_KW, "nsrc": 10**6, "freemem": fm}) for fm in
+              (2**34, 2**30, 2**28, 2**26, 2**20)]
+    assert counts == sorted(counts) and counts[-1] == 100
+
 def test_desired_chunks_counts_grid_pixels():
     beams = workloads.dipole_beams(np.random.default_rng(0), 2, dgrid_deg=10.0)
     n, per = _utils.get_desired_chunks(2**40, 3, beams, 2, 2, 10, 1000, 1)
