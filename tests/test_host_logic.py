@@ -477,3 +477,19 @@ def test_public_api_and_rotation_registry():
         assert CoordinateRotation._methods["CallerRotation"] is CallerRotation
     finally:
         del CoordinateRotation._methods["CallerRotation"]
+
+
+@pytest.mark.parametrize(("kwarg", "value", "errmsg"), [
+    ("source_buffer", 0.0, "source_buffer must satisfy 0 < source_buffer <= 1"),
+    ("source_buffer", 1.5, "source_buffer must satisfy 0 < source_buffer <= 1"),
+    ("memory_buffer", 1.1, "memory_buffer must satisfy 0 < memory_buffer <= 1"),
+])
+def test_simulate_vis_buffer_validation(kwarg, value, errmsg):
+    """The reference's wrapper validation (tests/test_wrapper.py:39-70), raised
+    before any device work."""
+    from matvis_b200.simulate import simulate_vis
+
+    kw = dict(ants={0: (0.0, 0.0, 0.0), 1: (14.6, 0.0, 0.0)}, fluxes=np.ones((15, 1)), ra=np.linspace(0, 1, 15),
+              dec=np.full(15, -0.5), freqs=np.array([100e6]), times=np.zeros(5), beams=[], telescope_loc=-0.5)
+    with pytest.raises(ValueError, match=errmsg):
+        simulate_vis(**kw, **{kwarg: value})
