@@ -198,10 +198,13 @@ int mvb_absmax(const void *z, int z_c128, int64_t n, float *out, void *stream);
  * the workspace must be 16-byte aligned. */
 size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
 /* Upper-triangle 128 x 128 complex tiles of V = conj(Z) Z^T over K_valid
- * columns, split into k_chunk-column slices (a multiple of 64), on the tcgen05
- * tensor cores with TMEM accumulators, fed by one bulk copy (cp.async.bulk) per
- * operand and stage from the panel's stored shared-memory image; mode
- * MVB_GEMM_* selects the split precision.
+ * columns, on the tcgen05 tensor cores with TMEM accumulators, fed by one bulk
+ * copy (cp.async.bulk) per operand and stage from the panel's stored
+ * shared-memory image; mode MVB_GEMM_* selects the split precision.
+ * K_valid is cut into equal k-slices of at most k_chunk columns (a multiple of
+ * 64).  Their count, between ceil(K_valid / k_chunk) and 31 more, is chosen on
+ * the device from K_valid so that tiles x slices fills whole waves of SMs; one
+ * partial tile is written per (k-slice, tile).
  * drain_ksteps (1, 2 or 4; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
  * number of 32-byte k-steps summed in one TMEM block before the block is added
  * to FP32 registers: the tensor core rounds its accumulator toward zero at every
@@ -218,6 +221,8 @@ int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t 
  * npairs listed in pairs (int32 [npairs][2]).  out: complex64 (out_c128 = 0)
  * or complex128, each sum multiplied by vscale (1 / s^2 for MVB_GEMM_F16_3,
  * else 1); accumulate != 0 adds to out (the sum over source chunks).
+ * ws, Mpad, Kcap, n_dev / n_host, kmul and k_chunk must be those of the
+ * mvb_herk call that filled ws: the slice plan is recomputed from them.
  * Replaces MatProd.sum_chunks and the host transpose/gather of
  * GPUMatMul.sum_chunks (core/matprod.py:103-115, gpu/matprod.py:38-63). */
 int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
