@@ -91,3 +91,34 @@ def test_every_entry_point_rejects_null_buffers(name):
     assert _null_call(name, 1) == _lib.MVB_ERR_ARG
     assert _lib.lib.mvb_last_error().decode().startswith(name + ":")
 
+
+
+def _c_to_ctypes(decl: str):
+    decl = decl.strip()
+    if "*" in decl:
+        return "ptr"
+    base = decl.replace("const", "").split()[0]
+    return {"int": ctypes.c_int, "int64_t": ctypes.c_int64, "size_t": ctypes.c_size_t, "double": ctypes.c_double,
+            "float": ctypes.c_float, "int32_t": ctypes.c_int32}[base]
+
+
+def test_python_binding_matches_header_signatures():
+    """Every ctypes signature has the header's argument count and types (a
+    mismatch would pass garbage through the boundary without an error)."""
+    from matvis_b200 import _lib
+
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    decls = re.findall(r"^\s*([a-z_0-9 ]+?\**)\s*\b(mvb_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", text, flags=re.M | re.S)
+    assert len(decls) == len(declared_symbols())
+    for ret, name, args in decls:
+        res, argtypes = _lib._SIGNATURES[name]
+        params = [] if args.strip() in ("", "void") else [a for a in args.split(",")]
+        assert len(params) == len(argtypes), name
+        for i, (p, t) in enumerate(zip(params, argtypes)):
+            want = _c_to_ctypes(p)
+            if want == "ptr":
+                assert t in (ctypes.c_void_p, ctypes.c_char_p), (name, i, p)
+            else:
+                assert t is want, (name, i, p, t)
+        want_ret = "ptr" if "*" in ret else _c_to_ctypes(ret)
+        assert (res in (ctypes.c_void_p, ctypes.c_char_p)) if want_ret == "ptr" else res is want_ret, name
