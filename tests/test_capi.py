@@ -122,3 +122,17 @@ def test_python_binding_matches_header_signatures():
                 assert t is want, (name, i, p, t)
         want_ret = "ptr" if "*" in ret else _c_to_ctypes(ret)
         assert (res in (ctypes.c_void_p, ctypes.c_char_p)) if want_ret == "ptr" else res is want_ret, name
+
+
+def test_integration_binding_example_matches_library():
+    """The reference-side ctypes stub shown in INTEGRATION.md binds the same signatures."""
+    from matvis_b200 import _lib
+
+    text = (ROOT / "INTEGRATION.md").read_text()
+    alias = {"_p": ctypes.c_void_p, "_i": ctypes.c_int, "_i64": ctypes.c_int64, "_sz": ctypes.c_size_t,
+             "_f": ctypes.c_float, "_d": ctypes.c_double}
+    stubs = re.findall(r"_lib\.(mvb_[a-z0-9_]+)\.argtypes = \[([^\]]*)\]", text)
+    assert len(stubs) >= 5
+    for name, args in stubs:
+        got = [alias[a.strip()] for a in args.split(",")]
+        assert got == list(_lib._SIGNATURES[name][1]), name
