@@ -145,8 +145,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def load_config(args) -> tuple[dict, str]:
-    """The workload named by --config, with its description."""
+def load_config(args, host_only: bool = False) -> tuple[dict, str]:
+    """The workload named by --config, with its description.  ``host_only``: build
+    it without the GPU library (the reference arm; redundant pairs then come from
+    the oracle's restatement of get_redundancies)."""
     from matvis_b200 import workloads as wl
 
     if args.config == 2:
@@ -168,7 +170,10 @@ def load_config(args) -> tuple[dict, str]:
     if args.sparse and args.config != 3:
         raise SystemExit("--sparse applies to config 3")
     if args.pairs == "redundant":
-        from matvis_b200.pairs import redundant_antpairs
+        if host_only:
+            from oracle.oracle import redundant_antpairs
+        else:
+            from matvis_b200.pairs import redundant_antpairs
 
         cfg["antpairs"] = redundant_antpairs(cfg["antpos"])
         desc += f"; {len(cfg['antpairs'])} redundant-baseline pairs on the VectorDot path"
@@ -195,12 +200,14 @@ def terms_per_job(cfg, astrom=None) -> tuple[float, np.ndarray]:
 
 
 # ----------------------------------------------------------------------------- plain GPU path
-def plain_gpu_sample(cfg, nslices: int = 6):
+def plain_gpu_sample(cfg, slices):
     """Complex64 torch restatement of the reference GPU driver (gpu/gpu.py:197-254) on
-    `nslices` (f, t) slices: FP32 rotation, horizon gather with a host count,
+    the listed (f, t) slices: FP32 rotation, horizon gather with a host count,
     bilinear beam via grid_sample, FP32 phase, per-antenna Z loop, full complex64
     matmul (TF32 off) or, for a pair list, one matmul per pair (GPUVectorDot,
-    gpu/matprod.py:66-98), device->host copy of the result per slice."""
+    gpu/matprod.py:66-98), device->host copy of the result per slice.  The first
+    slice runs once untimed (warm-up).  Returns the rate and, per listed slice, the
+    host visibilities in the reference layout (npairs, F, F)."""
     import torch
     import torch.nn.functional as Fnn
 
@@ -220,9 +227,8 @@ def plain_gpu_sample(cfg, nslices: int = 6):
     flux = torch.as_tensor(np.sqrt(0.5 * cfg["fluxes"]), dtype=torch.float32, device=dev)
     terms = 0.0
     times = []
-    for k in range(nslices + 1):
-        f = k % len(cfg["freqs"])
-        t = k % len(cfg["lsts"])
+    out = []
+    for k, (f, t) in enumerate([slices[0]] + list(slices)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         R = torch.as_tensor(eci_to_enu_matrix(cfg["lsts"][t], cfg["latitude"]), dtype=torch.float32, device=dev)
@@ -250,70 +256,117 @@ def plain_gpu_sample(cfg, nslices: int = 6):
         else:
             zz = z.view(nant, F, X * n)
             v = torch.stack([zz[aj] @ zz[ai].conj().T for ai, aj in pairs])
-        _ = v.cpu()
+        vh = v.cpu()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        if k > 0:  # first slice is warm-up
+        if k > 0:  # the first pass is warm-up
             times.append(dt)
             terms += npairs * n
-    return {"value": terms / sum(times), "unit": UNIT, "slices": nslices,
-            "sample": f"{nslices} (f, t) slices of the workload, complex64, TF32 off"}
+            if pairs is None:  # V[i F + q, j F + p] -> out[i A + j, p, q] (cpu/matprod.py:21-30)
+                vh = vh.numpy().reshape(nant, F, nant, F).transpose(0, 2, 3, 1).reshape(nant * nant, F, F)
+            else:
+                vh = vh.numpy()
+            out.append(vh)
+    return {"value": terms / sum(times), "unit": UNIT, "slices": len(slices),
+            "sample": f"{len(slices)} (f, t) slices of the workload, complex64, TF32 off"}, out
 
 
 # ----------------------------------------------------------------------------- CPU oracle
-def cpu_oracle_sample(cfg, nsrc_sample: int, nslices: int = 1):
-    """FP64 oracle (reference CPU algorithm) on `nslices` slices with a source subset."""
+def above_horizon(cfg, t, astrom=None) -> int:
+    return int(terms_per_job(dict(cfg, lsts=np.asarray(cfg["lsts"])[t:t + 1], freqs=np.zeros(1), antpairs=None),
+                             None if astrom is None else astrom[t:t + 1])[1][0])
+
+
+def accuracy_slices(cfg) -> list[tuple[int, int]]:
+    """Three (f, t) slices spread over the job: first, middle, last."""
+    nf, nt = len(cfg["freqs"]), len(cfg["lsts"])
+    out = []
+    for s in [(0, 0), (nf // 2, nt // 2), (nf - 1, nt - 1)]:
+        if s not in out:
+            out.append(s)
+    return out
+
+
+def oracle_slices(cfg, slices, nsrc_sample: int | None = None):
+    """FP64 oracle (the reference CPU algorithm) on the listed (f, t) slices, all
+    antennas and pairs; the sky is the workload's own, or a seeded subset of
+    ``nsrc_sample`` sources.  Returns (terms/s, seconds, sample text, [vis per
+    slice, (nant^2, 2, 2) complex128])."""
     from oracle import oracle as orc
 
     from matvis_b200 import workloads as wl
 
-    sub = wl.subset(cfg, nsrc=nsrc_sample, nfreq=1, ntimes=1, seed=11)
-    sub["antpairs"] = None  # the oracle computes all pairs; the count below uses all of them
+    sub = cfg
+    if nsrc_sample is not None and nsrc_sample < len(cfg["ra"]):
+        sub = wl.subset(cfg, nsrc=nsrc_sample, seed=11)
     beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in sub["beams"]]
     antpos = np.asarray(sub["antpos"])
     terms = 0.0
+    vis = []
     t0 = time.perf_counter()
-    for _ in range(nslices):
-        vis = orc.simulate(antpos=antpos, freq=float(sub["freqs"][0]), lsts=sub["lsts"], latitude=sub["latitude"],
-                           ra=sub["ra"], dec=sub["dec"], I_sky=sub["fluxes"][:, 0], beam_list=beams, polarized=True,
-                           beam_idx=sub["beam_idx"])
-        n = terms_per_job(sub)[1].sum()
-        terms += len(antpos) ** 2 * n
+    for f, t in slices:
+        v = orc.simulate(antpos=antpos, freq=float(sub["freqs"][f]), lsts=np.asarray(sub["lsts"])[t:t + 1],
+                         latitude=sub["latitude"], ra=sub["ra"], dec=sub["dec"], I_sky=sub["fluxes"][:, f],
+                         beam_list=beams, polarized=True, beam_idx=sub["beam_idx"])
+        vis.append(v[0])
+        terms += len(antpos) ** 2 * above_horizon(sub, t)
     dt = time.perf_counter() - t0
-    del vis
-    srcs = (f"all {len(cfg['ra'])} sources" if nsrc_sample >= len(cfg["ra"])
+    srcs = (f"all {len(cfg['ra'])} sources" if sub is cfg
             else f"{nsrc_sample} of {len(cfg['ra'])} sources (seeded subset)")
-    return terms / dt, dt, f"{nslices} (f, t) slice(s) of the workload, all {len(antpos)} antennas, {srcs}, " \
-                           f"FP64 numpy/scipy oracle"
+    return terms / dt, dt, (f"{len(slices)} (f, t) slice(s) {list(slices)} of the workload, all {len(antpos)} "
+                            f"antennas and pairs, {srcs}, FP64 numpy/scipy oracle"), vis
+
+
+def workload_config(args, cfg, desc, terms, counts) -> dict:
+    """The ``config`` object of the JSON line, identical for both arms run with the
+    same arguments (it names the workload only; how each arm computes it is
+    reported elsewhere in the line)."""
+    matprod = "VectorDot" if args.sparse or args.pairs != "all" else "MatMul"
+    nant = len(cfg["antpos"])
+    mpad = -(-2 * nant // 128) * 128
+    plane_bytes = {"fp16x3": 8, "bf16x3": 8, "bf16x6": 12, "tf32x3": 16}[args.gemm_mode]
+    panel_gb = mpad * 2 * int(np.max(counts)) * plane_bytes / 1e9
+    return {
+        "workload": desc,
+        "matprod": matprod,
+        "gemm_mode": args.gemm_mode,
+        "terms_per_job": terms,
+        "above_horizon_per_time": [int(c) for c in counts],
+        "l2": f"inputs larger than L2: {len(cfg['ra'])} sources, and each (f, t) slice's Z panel is "
+              f"{panel_gb:.2f} GB (126 MB L2)",
+    }
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    from matvis_b200 import workloads as wl
-
-    cfg, desc = load_config(args)
+    cfg, desc = load_config(args, host_only=True)
+    terms, counts = terms_per_job(cfg)
     # one (f, t) slice per step: all sources of config 2 (a few seconds on the host
     # cores), a 196,608-source seeded subset of the larger skies
     nsrc_sample = min(len(cfg["ra"]), 196_608)
-    for _ in range(max(args.warmup, 0)):
-        cpu_oracle_sample(cfg, nsrc_sample)
+    sl = accuracy_slices(cfg)
+    for i in range(max(args.warmup, 0)):
+        oracle_slices(cfg, [sl[i % len(sl)]], nsrc_sample)
     vals, dts = [], []
-    for _ in range(args.steps):
-        v, dt, sample = cpu_oracle_sample(cfg, nsrc_sample)
+    for i in range(args.steps):
+        v, dt, sample, _ = oracle_slices(cfg, [sl[i % len(sl)]], nsrc_sample)
         vals.append(v)
         dts.append(dt)
     value = float(np.median(vals))
     cores = os.cpu_count()
+    sample = sample.replace(str([sl[(args.steps - 1) % len(sl)]]), "(one per step, cycling over %s)" % sl)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.median(dts)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "sample": sample},
+        "config": workload_config(args, cfg, desc, terms, counts),
+        "sample": sample,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference package not importable here (astropy, pyuvdata absent); its CPU algorithm is timed "
-                "through the FP64 oracle restatement (oracle/oracle.py), pinned to fixtures from the reference code",
+                "through the FP64 oracle restatement (oracle/oracle.py), pinned to fixtures from the reference "
+                "code.  This arm loads no library of this repository.",
     }
     print(json.dumps(line), flush=True)
 
@@ -500,15 +553,12 @@ def run_b200(args, rank, world, local_rank):
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": dtype,
         "data": f"synthetic (seeded; {sky}, HERA-350-like array, dipole-like beams)",
-        "config": {
-            "workload": desc,
-            "matprod": matprod, "pair_kernel": eng.pair_kernel,
+        "config": workload_config(args, cfg, desc, terms, counts),
+        "implementation": {
+            "pair_kernel": eng.pair_kernel,
             "gemm_mode": None if eng.method == "VectorDot" else args.gemm_mode, "k_chunk": kc,
-            "terms_per_job": terms,
-            "above_horizon_per_time": [int(c) for c in counts],
-            "l2": "inputs larger than L2 (Z panel ~%.1f GB per slice)" % (panel.data.numel() *
-                                                                          panel.data.element_size() / 1e9 * kvalid /
-                                                                          panel.Kcap),
+            "z_panel": "%.2f GB per slice" % (panel.data.numel() * panel.data.element_size() / 1e9 * kvalid /
+                                              panel.Kcap),
             "parallelism": "replicas (one job per GPU)" if world > 1 else "1 GPU",
             "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, " + product,
         },
@@ -517,16 +567,38 @@ def run_b200(args, rank, world, local_rank):
         "clocks": clocks,
     }
 
+    slices = accuracy_slices(cfg)
+    full_sky = len(cfg["ra"]) <= 196_608  # the oracle runs on the timed job's own sky
+    ovis = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         # three (f, t) slices: about 10 s of FP64 work on the host cores (all sources of
         # config 2, a 196,608-source seeded subset of the larger skies)
-        v, dt, sample = cpu_oracle_sample(cfg, min(len(cfg["ra"]), 196_608), nslices=3)
+        v, dt, sample, ovis = oracle_slices(cfg, slices, None if full_sky else 196_608)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample,
                                 "seconds": dt}
+        if full_sky and cfg.get("antpairs") is None and args.sky == "stokes" and args.rotation == "lst":
+            from oracle.oracle import cosine_error_metric
+
+            errs = [cosine_error_metric(eng.vis[f, t].cpu().numpy(), ref, 2) for (f, t), ref in zip(slices, ovis)]
+            line["accuracy"] = {
+                "max_norm_err": max(errs), "per_slice": errs, "slices": slices, "bar": 1e-6,
+                "of": "the timed job's own visibilities (the last graph replay) at these (f, t) slices",
+                "metric": "max over outputs of |V - V_oracle| / sqrt(|V_ii| |V_jj|), against the FP64 oracle on "
+                          "all sources, antennas and pairs",
+            }
     if rank == 0 and not args.skip_plain:
         try:
-            line["plain_gpu"] = plain_gpu_sample(cfg)
-            line["vs_plain_gpu"] = value / world / line["plain_gpu"]["value"]
+            extra = [((f + 7) % len(cfg["freqs"]), (t + 5) % len(cfg["lsts"])) for f, t in slices]
+            pg, pvis = plain_gpu_sample(cfg, slices + extra)
+            line["plain_gpu"] = pg
+            line["vs_plain_gpu"] = value / world / pg["value"]
+            if ovis is not None and "accuracy" in line:
+                from oracle.oracle import cosine_error_metric
+
+                perr = [cosine_error_metric(v, ref, 2) for v, ref in zip(pvis, ovis)]
+                pg["max_norm_err"] = max(perr)
+                pg["per_slice_err"] = perr
+                line["accuracy"]["plain_gpu_max_norm_err"] = max(perr)
         except Exception as exc:  # the denominator is informative only
             line["plain_gpu"] = {"error": repr(exc)[:200]}
 

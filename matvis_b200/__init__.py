@@ -3,54 +3,66 @@
 Drop-in for ``matvis.simulate_vis`` / ``simulate`` and the backend plugin classes
 (``CoordinateRotation``, ``BeamInterpolator``, ``TauCalculator``, ``ZMatrixCalc``,
 ``MatProd``), computing on hand-written CUDA kernels behind the C ABI of
-``include/matvis_b200.h``.  There is no CPU fallback: importing the package
-without the built library raises ImportError.
+``include/matvis_b200.h``.  There is no CPU fallback.
+
+The names below are resolved on first use: the host-only modules
+(``beam_models``, ``coordinates``, ``workloads``, ``_utils``, ``beamfits``,
+``sharding``) import without the GPU library, and the first access to anything
+that computes (``simulate_vis``, the plugin classes, ``VisEngine`` ...) loads
+``libmatvis_b200.so`` and raises ImportError if it is not built.
 """
 
-from . import _lib  # noqa: F401  (loads libmatvis_b200.so, fails loudly if absent)
-from ._lib import GEMM_MODES, MatvisB200Error
-from ._utils import get_desired_chunks, get_dtypes, get_required_chunks
-from .beamfits import BeamFits, read_beamfits, write_beamfits
-from .beams import B200BeamInterpolator, BeamInterpolator, GaussianBeam, GridBeam
-from .coordinates import SkyCoords, eci_to_enu_matrix, enu_to_az_za, enu_to_eci_matrix, point_source_crd_eq
-from .coords import CoordinateRotation, CoordinateRotationERFA, CoordinateRotationLST
-from .engine import JobSpec, VisEngine
-from .getz import ZMatrixCalc, ZPanel
-from .matprod import B200MatMul, B200VectorDot, MatProd
-from .simulate import simulate, simulate_vis
-from .tau import TauCalculator
+from __future__ import annotations
+
+import importlib
+
+#: public name -> submodule that defines it
+_EXPORTS = {
+    "GEMM_MODES": "_lib",
+    "MatvisB200Error": "_lib",
+    "get_desired_chunks": "_utils",
+    "get_dtypes": "_utils",
+    "get_required_chunks": "_utils",
+    "BeamFits": "beamfits",
+    "read_beamfits": "beamfits",
+    "write_beamfits": "beamfits",
+    "GaussianBeam": "beam_models",
+    "GridBeam": "beam_models",
+    "B200BeamInterpolator": "beams",
+    "BeamInterpolator": "beams",
+    "SkyCoords": "coordinates",
+    "eci_to_enu_matrix": "coordinates",
+    "enu_to_az_za": "coordinates",
+    "enu_to_eci_matrix": "coordinates",
+    "point_source_crd_eq": "coordinates",
+    "CoordinateRotation": "coords",
+    "CoordinateRotationERFA": "coords",
+    "CoordinateRotationLST": "coords",
+    "JobSpec": "engine",
+    "VisEngine": "engine",
+    "ZMatrixCalc": "getz",
+    "ZPanel": "getz",
+    "B200MatMul": "matprod",
+    "B200VectorDot": "matprod",
+    "MatProd": "matprod",
+    "simulate": "wrapper",
+    "simulate_vis": "wrapper",
+    "TauCalculator": "tau",
+}
 
 HAVE_GPU = True
 
-__all__ = [
-    "B200BeamInterpolator",
-    "BeamFits",
-    "B200MatMul",
-    "B200VectorDot",
-    "BeamInterpolator",
-    "CoordinateRotation",
-    "CoordinateRotationERFA",
-    "CoordinateRotationLST",
-    "GEMM_MODES",
-    "GaussianBeam",
-    "GridBeam",
-    "JobSpec",
-    "MatProd",
-    "MatvisB200Error",
-    "SkyCoords",
-    "TauCalculator",
-    "VisEngine",
-    "ZMatrixCalc",
-    "ZPanel",
-    "eci_to_enu_matrix",
-    "enu_to_az_za",
-    "enu_to_eci_matrix",
-    "get_desired_chunks",
-    "get_dtypes",
-    "get_required_chunks",
-    "point_source_crd_eq",
-    "read_beamfits",
-    "simulate",
-    "simulate_vis",
-    "write_beamfits",
-]
+__all__ = sorted(_EXPORTS)
+
+
+def __getattr__(name: str):
+    mod = _EXPORTS.get(name)
+    if mod is None:
+        raise AttributeError(f"module 'matvis_b200' has no attribute {name!r}")
+    value = getattr(importlib.import_module(f".{mod}", __name__), name)
+    globals()[name] = value
+    return value
+
+
+def __dir__():
+    return sorted(set(globals()) | set(_EXPORTS))

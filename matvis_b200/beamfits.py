@@ -32,7 +32,7 @@ from pathlib import Path
 
 import numpy as np
 
-from .beams import GridBeam
+from .beam_models import GridBeam
 
 _BLOCK = 2880
 _CARD = 80

@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .beams import GaussianBeam, GridBeam
+from .beam_models import GaussianBeam, GridBeam
 
 SIDEREAL_DAY_S = 86164.0905
 HERA_LAT = np.deg2rad(-30.72)

@@ -444,6 +444,33 @@ def simulate_vis(
 
 
 # ---------------------------------------------------------------------------
+# Redundant-baseline pair selection (src/matvis/cli.py:273-290, :316)
+# ---------------------------------------------------------------------------
+def get_redundancies(bls, ndecimals: int = 2):
+    """One (i, j), i < j, per class of equal rounded (u, v) up to sign, in the
+    order the reference's double loop meets them; ``cli.py:273-290``."""
+    bls = np.round(np.asarray(bls, dtype=np.float64), decimals=ndecimals)
+    seen = set()
+    pairs = []
+    nant = bls.shape[0]
+    for i in range(nant):
+        for j in range(i + 1, nant):
+            u, v = bls[i, j]
+            if (u, v) not in seen and (-u, -v) not in seen:
+                seen.add((u, v))
+                pairs.append([i, j])
+    return pairs
+
+
+def redundant_antpairs(antpos, ndecimals: int = 2):
+    """(npairs, 2) representatives for the east/north baselines ``pos[j] - pos[i]``
+    (``cli.py:316``)."""
+    antpos = np.asarray(antpos, dtype=np.float64)
+    bls = antpos[np.newaxis, :, :2] - antpos[:, np.newaxis, :2]
+    return np.asarray(get_redundancies(bls, ndecimals), dtype=np.int64).reshape(-1, 2)
+
+
+# ---------------------------------------------------------------------------
 # Chunk planning (src/matvis/_utils.py:124-319)
 # ---------------------------------------------------------------------------
 def get_required_chunks(freemem, nax, nfeed, nant, nsrc, nbeam, nbeampix, precision, source_buffer=1.0, memory_buffer=0.9):

@@ -61,7 +61,39 @@ def test_reference_arm_line(monkeypatch, capsys):
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
-    assert "768 sources" in line["config"]["sample"]
+    assert "768 sources" in line["sample"] and line["cpu_baseline"]["sample"] == line["sample"]
+
+
+def test_reference_arm_loads_no_repo_library(monkeypatch, capsys):
+    """The reference arm builds its workload and times the oracle without mapping
+    this repository's shared library (checked in a fresh interpreter)."""
+    import subprocess
+
+    code = ("import sys, bench\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', '--nside', '4', "
+            "'--nfreq', '1', '--ntimes', '1']\n"
+            "bench.main()\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libmatvis_b200' not in maps, 'library mapped'\n"
+            "assert 'matvis_b200._lib' not in sys.modules\n")
+    root = str(__import__("pathlib").Path(bench.__file__).resolve().parent)
+    res = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr[-2000:]
+    assert json.loads(res.stdout.strip().splitlines()[-1])["impl"] == "reference"
+
+
+def test_both_arms_share_the_config_object(monkeypatch):
+    """The config object names the workload only, so the two arms print the same one."""
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--nside", "8", "--nfreq", "2", "--ntimes", "2"])
+    args = bench.parse()
+    cfg, desc = bench.load_config(args, host_only=True)
+    terms, counts = bench.terms_per_job(cfg)
+    c1 = bench.workload_config(args, cfg, desc, terms, counts)
+    cfg2, desc2 = bench.load_config(args)
+    c2 = bench.workload_config(args, cfg2, desc2, *bench.terms_per_job(cfg2))
+    assert c1 == c2 and set(c1) == {"workload", "matprod", "gemm_mode", "terms_per_job", "above_horizon_per_time",
+                                    "l2"}
+    assert bench.accuracy_slices(cfg) == [(0, 0), (1, 1)]
 
 
 def test_reference_arm_other_ranks_do_nothing(monkeypatch, capsys):

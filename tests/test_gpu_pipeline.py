@@ -196,7 +196,7 @@ def test_simulate_vis_frequency_batches(device, caplog):
     max_memory = (size(2) + size(3)) / 2 / 0.9
     assert plan_job(spec, max_memory * 0.9) == (2, 1)
     whole = mv.simulate_vis(ants, **kw)
-    with caplog.at_level(logging.INFO, logger="matvis_b200.simulate"):
+    with caplog.at_level(logging.INFO, logger="matvis_b200.wrapper"):
         batched = mv.simulate_vis(ants, max_memory=max_memory, **kw)
     assert "in batches of 2" in caplog.text
     assert batched.shape == whole.shape == (5, 2, 24 * 24, 2, 2)

@@ -149,7 +149,7 @@ def test_simulate_vis_keywords():
     """Reference keywords are accepted; an unknown keyword is a TypeError, as in the reference."""
     import inspect
 
-    from matvis_b200.simulate import simulate_vis
+    from matvis_b200.wrapper import simulate_vis
 
     params = inspect.signature(simulate_vis).parameters
     for name in ("max_memory", "memory_buffer", "min_chunks", "source_buffer", "beam_spline_opts", "coord_method",
@@ -371,7 +371,7 @@ def test_bcrs_refresh_plan_follows_update_interval():
 
 
 def test_coord_method_keywords():
-    from matvis_b200.simulate import _check_coord_method
+    from matvis_b200.wrapper import _check_coord_method
 
     assert _check_coord_method("CoordinateRotationLST") == {}
     with pytest.raises(NotImplementedError):
@@ -487,7 +487,7 @@ def test_public_api_and_rotation_registry():
 def test_simulate_vis_buffer_validation(kwarg, value, errmsg):
     """The reference's wrapper validation (tests/test_wrapper.py:39-70), raised
     before any device work."""
-    from matvis_b200.simulate import simulate_vis
+    from matvis_b200.wrapper import simulate_vis
 
     kw = dict(ants={0: (0.0, 0.0, 0.0), 1: (14.6, 0.0, 0.0)}, fluxes=np.ones((15, 1)), ra=np.linspace(0, 1, 15),
               dec=np.full(15, -0.5), freqs=np.array([100e6]), times=np.zeros(5), beams=[], telescope_loc=-0.5)

@@ -215,3 +215,14 @@ def test_oracle_unpolarised_coherency_equals_scalar():
     a = orc.simulate_vis(fluxes=cfg["fluxes"], **kw)
     b = orc.simulate_vis(fluxes=orc.stokes_to_coherency(cfg["fluxes"], 0, 0, 0), **kw)
     np.testing.assert_allclose(b, a, rtol=0, atol=1e-12 * np.abs(a).max())
+
+
+@pytest.mark.parametrize("layout", ["hex37", "hex127_jitter", "hera350", "random40", "colocated", "line_half", "two",
+                                    "one"])
+@pytest.mark.parametrize("nd", [2, 0, -1])
+def test_oracle_redundancies_match_reference(layout, nd):
+    """The oracle's get_redundancies (the reference arm's pair list) against the
+    reference's own function (cli.py:273-290)."""
+    g = golden("redundancies")
+    got = orc.redundant_antpairs(g[f"{layout}_pos"], ndecimals=nd)
+    np.testing.assert_array_equal(got, g[f"{layout}_nd{nd}"].reshape(-1, 2))
