@@ -105,7 +105,10 @@ int mvb_horizon_compact(const double *topo, int64_t ld, int64_t c0, int64_t c1, 
  * 4,194,304 sources (c1 - c0), larger ones are rejected with MVB_ERR_ARG.  The
  * first call on a device looks up the array's device address (with that device
  * current) and caches it, so that first call should come before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU race,
+ * capture; a reset of the device's primary context (cudaDeviceReset)
+ * invalidates the cached address, so the entry point must not be called on a
+ * device after its context was reset.  All calls share the one array: calls
+ * that overlap on the GPU race,
  * so serialise them (one stream, or events).  Inputs, outputs and semantics are
  * those of mvb_horizon_compact; it calls no allocator. */
 int mvb_horizon_compact_static(const double *topo, int64_t ld, int64_t c0, int64_t c1, const double *flux,
@@ -218,20 +221,37 @@ int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t 
  * 2^-44 relative), rounds to FP64 and writes the visibilities in the
  * reference layout out[pair, p, q] = V[ant_i*F + q, ant_j*F + p]
  * (cpu/matprod.py:21-30): all nant^2 pairs (pairs = NULL, i slow) or the
- * npairs listed in pairs (int32 [npairs][2]).  out: complex64 (out_c128 = 0)
- * or complex128, each sum multiplied by vscale (1 / s^2 for MVB_GEMM_F16_3,
- * else 1); accumulate != 0 adds to out (the sum over source chunks).
- * ws, Mpad, Kcap, n_dev / n_host, kmul and k_chunk must be those of the
- * mvb_herk call that filled ws: the slice plan is recomputed from them.
+ * npairs listed in pairs (int32 [npairs][2], each entry in [0, nant); an entry
+ * outside that range reads nothing and its outputs are NaN).  out: complex64
+ * (out_c128 = 0) or complex128, each sum multiplied by vscale (1 / s^2 for
+ * MVB_GEMM_F16_3, else 1); accumulate != 0 adds to out (the sum over source
+ * chunks).  ws / ws_bytes, Mpad, Kcap, n_dev / n_host, kmul and k_chunk must be
+ * those of the mvb_herk call that filled ws: the slice plan is recomputed from
+ * them, and the same argument checks apply (ws_bytes at least
+ * mvb_herk_ws_bytes(Mpad, Kcap, k_chunk)).
  * Replaces MatProd.sum_chunks and the host transpose/gather of
  * GPUMatMul.sum_chunks (core/matprod.py:103-115, gpu/matprod.py:38-63). */
-int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
-                    int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs, void *out, int out_c128,
-                    double vscale, int accumulate, void *stream);
+int mvb_herk_reduce(const void *ws, size_t ws_bytes, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
+                    int64_t n_host, int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs,
+                    void *out, int out_c128, double vscale, int accumulate, void *stream);
+/* Wall-time limit, in nanoseconds, of each pipeline wait inside mvb_herk
+ * (process-wide; 0 restores the default of 4 s).  Returns the previous limit.
+ * A wait that runs out sets MVB_DEV_TIMEOUT in the status word; the kernel then
+ * stops issuing work, waits (at most 0.2 s) for the copies and tensor-core
+ * operations it issued, releases its tensor memory and returns, so the context
+ * stays usable.  For failure-detection tests and diagnostics: a limit shorter
+ * than a normal wait makes products fail.  No counterpart in the reference,
+ * whose device waits are unbounded (gpu/gpu.py:249). */
+uint64_t mvb_set_wait_limit_ns(uint64_t limit_ns);
+/* out[i] = sum_c vis[c * n + i] over nchunks per-chunk results (complex64 when
+ * c128 = 0, else complex128), accumulated in FP64 in chunk order.
+ * Replaces MatProd.sum_chunks (core/matprod.py:103-115). */
+int mvb_chunk_sum(const void *vis, int64_t nchunks, int64_t n, int c128, void *out, void *stream);
 
 /* ---- A8: per-pair source sums ----------------------------------------------- */
 size_t mvb_vecdot_ws_bytes(int64_t npairs, int nfeed, int64_t Kcap, int k_chunk);
 /* out[i, p, q] = sum_k Z[aj*F+p, k] conj(Z[ai*F+q, k]) for (ai, aj) = pairs[i]
+ * (each entry in [0, nant), the rows of Z being nant * nfeed)
  * over K_valid columns (as for mvb_herk), Z a plain complex64 panel (row pitch
  * Kcap), one warp per (k-slice, pair), FP64 slice sums in a fixed order.
  * Replaces GPUVectorDot.compute (one cuBLAS call per pair, gpu/matprod.py:66-98)

@@ -88,8 +88,11 @@ _SIGNATURES = {
     "mvb_herk": (c_int, [_p, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, _p, c_size_t, _p, _p]),
     "mvb_herk_reduce": (
         c_int,
-        [_p, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, c_int, _p, c_int64, _p, c_int, c_double, c_int, _p],
+        [_p, c_size_t, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, c_int, _p, c_int64, _p, c_int, c_double,
+         c_int, _p],
     ),
+    "mvb_set_wait_limit_ns": (ctypes.c_uint64, [ctypes.c_uint64]),
+    "mvb_chunk_sum": (c_int, [_p, c_int64, c_int64, c_int, _p, _p]),
     "mvb_vecdot_ws_bytes": (c_size_t, [c_int64, c_int, c_int64, c_int]),
     "mvb_vecdot": (
         c_int,

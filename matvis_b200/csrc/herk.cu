@@ -45,10 +45,12 @@
 // K_valid is cut into equal k-slices (multiples of 64 columns, at most k_chunk)
 // whose number is chosen on the device, from the device-side source count, to
 // fill whole waves of SMs (plan_splits).
-// Every mbarrier wait is bounded by wall time; on expiry the CTA records
-// MVB_DEV_TIMEOUT in the status word, stops issuing work, drains the copies and
-// MMAs it issued, frees TMEM and returns.
+// Every mbarrier wait is bounded by wall time (wait_ns, 4 s unless
+// mvb_set_wait_limit_ns changed it); on expiry the CTA records MVB_DEV_TIMEOUT
+// in the status word, stops issuing work, drains the copies and MMAs it issued
+// (each drain wait bounded by kDrainLimitNs), frees TMEM and returns.
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 
@@ -57,7 +59,7 @@ namespace mvb {
 constexpr int kEpiWarps = 16;
 constexpr int kPlanExtra = 31;  // extra k-slices the split planner may add to fill the SMs (one per lane)
 constexpr int kHerkThreads = 64 + 32 * kEpiWarps;
-constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s
+constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s: the default limit of a pipeline wait
 constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
 constexpr int kPlaneBytes = 128 * 64;              // one 128-row x 64-byte plane tile (two k-steps)
 constexpr int kSmemBudget = 192 * 1024;
@@ -158,7 +160,7 @@ template <int MODE, int KD>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const uint8_t *__restrict__ zpanel, int T, int n_tiles, const int32_t *__restrict__ n_dev,
                 int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, float *__restrict__ partials,
-                int32_t *__restrict__ status) {
+                int32_t *__restrict__ status, uint64_t wait_ns) {
   using C = HerkCfg<MODE>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[C::STAGES];
@@ -215,7 +217,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const bool diag = I == J;
       const uint32_t bytes = diag ? C::OPER_BYTES : 2 * C::OPER_BYTES;
       for (int kbi = 0; kbi < nkb; ++kbi) {
-        if (!mbar_wait(&empty_bar[st], ph ^ 1, kWaitLimitNs)) {
+        if (!mbar_wait(&empty_bar[st], ph ^ 1, wait_ns)) {
           atomicOr(status, MVB_DEV_TIMEOUT);
           abort_flag = 1;
           break;
@@ -251,14 +253,14 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       // k-block) two: the block and stage boundaries are independent
       for (int ks = 0; ks < nks; ++ks) {
         if (ks % KD == 0) {  // a fresh TMEM block
-          if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, kWaitLimitNs)) {
+          if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, wait_ns)) {
             ok = false;
             break;
           }
           tc_fence_after();
         }
         if ((ks & 1) == 0) {  // a new stage
-          if (!mbar_wait(&full_bar[st], ph, kWaitLimitNs)) {
+          if (!mbar_wait(&full_bar[st], ph, wait_ns)) {
             ok = false;
             break;
           }
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       bool ok = true;
       for (int g0 = 0; g0 < nks; g0 += KD) {
         // every lane waits; the vote keeps the warp converged for tcgen05.ld
-        ok = __all_sync(0xffffffffu, mbar_wait(&dfull_bar[buf], (dph >> buf) & 1u, kWaitLimitNs));
+        ok = __all_sync(0xffffffffu, mbar_wait(&dfull_bar[buf], (dph >> buf) & 1u, wait_ns));
         if (!ok) break;
         tc_fence_after();
         const uint32_t taddr = tbase + ((uint32_t)(quad * 32) << 16) + buf * 256 + quarter * 64;
@@ -469,10 +471,11 @@ __global__ void __launch_bounds__(256)
 }
 
 // Explicit pair list: one thread per (pair, p, q).
+// A pair naming an antenna outside [0, A) reads nothing and gets NaN.
 template <typename OT>
 __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, int n_tiles,
                                          const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap,
-                                         int k_chunk, int nsm, int F, const int32_t *__restrict__ pairs,
+                                         int k_chunk, int nsm, int A, int F, const int32_t *__restrict__ pairs,
                                          int64_t npairs,
                                          void *__restrict__ out, double vscale, int accumulate) {
   const int64_t total = npairs * F * F;
@@ -483,7 +486,12 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, 
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pr = e / (F * F);
     const int p = (int)((e / F) % F), q = (int)(e % F);
-    int m = pairs[2 * pr] * F + q, n = pairs[2 * pr + 1] * F + p;
+    const int ai = pairs[2 * pr], aj = pairs[2 * pr + 1];
+    if (ai < 0 || ai >= A || aj < 0 || aj >= A) {
+      store_out<OT>(out, e, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0);
+      continue;
+    }
+    int m = ai * F + q, n = aj * F + p;
     bool conj = false;
     if (m / 128 > n / 128) {
       const int tmp = m;
@@ -521,6 +529,10 @@ int set_smem_once(const void *fn, int bytes, int slot) {
   return MVB_OK;
 }
 
+// Wall-time limit of the product's pipeline waits, process-wide (see
+// mvb_set_wait_limit_ns); read at each launch.
+static std::atomic<uint64_t> g_wait_limit_ns{kWaitLimitNs};
+
 template <int MODE, int KD>
 static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
                        int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
@@ -537,13 +549,18 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
   herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), T, n_tiles, n_dev, n_host,
-                                                         kmul, Kcap, k_chunk, nsm, partials, status);
+                                                         kmul, Kcap, k_chunk, nsm, partials, status,
+                                                         g_wait_limit_ns.load(std::memory_order_relaxed));
   return check_launch("herk_kernel");
 }
 
 }  // namespace mvb
 
 using namespace mvb;
+
+extern "C" uint64_t mvb_set_wait_limit_ns(uint64_t limit_ns) {
+  return g_wait_limit_ns.exchange(limit_ns ? limit_ns : kWaitLimitNs);
+}
 
 extern "C" size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk) {
   if (Mpad <= 0 || Kcap <= 0 || k_chunk <= 0) return 0;
@@ -582,12 +599,18 @@ extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, con
 #undef MVB_HERK
 }
 
-extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
-                               int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs,
-                               void *out, int out_c128, double vscale, int accumulate, void *stream) {
-  if (!ws || !out || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || nant <= 0 || (nfeed != 1 && nfeed != 2) ||
-      k_chunk <= 0 || kmul <= 0 || (int64_t)nant * nfeed > Mpad || (pairs && npairs < 0))
+extern "C" int mvb_herk_reduce(const void *ws, size_t ws_bytes, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
+                               int64_t n_host, int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs,
+                               int64_t npairs, void *out, int out_c128, double vscale, int accumulate, void *stream) {
+  // the checks of mvb_herk: the slice plan recomputed here is then the product's
+  if (!ws || !out || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || Kcap % kKAlign || k_chunk <= 0 || k_chunk % kKAlign ||
+      n_host < 0 || kmul <= 0 || nant <= 0 || (nfeed != 1 && nfeed != 2) || (int64_t)nant * nfeed > Mpad ||
+      (pairs && npairs < 0))
     return fail(MVB_ERR_ARG, "mvb_herk_reduce: bad arguments");
+  if (!n_dev && n_host * kmul > Kcap) return fail(MVB_ERR_ARG, "mvb_herk_reduce: n * kmul exceeds Kcap");
+  if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk_reduce: panel too large");
+  if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk))
+    return fail(MVB_ERR_ARG, "mvb_herk_reduce: workspace smaller than the product's (mvb_herk_ws_bytes)");
   if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "mvb_herk_reduce: ws must be 16-byte aligned");
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
@@ -611,12 +634,45 @@ extern "C" int mvb_herk_reduce(const void *ws, int64_t Mpad, int64_t Kcap, const
     const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), (int64_t)num_sms() * 8);
     if (out_c128)
       herk_reduce_pairs_kernel<double2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
-                                                                         k_chunk, nsm, nfeed, pairs, npairs, out,
-                                                                         vscale, accumulate);
+                                                                         k_chunk, nsm, nant, nfeed, pairs, npairs,
+                                                                         out, vscale, accumulate);
     else
       herk_reduce_pairs_kernel<float2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
-                                                                        k_chunk, nsm, nfeed, pairs, npairs, out,
-                                                                        vscale, accumulate);
+                                                                        k_chunk, nsm, nant, nfeed, pairs, npairs,
+                                                                        out, vscale, accumulate);
   }
   return check_launch("herk_reduce");
+}
+
+// ---------------------------------------------------------------------------
+// Sum of per-chunk visibilities (MatProd.sum_chunks, core/matprod.py:103-115):
+// out[i] = sum_c vis[c][i] in chunk order, accumulated in FP64.
+// ---------------------------------------------------------------------------
+namespace mvb {
+template <typename T>
+__global__ void chunk_sum_kernel(const T *__restrict__ vis, int64_t nchunks, int64_t n, T *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const T v = vis[c * n + i];
+      re += (double)v.x;
+      im += (double)v.y;
+    }
+    out[i].x = re;
+    out[i].y = im;
+  }
+}
+}  // namespace mvb
+
+extern "C" int mvb_chunk_sum(const void *vis, int64_t nchunks, int64_t n, int c128, void *out, void *stream) {
+  if (nchunks < 1 || n < 0 || (n > 0 && (!vis || !out))) return fail(MVB_ERR_ARG, "mvb_chunk_sum: bad arguments");
+  if (n == 0) return MVB_OK;
+  const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)num_sms() * 8);
+  if (c128)
+    chunk_sum_kernel<double2><<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(static_cast<const double2 *>(vis),
+                                                                               nchunks, n, static_cast<double2 *>(out));
+  else
+    chunk_sum_kernel<float2><<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(static_cast<const float2 *>(vis),
+                                                                              nchunks, n, static_cast<float2 *>(out));
+  return check_launch("chunk_sum_kernel");
 }

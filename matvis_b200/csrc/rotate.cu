@@ -259,7 +259,10 @@ constexpr int kStaticCompactBlocks = 4096;  // chunks of up to 4096 x 1024 sourc
 static __device__ __align__(256) int32_t g_compact_counts[kStaticCompactBlocks];
 
 // Device address of g_compact_counts for the current device, looked up once
-// per device (with that device current) and cached.
+// per device (with that device current) and cached for the life of the
+// process.  A reset of the device's primary context (cudaDeviceReset) reloads
+// the module and invalidates the cached address: a process that resets a
+// device must not call mvb_horizon_compact_static on it afterwards.
 static int static_counts_ptr(int32_t **out) {
   static int32_t *cache[64] = {};
   static std::mutex mu;

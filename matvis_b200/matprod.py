@@ -66,6 +66,12 @@ def pair_product(nant: int, nfeed: int, npairs: int, gemm_mode="fp16x3") -> str:
     return "herk" if herk < vecdot else "vecdot"
 
 
+class AntpairsOutOfRange(IndexError, ValueError):
+    """A pair list names an antenna outside [0, nant).  An IndexError, as the
+    reference's gather ``vis[ant1_idx, ant2_idx]`` raises (cpu/matprod.py:29-30),
+    and a ValueError, as for the other argument checks."""
+
+
 def _pairs_tensor(antpairs, device):
     if antpairs is None:
         return None
@@ -77,7 +83,6 @@ class MatProd(ABC):
     """Abstract source-summing operation; core/matprod.py:11-115."""
 
     def __init__(self, nchunks: int, nfeed: int, nant: int, antpairs, precision=1, device=None):
-        self.device = _lib.require_cuda(device)
         if antpairs is None:
             self.all_pairs = True
             idx = np.arange(nant)
@@ -85,6 +90,12 @@ class MatProd(ABC):
         else:
             self.all_pairs = False
             self.antpairs = np.asarray(antpairs)
+            if self.antpairs.size and (self.antpairs.ndim != 2 or self.antpairs.shape[1] != 2):
+                raise ValueError("antpairs must have shape (npairs, 2)")
+            self.antpairs = self.antpairs.reshape(-1, 2)
+            if self.antpairs.size and (self.antpairs.min() < 0 or self.antpairs.max() >= nant):
+                raise AntpairsOutOfRange(f"antpairs name antennas outside [0, {nant})")
+        self.device = _lib.require_cuda(device)
         self.nchunks = nchunks
         self.nfeed = nfeed
         self.nant = nant
@@ -114,8 +125,13 @@ class MatProd(ABC):
         return self.vis[chunk]
 
     def sum_chunks(self, out):
-        """Sum the chunks into ``out`` (host array or device tensor)."""
-        tot = self.vis[0] if self.nchunks == 1 else self.vis.sum(dim=0)
+        """Sum the chunks into ``out`` (host array or device tensor), in chunk
+        order with FP64 accumulation (``mvb_chunk_sum``)."""
+        tot = self.vis[0]
+        if self.nchunks > 1:
+            tot = torch.empty_like(self.vis[0])
+            check(_lib.lib.mvb_chunk_sum(ptr(self.vis), self.nchunks, tot.numel(),
+                                         1 if tot.dtype == torch.complex128 else 0, ptr(tot), stream_handle()))
         if self.status is not None:
             _lib.check_status_word(self.status, type(self).__name__)
         if isinstance(out, torch.Tensor):
@@ -202,7 +218,8 @@ class B200MatMul(MatProd):
         pairs = None if self.all_pairs else self._pairs_dev
         check(
             _lib.lib.mvb_herk_reduce(
-                ptr(ws), panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc, self.nant, self.nfeed,
+                ptr(ws), ws.numel(), panel.Mpad, panel.Kcap, ptr(panel.n_dev), panel.n_host, kmul, kc, self.nant,
+                self.nfeed,
                 ptr(pairs), self.npairs, ptr(out), 1 if out.dtype == torch.complex128 else 0, 1.0 / panel.scale**2,
                 int(accumulate), sh,
             )

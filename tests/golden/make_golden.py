@@ -2,7 +2,11 @@
 
 Run from the repository root with the reference tree present::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference-root <path to the matvis project>
+
+(or set MATVIS_REFERENCE_ROOT).  ``NF_HERA_Dipole_small.fits`` beside the
+fixtures is the reference's own beam file (``src/matvis/data``), copied as is
+for the beamfits reader tests.
 
 It loads the reference modules through ``refload`` (inert stand-ins replace the
 absent astropy / pyuvdata / cupy) and records, for seeded inputs, what the
@@ -48,6 +52,8 @@ sys.path.insert(0, str(HERE))
 
 import refload  # noqa: E402
 
+if "--reference-root" in sys.argv:
+    refload.set_reference_root(sys.argv[sys.argv.index("--reference-root") + 1])
 ref = refload.load_reference()
 
 

@@ -21,14 +21,24 @@ fixture generator uses it, and only where the reference tree is present.
 from __future__ import annotations
 
 import importlib
+import os
 import sys
 import types
 from pathlib import Path
 
 import numpy as np
 
-REF_ROOT = Path("/root/reference")
+#: Root of the reference (matvis) project tree: the MATVIS_REFERENCE_ROOT
+#: environment variable, or ``make_golden.py --reference-root``.
+REF_ROOT = Path(os.environ.get("MATVIS_REFERENCE_ROOT", "reference"))
 REF_PKG = REF_ROOT / "src" / "matvis"
+
+
+def set_reference_root(path) -> None:
+    """Point the loader at the reference project tree (before ``load_reference``)."""
+    global REF_ROOT, REF_PKG
+    REF_ROOT = Path(path)
+    REF_PKG = REF_ROOT / "src" / "matvis"
 
 
 class _Placeholder:

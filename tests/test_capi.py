@@ -99,7 +99,7 @@ def _c_to_ctypes(decl: str):
         return "ptr"
     base = decl.replace("const", "").split()[0]
     return {"int": ctypes.c_int, "int64_t": ctypes.c_int64, "size_t": ctypes.c_size_t, "double": ctypes.c_double,
-            "float": ctypes.c_float, "int32_t": ctypes.c_int32}[base]
+            "float": ctypes.c_float, "int32_t": ctypes.c_int32, "uint64_t": ctypes.c_uint64}[base]
 
 
 def test_python_binding_matches_header_signatures():
@@ -124,15 +124,64 @@ def test_python_binding_matches_header_signatures():
         assert (res in (ctypes.c_void_p, ctypes.c_char_p)) if want_ret == "ptr" else res is want_ret, name
 
 
-def test_integration_binding_example_matches_library():
-    """The reference-side ctypes stub shown in INTEGRATION.md binds the same signatures."""
+def test_reference_side_binding_matches_library():
+    """The reference-side ctypes binding (include/matvis_gpu_b200.py, the module a
+    maintainer adds to matvis) declares the library's own signatures, and loads
+    the built library."""
+    import importlib.util
+
     from matvis_b200 import _lib
 
-    text = (ROOT / "INTEGRATION.md").read_text()
-    alias = {"_p": ctypes.c_void_p, "_i": ctypes.c_int, "_i64": ctypes.c_int64, "_sz": ctypes.c_size_t,
-             "_f": ctypes.c_float, "_d": ctypes.c_double}
-    stubs = re.findall(r"_lib\.(mvb_[a-z0-9_]+)\.argtypes = \[([^\]]*)\]", text)
-    assert len(stubs) >= 5
-    for name, args in stubs:
-        got = [alias[a.strip()] for a in args.split(",")]
-        assert got == list(_lib._SIGNATURES[name][1]), name
+    spec = importlib.util.spec_from_file_location("matvis_gpu_b200", ROOT / "include" / "matvis_gpu_b200.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    assert len(mod.SIGNATURES) >= 5
+    for name, (res, args) in mod.SIGNATURES.items():
+        assert (res, list(args)) == (_lib._SIGNATURES[name][0], list(_lib._SIGNATURES[name][1])), name
+    lib = mod.load(str(LIB))
+    assert lib.mvb_herk_ws_bytes(768, 4096, 2048) == _lib.lib.mvb_herk_ws_bytes(768, 4096, 2048)
+
+
+def test_herk_reduce_applies_the_products_checks_without_gpu():
+    """mvb_herk_reduce rejects, on the host, arguments the product would reject and
+    a workspace smaller than the product's (nothing is read from the pointers)."""
+    from matvis_b200 import _lib
+
+    ws_need = _lib.lib.mvb_herk_ws_bytes(768, 4096, 2048)
+    fake = ctypes.c_void_p(256)  # never dereferenced: every call below fails its checks first
+    args = dict(ws=fake, ws_bytes=ws_need, Mpad=768, Kcap=4096, n_dev=None, n_host=2048, kmul=2, k_chunk=2048,
+                nant=350, nfeed=2, pairs=None, npairs=0, out=fake, c128=0, vscale=1.0, acc=0, stream=None)
+    for bad in (dict(ws_bytes=ws_need - 1), dict(k_chunk=2000), dict(Kcap=4000), dict(n_host=2049),
+                dict(Mpad=700), dict(nfeed=3), dict(nant=385)):
+        a = {**args, **bad}
+        rc = _lib.lib.mvb_herk_reduce(*a.values())
+        assert rc == _lib.MVB_ERR_ARG, bad
+        assert _lib.lib.mvb_last_error().startswith(b"mvb_herk_reduce:")
+
+
+def test_set_wait_limit_round_trip_without_gpu():
+    from matvis_b200 import _lib
+
+    prev = _lib.lib.mvb_set_wait_limit_ns(123)
+    assert prev == 4_000_000_000
+    assert _lib.lib.mvb_set_wait_limit_ns(0) == 123
+    assert _lib.lib.mvb_set_wait_limit_ns(0) == prev
+
+
+def test_pair_lists_are_range_checked_on_the_host():
+    """A pair naming an antenna outside [0, nant) is refused before any device
+    work (the reference's gather raises IndexError, cpu/matprod.py:29-30)."""
+    import numpy as np
+
+    from matvis_b200.matprod import AntpairsOutOfRange, B200MatMul, B200VectorDot
+
+    for cls in (B200MatMul, B200VectorDot):
+        for bad in ([[0, 3]], [[-1, 0]], [[2, 7], [0, 1]]):
+            with pytest.raises(IndexError):
+                cls(1, 2, 3, np.array(bad))
+            with pytest.raises(ValueError):
+                cls(1, 2, 3, np.array(bad))
+    with pytest.raises(AntpairsOutOfRange):
+        B200MatMul(1, 1, 3, np.array([[0, 3]]))
+    with pytest.raises(ValueError, match="shape"):
+        B200MatMul(1, 1, 3, np.array([[0, 1, 2]]))

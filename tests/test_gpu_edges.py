@@ -77,3 +77,21 @@ def test_pairs_in_both_orders(device, matprod, kernel):
     # V_ji = V_ij^H, and the one-feed autocorrelations of (3, 3) are real
     np.testing.assert_allclose(vis[:, :, 1], np.conj(np.swapaxes(vis[:, :, 0], -1, -2)), rtol=0, atol=1e-6 * scale)
     assert np.all(vis[:, :, 2, 0, 0].imag == 0) and np.all(vis[:, :, 2, 1, 1].imag == 0)
+
+
+@pytest.mark.parametrize("polarized", [True, False])
+def test_nonfinite_beam_raises_the_reference_error(device, polarized):
+    """A NaN in a beam grid that the sources sample makes simulate_vis raise the
+    reference's ValueError (core/beams.py:202-206), from the kernel's status word."""
+    cfg = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=2000, nfreq=1, ntimes=1, nant=8, seed=5)
+    bad = cfg["beams"][0].data.copy()
+    bad[:, :, :30, :] = np.nan  # zenith angles 0..29 deg: every beam axis and feed
+    cfg["beams"] = [mv.GridBeam(data=bad, az=cfg["beams"][0].az, za=cfg["beams"][0].za)] + list(cfg["beams"][1:])
+    cfg["beam_idx"] = np.zeros(8, dtype=int)
+    cfg["polarized"] = polarized
+    with pytest.raises(ValueError, match="Beam interpolation resulted in an invalid value"):
+        _sim(cfg)
+    # the same job on the intact beam still runs on this device afterwards
+    cfg["beams"] = wl.subset(wl.config2(nfreq=2, ntimes=2), nsrc=2000, nfreq=1, ntimes=1, nant=8, seed=5)["beams"]
+    vis = _sim(cfg)
+    assert np.all(np.isfinite(vis))

@@ -78,3 +78,24 @@ def test_static_scratch_rejects_oversize_chunk(device):
                                              None, _lib.ptr(nout), 1, None, _lib.stream_handle())
     assert rc == _lib.MVB_ERR_ARG
     assert b"static limit" in _lib.lib.mvb_last_error()
+
+
+def test_static_scratch_at_its_limit(device):
+    """A chunk of exactly 4,194,304 sources (4,096 blocks: every slot of the static
+    array) selects the same sources as the workspace entry point."""
+    rng = np.random.default_rng(7)
+    n = 4096 * 1024
+    ra, dec = rng.uniform(0, 2 * np.pi, n), np.arcsin(rng.uniform(-1, 1, n))
+    eci = torch.as_tensor(np.ascontiguousarray(point_source_crd_eq(ra, dec)), device=device)
+    flux = torch.as_tensor(rng.uniform(0.1, 3.0, n), device=device)
+    topo = torch.empty((3, n), dtype=torch.float64, device=device)
+    R = np.ascontiguousarray(eci_to_enu_matrix(1.1, np.deg2rad(-30.72)))
+    _lib.check(_lib.lib.mvb_rotate(_lib.ptr(eci), n, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(topo),
+                                   _lib.stream_handle()))
+    ref = _select(topo, n, 0, n, flux, n, static=False)
+    got = _select(topo, n, 0, n, flux, n, static=True)
+    assert got[0] == ref[0] > n // 3
+    np.testing.assert_array_equal(got[1], ref[1])
+    np.testing.assert_array_equal(got[2], ref[2])
+    np.testing.assert_array_equal(got[3], ref[3])
+    assert got[4] == ref[4] == 0
