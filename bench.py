@@ -90,7 +90,7 @@ def parse():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--serve", action="store_true", help="served form: Poisson job stream, p50/p99 latency")
-    ap.add_argument("--serve-jobs", type=int, default=200)
+    ap.add_argument("--serve-jobs", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-nsrc-max", type=int, default=500_000)
     ap.add_argument("--serve-max-active", type=int, default=8)
@@ -675,23 +675,35 @@ def run_beamfits(args, local_rank):
 
 
 def run_serve(args, local_rank):
-    """Served form (config 5): Poisson arrivals into the continuous-batching server."""
+    """Served form (config 5): Poisson arrivals into the continuous-batching server.
+    The stream is generated lazily (each job's sky is built when it arrives) and
+    only latencies and term counts are kept, so host memory stays bounded."""
     import torch
 
+    from matvis_b200 import devcache
     from matvis_b200 import workloads as wl
     from matvis_b200.serve import VisServer, latency_summary
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    jobs = wl.config5_jobs(njobs=args.serve_jobs, rate_hz=args.serve_rate, nsrc_max=args.serve_nsrc_max)
-    for _, spec in jobs:
-        spec.gemm_mode = args.gemm_mode
-    warm = VisServer(device=dev, max_active=args.serve_max_active)
-    warm.serve_stream([(0.0, jobs[0][1])])  # kernel warm-up, not timed
+
+    def stream():
+        for t, spec in wl.config5_stream(njobs=args.serve_jobs, rate_hz=args.serve_rate,
+                                         nsrc_max=args.serve_nsrc_max):
+            spec.gemm_mode = args.gemm_mode
+            arrivals[0] = t
+            yield t, spec
+
+    arrivals = [0.0]
+    _, first = next(wl.config5_stream(njobs=1, rate_hz=args.serve_rate, nsrc_max=args.serve_nsrc_max))
+    first.gemm_mode = args.gemm_mode
+    warm = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False)
+    warm.serve_stream([(0.0, first)])  # kernel warm-up, not timed
     warm.close()
-    srv = VisServer(device=dev, max_active=args.serve_max_active)
+    srv = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False)
+    hits0, miss0 = devcache.CACHE.hits, devcache.CACHE.misses
     t0 = time.perf_counter()
-    srv.serve_stream(jobs)
+    srv.serve_stream(stream())
     wall = time.perf_counter() - t0
     srv.close()
     summ = latency_summary(srv.results)
@@ -699,7 +711,9 @@ def run_serve(args, local_rank):
         "metric": "served form: job latency p50/p99 and throughput", "impl": "b200", "unit": UNIT,
         "throughput": summ["terms"] / wall, "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
         "mean_queue_s": summ["mean_queue_s"], "jobs": summ["jobs"], "errors": summ["errors"], "wall_s": wall,
-        "arrival_span_s": jobs[-1][0], "max_concurrent": srv.max_concurrent, "peak_hbm_gb": srv.peak_in_use / 1e9,
+        "arrival_span_s": arrivals[0], "max_concurrent": srv.max_concurrent, "peak_hbm_gb": srv.peak_in_use / 1e9,
+        "launches_per_job": srv.launches / max(summ["jobs"] + summ.get("errors", 0), 1),
+        "device_cache": {"hits": devcache.CACHE.hits - hits0, "misses": devcache.CACHE.misses - miss0},
         "config": {"workload": f"config5 stream: {args.serve_jobs} jobs, Poisson {args.serve_rate}/s, Nant log-U[16,512], "
                                f"Nsrc log-U[1e3,{args.serve_nsrc_max}], Nf U{{1..32}}, Nt U{{1..16}}, Gaussian or "
                                f"polarised grid beam", "gemm_mode": args.gemm_mode,

@@ -174,6 +174,16 @@ int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64
               int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld, int nbeam,
               const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap,
               void *stream);
+/* mvb_tau_z for nfreq frequencies of one time step in one launch (the grouped
+ * chain of a batched job): frequency g = freqs[g] (a DEVICE array of nfreq
+ * doubles, Hz), its fluxes sflux + g * sflux_ld (floats) and its panel
+ * z + g * z_stride bytes (z_stride >= mvb_zpanel_bytes, a multiple of 16).
+ * Each panel equals what mvb_tau_z writes for that frequency.  Replaces the
+ * per-frequency TauCalculator / ZMatrixCalc calls of wrapper.py:180-199. */
+int mvb_tau_z_grouped(const double *antpos, int A, const double *freqs, int nfreq, const double *crd, int64_t ld,
+                      const int32_t *n_dev, int64_t nsrc, const float *sflux, int64_t sflux_ld, const int32_t *sidx,
+                      const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx, int F, int X, int mode,
+                      float zscale, void *z, size_t z_stride, int64_t Mpad, int64_t Kcap, void *stream);
 /* Z panel (or plain complex64 Z) from a caller exptau (A, e_ld), complex64
  * (e_c128 = 0) or complex128: Z[a*F+f, s*X+x] = exptau[a, s] * sflux[s] *
  * beam[bidx[a], f, x, s] for s < nsrc, zeros up to roundup(nsrc*X, 64)/X.
@@ -217,6 +227,17 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
  * (cpu/matprod.py:11-32); computes only the upper-triangle tiles. */
 int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
              int k_chunk, int drain_ksteps, void *ws, size_t ws_bytes, int32_t *status, void *stream);
+/* mvb_herk over ngroup panels of one shape in one launch: panel g at
+ * z + g * z_stride bytes (z_stride >= mvb_zpanel_bytes(mode, Mpad, Kcap), a
+ * multiple of 16), all with the same column count (n_dev / n_host, kmul).  The
+ * work units of all panels share the persistent CTAs, and the k-slice plan
+ * fills whole waves for ngroup x tiles units; ws holds ngroup x
+ * mvb_herk_ws_bytes(Mpad, Kcap, k_chunk) bytes.  Each panel's sums equal
+ * those of its own product under that plan.  Replaces the per-frequency
+ * GPUMatMul calls (gpu/gpu.py:197-254, wrapper.py:180-199). */
+int mvb_herk_grouped(const void *z, size_t z_stride, int ngroup, int mode, int64_t Mpad, int64_t Kcap,
+                     const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int drain_ksteps, void *ws,
+                     size_t ws_bytes, int32_t *status, void *stream);
 /* Sums the FP32 partial tiles over k-slices in float-float (TwoSum, about
  * 2^-44 relative), rounds to FP64 and writes the visibilities in the
  * reference layout out[pair, p, q] = V[ant_i*F + q, ant_j*F + p]
@@ -234,6 +255,13 @@ int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t 
 int mvb_herk_reduce(const void *ws, size_t ws_bytes, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
                     int64_t n_host, int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs, int64_t npairs,
                     void *out, int out_c128, double vscale, int accumulate, void *stream);
+/* mvb_herk_reduce for the ngroup panels of one mvb_herk_grouped call (same
+ * ws, ngroup and shape arguments): panel g's visibilities go to
+ * out + g * out_stride bytes. */
+int mvb_herk_reduce_grouped(const void *ws, size_t ws_bytes, int ngroup, int64_t Mpad, int64_t Kcap,
+                            const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int nant, int nfeed,
+                            const int32_t *pairs, int64_t npairs, void *out, size_t out_stride, int out_c128,
+                            double vscale, int accumulate, void *stream);
 /* Wall-time limit, in nanoseconds, of each pipeline wait inside mvb_herk
  * (process-wide; 0 restores the default of 4 s).  Returns the previous limit.
  * A wait that runs out sets MVB_DEV_TIMEOUT in the status word; the kernel then
@@ -292,6 +320,14 @@ int mvb_tau_z_pol(const double *antpos, int A, double freq, const double *crd, i
                   int64_t nsrc, const float *coh, const int32_t *sidx, const double *rot, const void *beam,
                   int64_t beam_ld, int nbeam, const int32_t *beam_idx, int mode, float zscale, void *z, int64_t Mpad,
                   int64_t Kcap, void *stream);
+/* mvb_tau_z_pol for nfreq frequencies in one launch, as mvb_tau_z_grouped:
+ * freqs a DEVICE array, frequency g's coherency rows at coh + g * coh_ld
+ * records of 4 floats, its panel at z + g * z_stride bytes. */
+int mvb_tau_z_pol_grouped(const double *antpos, int A, const double *freqs, int nfreq, const double *crd, int64_t ld,
+                          const int32_t *n_dev, int64_t nsrc, const float *coh, int64_t coh_ld, const int32_t *sidx,
+                          const double *rot, const void *beam, int64_t beam_ld, int nbeam, const int32_t *beam_idx,
+                          int mode, float zscale, void *z, size_t z_stride, int64_t Mpad, int64_t Kcap,
+                          void *stream);
 
 /* ---- Redundant-baseline pair selection (host memory, no device work) ------- */
 /* bls: (nant, nant, 2) float64 baselines, bls[i, j] = pos[j, :2] - pos[i, :2].

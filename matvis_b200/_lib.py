@@ -92,6 +92,23 @@ _SIGNATURES = {
          c_int, _p],
     ),
     "mvb_set_wait_limit_ns": (ctypes.c_uint64, [ctypes.c_uint64]),
+    "mvb_herk_grouped": (c_int, [_p, c_size_t, c_int, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, _p,
+                                 c_size_t, _p, _p]),
+    "mvb_herk_reduce_grouped": (
+        c_int,
+        [_p, c_size_t, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, c_int, _p, c_int64, _p, c_size_t,
+         c_int, c_double, c_int, _p],
+    ),
+    "mvb_tau_z_grouped": (
+        c_int,
+        [_p, c_int, _p, c_int, _p, c_int64, _p, c_int64, _p, c_int64, _p, _p, c_int64, c_int, _p, c_int, c_int, c_int,
+         c_float, _p, c_size_t, c_int64, c_int64, _p],
+    ),
+    "mvb_tau_z_pol_grouped": (
+        c_int,
+        [_p, c_int, _p, c_int, _p, c_int64, _p, c_int64, _p, c_int64, _p, _p, _p, c_int64, c_int, _p, c_int, c_float,
+         _p, c_size_t, c_int64, c_int64, _p],
+    ),
     "mvb_chunk_sum": (c_int, [_p, c_int64, c_int64, c_int, _p, _p]),
     "mvb_vecdot_ws_bytes": (c_size_t, [c_int64, c_int, c_int64, c_int]),
     "mvb_vecdot": (

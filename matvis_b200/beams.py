@@ -16,7 +16,7 @@ from abc import ABC, abstractmethod
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, devcache
 from ._lib import check, ptr, stream_handle
 from .beam_models import GaussianBeam, GridBeam  # noqa: F401  (re-exported)
 
@@ -171,9 +171,12 @@ class B200BeamInterpolator(BeamInterpolator):
                 grids = np.stack([b.power_grid() for b in self.beam_list]).astype(np.float32)
                 self.grid_kind = 1
             self.nza, self.naz = nza, naz
-            self.grids = torch.as_tensor(np.ascontiguousarray(grids), device=dev)
             params = np.array([[b.daz, b.dza, b.azmin] for b in self.beam_list], dtype=np.float64)
-            self.params = torch.as_tensor(params, device=dev)
+            grids = np.ascontiguousarray(grids)
+            # equal grids share one device copy across jobs (served form)
+            key = ("beam", devcache.device_key(dev), devcache.digest(grids, params))
+            self.grids, self.params = devcache.CACHE.get(
+                key, lambda: (torch.as_tensor(grids, device=dev), torch.as_tensor(params, device=dev)))
         else:
             if self.polarized:
                 raise ValueError("beam type must be efield if using polarized=True")

@@ -25,8 +25,10 @@
 // k-slice (k_chunk columns) of register sums is one partial tile; slices are
 // summed in float-float (TwoSum, ~2^-44) and rounded to FP64 by herk_reduce_*.
 //
-// Schedule.  Work unit u = (k-slice s, tile t), t fastest so the CTAs that run
-// together read the same Z columns (L2 reuse).  Persistent CTAs (one per SM,
+// Schedule.  Work unit u = (panel g, k-slice s, tile t), t fastest so the CTAs
+// that run together read the same Z columns (L2 reuse).  A launch covers ngroup
+// panels of one shape (the frequencies of a time step, zstride bytes apart)
+// that share the column count; with ngroup = 1 it is one product.  Persistent CTAs (one per SM,
 // 192 KB of shared memory) loop over units.  Warp roles (576 threads):
 //   warp 0 lane 0 : producer, one 1-D bulk copy per operand per stage: the
 //                   panel stores each (k-block, row block) as the stage's
@@ -158,9 +160,9 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
 // KD: k-steps accumulated in one TMEM block before it is drained (1, 2 or 4).
 template <int MODE, int KD>
 __global__ void __launch_bounds__(kHerkThreads, 1)
-    herk_kernel(const uint8_t *__restrict__ zpanel, int T, int n_tiles, const int32_t *__restrict__ n_dev,
-                int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, float *__restrict__ partials,
-                int32_t *__restrict__ status, uint64_t wait_ns) {
+    herk_kernel(const uint8_t *__restrict__ zpanels, int64_t zstride, int ngroup, int T, int n_tiles,
+                const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm,
+                float *__restrict__ partials, int32_t *__restrict__ status, uint64_t wait_ns) {
   using C = HerkCfg<MODE>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[C::STAGES];
@@ -175,8 +177,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
   int nsplit;
   int64_t kc;
-  plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
-  const int n_units = n_tiles * nsplit;
+  plan_splits(kvalid, n_tiles * ngroup, k_chunk, nsm, nsplit, kc);
+  const int per_panel = n_tiles * nsplit;
+  const int n_units = per_panel * ngroup;
   if ((int)blockIdx.x >= n_units) return;  // uniform over the CTA
 
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -208,7 +211,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     // ---------------- bulk-copy producer ----------------
     uint32_t st = 0, ph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      const int s = u / n_tiles, t = u % n_tiles;
+      const int g = u / per_panel, s = (u % per_panel) / n_tiles, t = u % n_tiles;
+      const uint8_t *zpanel = zpanels + (int64_t)g * zstride;
       int I, J;
       decode_tile(t, T, I, J);
       const int64_t k0 = (int64_t)s * kc;
@@ -241,7 +245,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     // ---------------- UMMA issuer: one fresh TMEM block per KD k-steps ----------------
     uint32_t st = 0, ph = 0, buf = 0, dph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      const int s = u / n_tiles, t = u % n_tiles;
+      const int s = (u % per_panel) / n_tiles, t = u % n_tiles;
       int I, J;
       decode_tile(t, T, I, J);
       const int64_t k0 = (int64_t)s * kc;
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 #pragma unroll
     for (int j = 0; j < 64; ++j) acc[j] = 0.f;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      const int s = u / n_tiles;
+      const int s = (u % per_panel) / n_tiles;
       const int64_t k0 = (int64_t)s * kc;
       const int64_t klen = min(kc, kvalid - k0);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
@@ -410,19 +414,23 @@ struct FF {
 // One CTA (8 warps) per 8 columns of an upper tile: warp w sums column c0 + w,
 // lane l rows 4l .. 4l + 3 (a 16-byte load per component per k-slice; a warp
 // reads the column's two contiguous 512-byte runs).  F is a template parameter
-// (no runtime integer division in the index arithmetic).
+// (no runtime integer division in the index arithmetic).  blockIdx.y is the
+// panel of a grouped product; its output is out_stride bytes further.
 template <typename OT, int F>
 __global__ void __launch_bounds__(256)
-    herk_reduce_all_kernel(const float *__restrict__ part, int T, int n_tiles, const int32_t *__restrict__ n_dev,
-                           int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm, int A,
-                           void *__restrict__ out, double vscale, int accumulate) {
+    herk_reduce_all_kernel(const float *__restrict__ part, int ngroup, int T, int n_tiles,
+                           const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap, int k_chunk,
+                           int nsm, int A, void *__restrict__ out_base, int64_t out_stride, double vscale,
+                           int accumulate) {
   const int t = blockIdx.x / kRedGroups, g = blockIdx.x % kRedGroups;
   int I, J;
   decode_tile(t, T, I, J);
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
   int nsplit;
   int64_t kc;
-  plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
+  plan_splits(kvalid, n_tiles * ngroup, k_chunk, nsm, nsplit, kc);
+  void *out = static_cast<uint8_t *>(out_base) + (int64_t)blockIdx.y * out_stride;
+  part += (size_t)blockIdx.y * nsplit * n_tiles * (256 * 128);
   const int M = A * F;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int c = g * 8 + w;
@@ -472,17 +480,20 @@ __global__ void __launch_bounds__(256)
 
 // Explicit pair list: one thread per (pair, p, q).
 // A pair naming an antenna outside [0, A) reads nothing and gets NaN.
+// blockIdx.y is the panel of a grouped product.
 template <typename OT>
-__global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int T, int n_tiles,
+__global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int ngroup, int T, int n_tiles,
                                          const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap,
                                          int k_chunk, int nsm, int A, int F, const int32_t *__restrict__ pairs,
-                                         int64_t npairs,
-                                         void *__restrict__ out, double vscale, int accumulate) {
+                                         int64_t npairs, void *__restrict__ out_base, int64_t out_stride,
+                                         double vscale, int accumulate) {
   const int64_t total = npairs * F * F;
   const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
   int nsplit;
   int64_t kc;
-  plan_splits(kvalid, n_tiles, k_chunk, nsm, nsplit, kc);
+  plan_splits(kvalid, n_tiles * ngroup, k_chunk, nsm, nsplit, kc);
+  void *out = static_cast<uint8_t *>(out_base) + (int64_t)blockIdx.y * out_stride;
+  part += (size_t)blockIdx.y * nsplit * n_tiles * (256 * 128);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pr = e / (F * F);
     const int p = (int)((e / F) % F), q = (int)(e % F);
@@ -534,13 +545,13 @@ int set_smem_once(const void *fn, int bytes, int slot) {
 static std::atomic<uint64_t> g_wait_limit_ns{kWaitLimitNs};
 
 template <int MODE, int KD>
-static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul,
-                       int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
+static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
+                       int64_t n_host, int kmul, int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
   using C = HerkCfg<MODE>;
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
   const int nsm = num_sms();
-  const int64_t max_units = (int64_t)n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
+  const int64_t max_units = (int64_t)ngroup * n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
   const int grid = (int)std::min<int64_t>(max_units, nsm);
   const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
   // slots 16 + 3 * MODE + {0, 1, 2} for KD = {1, 2, 4}
@@ -548,10 +559,104 @@ static int launch_herk(const void *z, int64_t Mpad, int64_t Kcap, const int32_t 
                          16 + 3 * MODE + (KD == 4 ? 2 : KD - 1));
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
-  herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), T, n_tiles, n_dev, n_host,
-                                                         kmul, Kcap, k_chunk, nsm, partials, status,
+  herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T, n_tiles,
+                                                         n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials, status,
                                                          g_wait_limit_ns.load(std::memory_order_relaxed));
   return check_launch("herk_kernel");
+}
+
+// Argument checks shared by the product and its reductions (the slice plan
+// the reductions recompute is the product's only if these hold).
+static int check_herk_shape(const char *who, int ngroup, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
+                            int64_t n_host, int kmul, int k_chunk) {
+  if (ngroup <= 0 || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || Kcap % kKAlign || k_chunk <= 0 || k_chunk % kKAlign ||
+      n_host < 0 || kmul <= 0)
+    return fail(MVB_ERR_ARG, "%s: bad arguments", who);
+  if (!n_dev && n_host * kmul > Kcap) return fail(MVB_ERR_ARG, "%s: n * kmul exceeds Kcap", who);
+  if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "%s: panel too large", who);
+  const int64_t T = Mpad / 128;
+  if ((int64_t)ngroup * (T * (T + 1) / 2) * (ceil_div(Kcap, k_chunk) + kPlanExtra) > INT32_MAX)
+    return fail(MVB_ERR_ARG, "%s: too many work units", who);
+  return MVB_OK;
+}
+
+static int herk_impl(const char *who, const void *z, int64_t zstride, int ngroup, int mode, int64_t Mpad, int64_t Kcap,
+                     const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int drain_ksteps, void *ws,
+                     size_t ws_bytes, int32_t *status, void *stream) {
+  if (!z || !ws || !status) return fail(MVB_ERR_ARG, "%s: bad arguments", who);
+  int rc = check_herk_shape(who, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk);
+  if (rc) return rc;
+  if (reinterpret_cast<uintptr_t>(z) % 16 || zstride % 16) return fail(MVB_ERR_ARG, "%s: panel not 16-byte aligned", who);
+  if (ngroup > 1 && (size_t)zstride < mvb_zpanel_bytes(mode, Mpad, Kcap))
+    return fail(MVB_ERR_ARG, "%s: panels overlap (stride below mvb_zpanel_bytes)", who);
+  if (ws_bytes / (size_t)ngroup < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk))
+    return fail(MVB_ERR_ARG, "%s: workspace too small", who);
+  if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "%s: ws must be 16-byte aligned", who);
+  if (drain_ksteps < 0 || drain_ksteps > 4 || drain_ksteps == 3)
+    return fail(MVB_ERR_ARG, "%s: drain_ksteps must be 0, 1, 2 or 4", who);
+  // default: 6-product mode drains every k-step, 3-product modes every 2
+  const int kd = drain_ksteps ? drain_ksteps : (mode == MVB_GEMM_BF16_6 ? 1 : 2);
+  cudaStream_t s = as_stream(stream);
+  float *part = static_cast<float *>(ws);
+#define MVB_HERK(M)                                                                                                \
+  return kd == 1   ? launch_herk<M, 1>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
+         : kd == 2 ? launch_herk<M, 2>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
+                   : launch_herk<M, 4>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s)
+  switch (mode) {
+    case MVB_GEMM_BF16_3: MVB_HERK(MVB_GEMM_BF16_3);
+    case MVB_GEMM_BF16_6: MVB_HERK(MVB_GEMM_BF16_6);
+    case MVB_GEMM_TF32_3: MVB_HERK(MVB_GEMM_TF32_3);
+    case MVB_GEMM_F16_3: MVB_HERK(MVB_GEMM_F16_3);
+    default: return fail(MVB_ERR_ARG, "%s: unknown mode %d", who, mode);
+  }
+#undef MVB_HERK
+}
+
+static int reduce_impl(const char *who, const void *ws, size_t ws_bytes, int ngroup, int64_t Mpad, int64_t Kcap,
+                       const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int nant, int nfeed,
+                       const int32_t *pairs, int64_t npairs, void *out, int64_t out_stride, int out_c128,
+                       double vscale, int accumulate, void *stream) {
+  // the checks of mvb_herk: the slice plan recomputed here is then the product's
+  if (!ws || !out || nant <= 0 || (nfeed != 1 && nfeed != 2) || (int64_t)nant * nfeed > Mpad || (pairs && npairs < 0))
+    return fail(MVB_ERR_ARG, "%s: bad arguments", who);
+  int rc = check_herk_shape(who, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk);
+  if (rc) return rc;
+  if (ws_bytes / (size_t)ngroup < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk))
+    return fail(MVB_ERR_ARG, "%s: workspace smaller than the product's (mvb_herk_ws_bytes)", who);
+  if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "%s: ws must be 16-byte aligned", who);
+  const int64_t per_out = (pairs ? npairs : (int64_t)nant * nant) * nfeed * nfeed * (out_c128 ? 16 : 8);
+  if (ngroup > 1 && out_stride < per_out) return fail(MVB_ERR_ARG, "%s: outputs overlap (out_stride too small)", who);
+  if (ngroup > 65535) return fail(MVB_ERR_ARG, "%s: at most 65535 panels per launch", who);
+  const int T = (int)(Mpad / 128);
+  const int n_tiles = T * (T + 1) / 2;
+  const int nsm = num_sms();
+  const float *part = static_cast<const float *>(ws);
+  cudaStream_t s = as_stream(stream);
+  if (!pairs) {
+    const dim3 grid((unsigned)(n_tiles * kRedGroups), (unsigned)ngroup);
+#define MVB_RED(OT, FF_)                                                                                    \
+  herk_reduce_all_kernel<OT, FF_><<<grid, 256, 0, s>>>(part, ngroup, T, n_tiles, n_dev, n_host, kmul, Kcap, \
+                                                       k_chunk, nsm, nant, out, out_stride, vscale, accumulate)
+    if (out_c128) {
+      if (nfeed == 2) MVB_RED(double2, 2); else MVB_RED(double2, 1);
+    } else {
+      if (nfeed == 2) MVB_RED(float2, 2); else MVB_RED(float2, 1);
+    }
+#undef MVB_RED
+  } else {
+    if (npairs == 0) return MVB_OK;
+    const int64_t total = npairs * nfeed * nfeed;
+    const dim3 grid((unsigned)std::min<int64_t>(ceil_div(total, 256), (int64_t)nsm * 8), (unsigned)ngroup);
+    if (out_c128)
+      herk_reduce_pairs_kernel<double2><<<grid, 256, 0, s>>>(part, ngroup, T, n_tiles, n_dev, n_host, kmul, Kcap,
+                                                             k_chunk, nsm, nant, nfeed, pairs, npairs, out, out_stride,
+                                                             vscale, accumulate);
+    else
+      herk_reduce_pairs_kernel<float2><<<grid, 256, 0, s>>>(part, ngroup, T, n_tiles, n_dev, n_host, kmul, Kcap,
+                                                            k_chunk, nsm, nant, nfeed, pairs, npairs, out, out_stride,
+                                                            vscale, accumulate);
+  }
+  return check_launch(who);
 }
 
 }  // namespace mvb
@@ -571,77 +676,32 @@ extern "C" size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk) {
 extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,
                         int kmul, int k_chunk, int drain_ksteps, void *ws, size_t ws_bytes, int32_t *status,
                         void *stream) {
-  if (!z || !ws || !status || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || Kcap % kKAlign || k_chunk <= 0 ||
-      k_chunk % kKAlign || n_host < 0 || kmul <= 0)
-    return fail(MVB_ERR_ARG, "mvb_herk: bad arguments");
-  if (!n_dev && n_host * kmul > Kcap) return fail(MVB_ERR_ARG, "mvb_herk: n * kmul exceeds Kcap");
-  if (reinterpret_cast<uintptr_t>(z) % 16) return fail(MVB_ERR_ARG, "mvb_herk: panel not 16-byte aligned");
-  if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk)) return fail(MVB_ERR_ARG, "mvb_herk: workspace too small");
-  if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "mvb_herk: ws must be 16-byte aligned");
-  if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk: panel too large");
-  if (drain_ksteps < 0 || drain_ksteps > 4 || drain_ksteps == 3)
-    return fail(MVB_ERR_ARG, "mvb_herk: drain_ksteps must be 0, 1, 2 or 4");
-  // default: 6-product mode drains every k-step, 3-product modes every 2
-  const int kd = drain_ksteps ? drain_ksteps : (mode == MVB_GEMM_BF16_6 ? 1 : 2);
-  cudaStream_t s = as_stream(stream);
-  float *part = static_cast<float *>(ws);
-#define MVB_HERK(M)                                                                           \
-  return kd == 1   ? launch_herk<M, 1>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
-         : kd == 2 ? launch_herk<M, 2>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
-                   : launch_herk<M, 4>(z, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s)
-  switch (mode) {
-    case MVB_GEMM_BF16_3: MVB_HERK(MVB_GEMM_BF16_3);
-    case MVB_GEMM_BF16_6: MVB_HERK(MVB_GEMM_BF16_6);
-    case MVB_GEMM_TF32_3: MVB_HERK(MVB_GEMM_TF32_3);
-    case MVB_GEMM_F16_3: MVB_HERK(MVB_GEMM_F16_3);
-    default: return fail(MVB_ERR_ARG, "mvb_herk: unknown mode %d", mode);
-  }
-#undef MVB_HERK
+  return herk_impl("mvb_herk", z, 0, 1, mode, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, drain_ksteps, ws, ws_bytes,
+                   status, stream);
+}
+
+extern "C" int mvb_herk_grouped(const void *z, size_t z_stride, int ngroup, int mode, int64_t Mpad, int64_t Kcap,
+                                const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int drain_ksteps,
+                                void *ws, size_t ws_bytes, int32_t *status, void *stream) {
+  if (z_stride > (size_t)INT64_MAX) return fail(MVB_ERR_ARG, "mvb_herk_grouped: bad arguments");
+  return herk_impl("mvb_herk_grouped", z, (int64_t)z_stride, ngroup, mode, Mpad, Kcap, n_dev, n_host, kmul, k_chunk,
+                   drain_ksteps, ws, ws_bytes, status, stream);
 }
 
 extern "C" int mvb_herk_reduce(const void *ws, size_t ws_bytes, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
                                int64_t n_host, int kmul, int k_chunk, int nant, int nfeed, const int32_t *pairs,
                                int64_t npairs, void *out, int out_c128, double vscale, int accumulate, void *stream) {
-  // the checks of mvb_herk: the slice plan recomputed here is then the product's
-  if (!ws || !out || Mpad <= 0 || Mpad % 128 || Kcap <= 0 || Kcap % kKAlign || k_chunk <= 0 || k_chunk % kKAlign ||
-      n_host < 0 || kmul <= 0 || nant <= 0 || (nfeed != 1 && nfeed != 2) || (int64_t)nant * nfeed > Mpad ||
-      (pairs && npairs < 0))
-    return fail(MVB_ERR_ARG, "mvb_herk_reduce: bad arguments");
-  if (!n_dev && n_host * kmul > Kcap) return fail(MVB_ERR_ARG, "mvb_herk_reduce: n * kmul exceeds Kcap");
-  if (Kcap > INT32_MAX || Mpad > 65536) return fail(MVB_ERR_ARG, "mvb_herk_reduce: panel too large");
-  if (ws_bytes < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk))
-    return fail(MVB_ERR_ARG, "mvb_herk_reduce: workspace smaller than the product's (mvb_herk_ws_bytes)");
-  if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "mvb_herk_reduce: ws must be 16-byte aligned");
-  const int T = (int)(Mpad / 128);
-  const int n_tiles = T * (T + 1) / 2;
-  const int nsm = num_sms();
-  const float *part = static_cast<const float *>(ws);
-  cudaStream_t s = as_stream(stream);
-  if (!pairs) {
-    const int grid = n_tiles * kRedGroups;
-#define MVB_RED(OT, FF_)                                                                                          \
-  herk_reduce_all_kernel<OT, FF_><<<grid, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm, \
-                                                       nant, out, vscale, accumulate)
-    if (out_c128) {
-      if (nfeed == 2) MVB_RED(double2, 2); else MVB_RED(double2, 1);
-    } else {
-      if (nfeed == 2) MVB_RED(float2, 2); else MVB_RED(float2, 1);
-    }
-#undef MVB_RED
-  } else {
-    if (npairs == 0) return MVB_OK;
-    const int64_t total = npairs * nfeed * nfeed;
-    const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), (int64_t)num_sms() * 8);
-    if (out_c128)
-      herk_reduce_pairs_kernel<double2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
-                                                                         k_chunk, nsm, nant, nfeed, pairs, npairs,
-                                                                         out, vscale, accumulate);
-    else
-      herk_reduce_pairs_kernel<float2><<<(unsigned)blocks, 256, 0, s>>>(part, T, n_tiles, n_dev, n_host, kmul, Kcap,
-                                                                        k_chunk, nsm, nant, nfeed, pairs, npairs,
-                                                                        out, vscale, accumulate);
-  }
-  return check_launch("herk_reduce");
+  return reduce_impl("mvb_herk_reduce", ws, ws_bytes, 1, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, nant, nfeed, pairs,
+                     npairs, out, 0, out_c128, vscale, accumulate, stream);
+}
+
+extern "C" int mvb_herk_reduce_grouped(const void *ws, size_t ws_bytes, int ngroup, int64_t Mpad, int64_t Kcap,
+                                       const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int nant,
+                                       int nfeed, const int32_t *pairs, int64_t npairs, void *out, size_t out_stride,
+                                       int out_c128, double vscale, int accumulate, void *stream) {
+  if (out_stride > (size_t)INT64_MAX) return fail(MVB_ERR_ARG, "mvb_herk_reduce_grouped: bad arguments");
+  return reduce_impl("mvb_herk_reduce_grouped", ws, ws_bytes, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, nant,
+                     nfeed, pairs, npairs, out, (int64_t)out_stride, out_c128, vscale, accumulate, stream);
 }
 
 // ---------------------------------------------------------------------------

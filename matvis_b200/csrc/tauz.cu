@@ -202,7 +202,9 @@ constexpr int kTauZBlockSrc = kTauZGroups * kTauZSrc;
 constexpr int kTauZRow = kTauZBlockSrc + 1;  // staged beam values per q, padded
 constexpr int kTauZMaxBFX = 16;              // beam planes staged in shared memory, else read through L1
 
-// grid.x: blocks of kTauZBlockSrc sources, grid.y: blocks of kTauZAnts antennas.
+// grid.x: blocks of kTauZBlockSrc sources, grid.y: blocks of kTauZAnts antennas,
+// grid.z: the frequencies of a grouped launch (freqs != nullptr): frequency
+// freqs[z], fluxes sflux + z sflux_ld (coh + z coh_ld), panel z + z zstride bytes.
 // EXT = 0: phase from antpos . crd (fused tau); EXT = 1 / 2: phase factor read
 // from a caller exptau (A, e_ld) in complex64 / complex128, multiplied by sflux.
 // POL (EXT = 0, X = 2): polarised sky.  Instead of sqrt(0.5 I) the source
@@ -218,8 +220,17 @@ __global__ void __launch_bounds__(kTauZThreads)
                  const int32_t *__restrict__ sidx, const float2 *__restrict__ beam, int64_t beam_ld, int nbeam,
                  const int32_t *__restrict__ beam_idx, int F, float zscale, void *__restrict__ z, int64_t Mpad,
                  int64_t Kcap, const void *__restrict__ ext = nullptr, int64_t e_ld = 0,
-                 const float4 *__restrict__ coh = nullptr, const double2 *__restrict__ rot = nullptr) {
+                 const float4 *__restrict__ coh = nullptr, const double2 *__restrict__ rot = nullptr,
+                 const double *__restrict__ freqs = nullptr, int64_t sflux_ld = 0, int64_t coh_ld = 0,
+                 int64_t zstride = 0) {
   static_assert(!POL || (X == 2 && EXT == 0), "the polarised sky needs two beam axes and the fused phase");
+  if (freqs) {  // grouped: this block's frequency
+    const int gz = blockIdx.z;
+    f_over_c = freqs[gz] * kInvC;
+    if (sflux) sflux += gz * sflux_ld;
+    if (coh) coh += gz * coh_ld;
+    z = static_cast<uint8_t *>(z) + gz * zstride;
+  }
   const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
   const int64_t s_end = round_up(n * X, kKAlign) / X;  // zero-fill up to here
   const int64_t s0 = (int64_t)blockIdx.x * kTauZBlockSrc + (threadIdx.x % kTauZGroups) * kTauZSrc;
@@ -472,32 +483,40 @@ extern "C" int mvb_exptau(const double *antpos, int A, double freq, const double
   return check_launch("exptau_kernel");
 }
 
-extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
-                         int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld,
-                         int nbeam, const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z,
-                         int64_t Mpad, int64_t Kcap, void *stream) {
+// Fused phase + Z writer for nfreq frequencies: freqs_dev == nullptr means one
+// frequency, freq; otherwise freqs_dev[0 .. nfreq) on the device, with the
+// fluxes sflux_ld floats and the panels z_stride bytes apart.
+static int tau_z_impl(const char *who, const double *antpos, int A, double freq, const double *freqs_dev, int nfreq,
+                      const double *crd, int64_t ld, const int32_t *n_dev, int64_t nsrc, const float *sflux,
+                      int64_t sflux_ld, const int32_t *sidx, const void *beam, int64_t beam_ld, int nbeam,
+                      const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z, int64_t z_stride,
+                      int64_t Mpad, int64_t Kcap, void *stream) {
   if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !sflux || (nsrc > 0 && !crd) || (F != 1 && F != 2) ||
-      (X != 1 && X != 2) || nbeam <= 0 || beam_ld < nsrc)
-    return fail(MVB_ERR_ARG, "mvb_tau_z: bad arguments");
-  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z");
+      (X != 1 && X != 2) || nbeam <= 0 || beam_ld < nsrc || nfreq <= 0 || nfreq > 65535)
+    return fail(MVB_ERR_ARG, "%s: bad arguments", who);
+  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, who);
   if (rc) return rc;
-  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z: Kcap too small for nsrc * nax");
+  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "%s: Kcap too small for nsrc * nax", who);
+  if (nfreq > 1 && (sflux_ld < nsrc || z_stride < (int64_t)mvb_zpanel_bytes(mode, Mpad, Kcap) || z_stride % 16))
+    return fail(MVB_ERR_ARG, "%s: flux rows or panels overlap", who);
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
-  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts), (unsigned)nfreq);
   const bool staged = nbeam * F * X <= kTauZMaxBFX;
   const size_t smem = staged ? (size_t)nbeam * F * X * kTauZRow * sizeof(float2) : 0;
   const double foc = freq * kInvC;
   const float2 *bm = static_cast<const float2 *>(beam);
   cudaStream_t s = as_stream(stream);
-#define MVB_TAUZ(M, XX)                                                                                    \
-  do {                                                                                                       \
-    if (staged)                                                                                              \
-      tau_z_kernel<M, XX, 0, true, false><<<grid, kTauZThreads, smem, s>>>(                                  \
-          antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
-    else                                                                                                     \
-      tau_z_kernel<M, XX, 0, false, false><<<grid, kTauZThreads, 0, s>>>(                                    \
-          antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap); \
+#define MVB_TAUZ(M, XX)                                                                                       \
+  do {                                                                                                        \
+    if (staged)                                                                                               \
+      tau_z_kernel<M, XX, 0, true, false><<<grid, kTauZThreads, smem, s>>>(                                   \
+          antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, \
+          Kcap, nullptr, 0, nullptr, nullptr, freqs_dev, sflux_ld, 0, z_stride);                              \
+    else                                                                                                      \
+      tau_z_kernel<M, XX, 0, false, false><<<grid, kTauZThreads, 0, s>>>(                                     \
+          antpos, A, foc, crd, ld, n_dev, nsrc, sflux, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, \
+          Kcap, nullptr, 0, nullptr, nullptr, freqs_dev, sflux_ld, 0, z_stride);                              \
   } while (0)
 #define MVB_TAUZ2(M) \
   if (X == 2)        \
@@ -514,6 +533,24 @@ extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double 
 #undef MVB_TAUZ2
 #undef MVB_TAUZ
   return check_launch("tau_z_kernel");
+}
+
+extern "C" int mvb_tau_z(const double *antpos, int A, double freq, const double *crd, int64_t ld, const int32_t *n_dev,
+                         int64_t nsrc, const float *sflux, const int32_t *sidx, const void *beam, int64_t beam_ld,
+                         int nbeam, const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z,
+                         int64_t Mpad, int64_t Kcap, void *stream) {
+  return tau_z_impl("mvb_tau_z", antpos, A, freq, nullptr, 1, crd, ld, n_dev, nsrc, sflux, 0, sidx, beam, beam_ld,
+                    nbeam, beam_idx, F, X, mode, zscale, z, 0, Mpad, Kcap, stream);
+}
+
+extern "C" int mvb_tau_z_grouped(const double *antpos, int A, const double *freqs, int nfreq, const double *crd,
+                                 int64_t ld, const int32_t *n_dev, int64_t nsrc, const float *sflux, int64_t sflux_ld,
+                                 const int32_t *sidx, const void *beam, int64_t beam_ld, int nbeam,
+                                 const int32_t *beam_idx, int F, int X, int mode, float zscale, void *z,
+                                 size_t z_stride, int64_t Mpad, int64_t Kcap, void *stream) {
+  if (!freqs || z_stride > (size_t)INT64_MAX) return fail(MVB_ERR_ARG, "mvb_tau_z_grouped: bad arguments");
+  return tau_z_impl("mvb_tau_z_grouped", antpos, A, 0.0, freqs, nfreq, crd, ld, n_dev, nsrc, sflux, sflux_ld, sidx,
+                    beam, beam_ld, nbeam, beam_idx, F, X, mode, zscale, z, (int64_t)z_stride, Mpad, Kcap, stream);
 }
 
 extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, int64_t ldz, int mode, float zscale,
@@ -547,23 +584,25 @@ extern "C" int mvb_z_pack(const void *zsrc, int z_c128, int64_t M, int64_t K, in
   return check_launch("z_pack_kernel");
 }
 
-extern "C" int mvb_tau_z_pol(const double *antpos, int A, double freq, const double *crd, int64_t ld,
-                             const int32_t *n_dev, int64_t nsrc, const float *coh, const int32_t *sidx,
-                             const double *rot, const void *beam, int64_t beam_ld, int nbeam,
-                             const int32_t *beam_idx, int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap,
-                             void *stream) {
+static int tau_z_pol_impl(const char *who, const double *antpos, int A, double freq, const double *freqs_dev,
+                          int nfreq, const double *crd, int64_t ld, const int32_t *n_dev, int64_t nsrc,
+                          const float *coh, int64_t coh_ld, const int32_t *sidx, const double *rot, const void *beam,
+                          int64_t beam_ld, int nbeam, const int32_t *beam_idx, int mode, float zscale, void *z,
+                          int64_t z_stride, int64_t Mpad, int64_t Kcap, void *stream) {
   const int F = 2, X = 2;
   if (A <= 0 || nsrc < 0 || !antpos || !z || !beam || !coh || !rot || (nsrc > 0 && !crd) || nbeam <= 0 ||
-      beam_ld < nsrc)
-    return fail(MVB_ERR_ARG, "mvb_tau_z_pol: bad arguments");
-  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, "mvb_tau_z_pol");
+      beam_ld < nsrc || nfreq <= 0 || nfreq > 65535)
+    return fail(MVB_ERR_ARG, "%s: bad arguments", who);
+  int rc = check_panel(mode, (int64_t)A * F, Mpad, Kcap, who);
   if (rc) return rc;
-  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "mvb_tau_z_pol: Kcap too small for nsrc * nax");
+  if (round_up(nsrc * X, kKAlign) > Kcap) return fail(MVB_ERR_ARG, "%s: Kcap too small for nsrc * nax", who);
   if (reinterpret_cast<uintptr_t>(coh) % 16 || reinterpret_cast<uintptr_t>(rot) % 16)
-    return fail(MVB_ERR_ARG, "mvb_tau_z_pol: coh and rot must be 16-byte aligned");
+    return fail(MVB_ERR_ARG, "%s: coh and rot must be 16-byte aligned", who);
+  if (nfreq > 1 && (coh_ld < nsrc || z_stride < (int64_t)mvb_zpanel_bytes(mode, Mpad, Kcap) || z_stride % 16))
+    return fail(MVB_ERR_ARG, "%s: coherency rows or panels overlap", who);
   const int64_t s_max = round_up(nsrc * X, kKAlign) / X;
   if (s_max == 0) return MVB_OK;
-  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts));
+  dim3 grid((unsigned)ceil_div(s_max, kTauZBlockSrc), (unsigned)ceil_div(A, kTauZAnts), (unsigned)nfreq);
   const bool staged = nbeam * F * X <= kTauZMaxBFX;
   const size_t smem = staged ? (size_t)nbeam * F * X * kTauZRow * sizeof(float2) : 0;
   const double foc = freq * kInvC;
@@ -571,14 +610,16 @@ extern "C" int mvb_tau_z_pol(const double *antpos, int A, double freq, const dou
   const float4 *c4 = reinterpret_cast<const float4 *>(coh);
   const double2 *r2 = reinterpret_cast<const double2 *>(rot);
   cudaStream_t s = as_stream(stream);
-#define MVB_TZP(M)                                                                                          \
+#define MVB_TZP(M)                                                                                                \
   do {                                                                                                             \
     if (staged)                                                                                                    \
       tau_z_kernel<M, 2, 0, true, true><<<grid, kTauZThreads, smem, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,      \
-          nullptr, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, nullptr, 0, c4, r2);               \
+          nullptr, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, nullptr, 0, c4, r2, freqs_dev, 0,  \
+          coh_ld, z_stride);                                                                                       \
     else                                                                                                           \
       tau_z_kernel<M, 2, 0, false, true><<<grid, kTauZThreads, 0, s>>>(antpos, A, foc, crd, ld, n_dev, nsrc,        \
-          nullptr, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, nullptr, 0, c4, r2);               \
+          nullptr, sidx, bm, beam_ld, nbeam, beam_idx, F, zscale, z, Mpad, Kcap, nullptr, 0, c4, r2, freqs_dev, 0,  \
+          coh_ld, z_stride);                                                                                       \
   } while (0)
   switch (mode) {
     case MVB_GEMM_BF16_3: MVB_TZP(MVB_GEMM_BF16_3); break;
@@ -589,6 +630,26 @@ extern "C" int mvb_tau_z_pol(const double *antpos, int A, double freq, const dou
   }
 #undef MVB_TZP
   return check_launch("tau_z_kernel(pol)");
+}
+
+extern "C" int mvb_tau_z_pol(const double *antpos, int A, double freq, const double *crd, int64_t ld,
+                             const int32_t *n_dev, int64_t nsrc, const float *coh, const int32_t *sidx,
+                             const double *rot, const void *beam, int64_t beam_ld, int nbeam,
+                             const int32_t *beam_idx, int mode, float zscale, void *z, int64_t Mpad, int64_t Kcap,
+                             void *stream) {
+  return tau_z_pol_impl("mvb_tau_z_pol", antpos, A, freq, nullptr, 1, crd, ld, n_dev, nsrc, coh, 0, sidx, rot, beam,
+                        beam_ld, nbeam, beam_idx, mode, zscale, z, 0, Mpad, Kcap, stream);
+}
+
+extern "C" int mvb_tau_z_pol_grouped(const double *antpos, int A, const double *freqs, int nfreq, const double *crd,
+                                     int64_t ld, const int32_t *n_dev, int64_t nsrc, const float *coh, int64_t coh_ld,
+                                     const int32_t *sidx, const double *rot, const void *beam, int64_t beam_ld,
+                                     int nbeam, const int32_t *beam_idx, int mode, float zscale, void *z,
+                                     size_t z_stride, int64_t Mpad, int64_t Kcap, void *stream) {
+  if (!freqs || z_stride > (size_t)INT64_MAX) return fail(MVB_ERR_ARG, "mvb_tau_z_pol_grouped: bad arguments");
+  return tau_z_pol_impl("mvb_tau_z_pol_grouped", antpos, A, 0.0, freqs, nfreq, crd, ld, n_dev, nsrc, coh, coh_ld,
+                        sidx, rot, beam, beam_ld, nbeam, beam_idx, mode, zscale, z, (int64_t)z_stride, Mpad, Kcap,
+                        stream);
 }
 
 extern "C" int mvb_z_from_exptau(const void *exptau, int e_c128, int64_t e_ld, int A, int64_t nsrc, const float *sflux,

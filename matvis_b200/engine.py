@@ -6,8 +6,11 @@ and chunk with a device synchronisation after each stage (cpu/cpu.py:247-272,
 gpu/gpu.py:197-254).  Here one job is one stream of launches:
 
     for t:      mvb_rotate -> (per chunk) mvb_horizon_compact -> mvb_beam_*
-      for f:    [mvb_beam_* for a beamfits beam] -> mvb_tau_z -> mvb_herk + mvb_herk_reduce
-                (or mvb_vecdot for a short pair list)
+      for each group of G frequencies:
+                mvb_tau_z_grouped -> mvb_herk_grouped -> mvb_herk_reduce_grouped
+                (G panels, one launch each; a beamfits beam, which changes with
+                frequency, or a pair list on mvb_vecdot goes one frequency at a time:
+                [mvb_beam_*] -> mvb_tau_z -> mvb_herk + mvb_herk_reduce or mvb_vecdot)
 
 Rotation, selection and (for an achromatic beam) beam interpolation depend on
 time only and are done once per time for all frequencies.  The above-horizon count never leaves the device:
@@ -26,7 +29,7 @@ from dataclasses import dataclass, replace
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, devcache
 from .beams import B200BeamInterpolator, GridBeam, beams_at_frequency, is_chromatic
 from .coordinates import (
     ENU_TO_ALTAZ,
@@ -36,7 +39,7 @@ from .coordinates import (
     pack_astrom,
     point_source_crd_eq,
 )
-from .getz import ZMatrixCalc
+from .getz import ZMatrixCalc, ZPanel
 from .autotune import tune_k_chunk
 from .matprod import B200MatMul, B200VectorDot, choose_k_chunk, pair_product
 
@@ -45,6 +48,12 @@ from .matprod import B200MatMul, B200VectorDot, choose_k_chunk, pair_product
 #: columns; shorter slices mean more partial tiles to reduce).  The number of
 #: slices is still fitted to whole waves of SMs on the device.
 DEFAULT_K_CHUNK = 4096
+
+#: Frequencies per grouped launch (tau/Z, product and reduction of that many
+#: frequencies of a time step in one launch each, on as many Z panels) unless
+#: the job sets ``freq_group``; fewer when the job has fewer frequencies or the
+#: device memory (``fit_freq_group``) allows fewer.
+DEFAULT_FREQ_GROUP = 8
 
 
 @dataclass
@@ -73,6 +82,11 @@ class JobSpec:
     time_s: np.ndarray | None = None
     #: (2, N) ra / dec in radians for the polarised sky's frame rotation (else from eci)
     radec: np.ndarray | None = None
+    #: frequencies per grouped launch (None: DEFAULT_FREQ_GROUP; 1: one frequency per launch)
+    freq_group: int | None = None
+    #: name of a sky model shared by several jobs: jobs with the same key (and sky
+    #: shape) share one device copy of the source directions and fluxes
+    sky_key: str | None = None
 
 
 def _norm_matprod(name: str) -> str:
@@ -222,6 +236,7 @@ class VisEngine:
         self.chromatic = is_chromatic(s.beams)
         self.beams_per_freq = ([beams_at_frequency(s.beams, f) for f in self.freqs] if self.chromatic
                                else [list(s.beams)])
+        self.fgroup = freq_group_of(s, self.method, self.chromatic)
         self.zscale = 1.0
         if self.method == "MatMul" and _lib.GEMM_MODES.get(s.gemm_mode, s.gemm_mode) == _lib.GEMM_F16_3:
             # |Z| <= max sqrt(0.5 I) * max |beam| (bilinear weights are convex, |exptau| = 1); for a
@@ -279,14 +294,21 @@ class VisEngine:
         self.matprod.setup()
         self.matprod.status = self.status
         self.zcalc = ZMatrixCalc(A, self.nfeed, self.nax, self.cap, mode=zmode, device=dev)
-        self.zcalc.setup()
+        if self.fgroup > 1:
+            # G panels of one allocation: the operands of one grouped launch
+            self.panels = ZPanel.group(self.fgroup, zmode, A, self.nfeed, self.nax, self.cap, dev)
+            self.zcalc.z = self.panels[0]
+            self.freqs_dev = torch.as_tensor(self.freqs, dtype=torch.float64, device=dev)
+        else:
+            self.zcalc.setup()
+            self.panels = [self.zcalc.z]
         self.npairs = self.matprod.npairs
         self.vis = torch.zeros((len(self.freqs), len(self.lsts), self.npairs, self.nfeed, self.nfeed), dtype=self.ctype,
                                device=dev)
         if self.method == "MatMul":
             panel = self.zcalc.z
             self.k_chunk = int(s.k_chunk) if s.k_chunk else DEFAULT_K_CHUNK
-            self.matprod.workspace(panel, self.k_chunk)
+            self.matprod.workspace(panel, self.k_chunk, self.fgroup)
         self._allocated = True
 
     def upload(self, stream=None):
@@ -294,21 +316,40 @@ class VisEngine:
         if not self._allocated:
             self.allocate()
         N = self.nsrc
+        self.antpos.copy_(_pinned(self.antpos_host), non_blocking=True)
+        key = self.spec.sky_key
+        if key is not None and not self.pol_sky and N:
+            # a named sky shared with other jobs: one device copy (read-only here)
+            ck = ("sky", devcache.device_key(self.eci.device), str(key), tuple(self.eci.shape),
+                  tuple(self.freqs.tolist()))
+            self.eci, self.sflux = devcache.CACHE.get(ck, self._upload_sky)
+            self._uploaded = True
+            return
         # every copy is asynchronous on the current stream, from page-locked staging
         if N:
             self.eci[:, :N].copy_(_pinned(self.eci_host), non_blocking=True)
-        self.antpos.copy_(_pinned(self.antpos_host), non_blocking=True)
         if self.pol_sky:
             self.sflux.zero_()  # not read: the polarised writer takes the coherency
         elif N:
-            fl = torch.empty(self.flux_host.shape, dtype=torch.float64, device=self.eci.device)
-            fl.copy_(_pinned(self.flux_host), non_blocking=True)
-            _lib.check(_lib.lib.mvb_flux_sqrt_half(_lib.ptr(fl), self.nsrc, len(self.freqs), _lib.ptr(self.sflux),
-                                                   _lib.stream_handle()))
+            self._fill_sflux(self.sflux)
         if self.pol_sky and N:
             self.coh[:, :N].copy_(_pinned(self.coh_host), non_blocking=True)
             self.radec[:, :N].copy_(_pinned(self.radec_host), non_blocking=True)
         self._uploaded = True
+
+    def _fill_sflux(self, sflux: torch.Tensor):
+        """sqrt(0.5 I) per frequency and source from the host Stokes I (on the device)."""
+        fl = torch.empty(self.flux_host.shape, dtype=torch.float64, device=sflux.device)
+        fl.copy_(_pinned(self.flux_host), non_blocking=True)
+        _lib.check(_lib.lib.mvb_flux_sqrt_half(_lib.ptr(fl), self.nsrc, len(self.freqs), _lib.ptr(sflux),
+                                               _lib.stream_handle()))
+
+    def _upload_sky(self) -> tuple[torch.Tensor, torch.Tensor]:
+        eci = torch.zeros_like(self.eci)
+        eci[:, :self.nsrc].copy_(_pinned(self.eci_host), non_blocking=True)
+        sflux = torch.zeros_like(self.sflux)
+        self._fill_sflux(sflux)
+        return eci, sflux
 
     def h2d_bytes(self) -> int:
         n = self.eci_host.nbytes + self.antpos_host.nbytes + (0 if self.pol_sky else self.flux_host.nbytes)
@@ -353,6 +394,9 @@ class VisEngine:
                     _lib.ptr(self.radec), self.nsrc, _lib.ptr(self.kept), _lib.ptr(self.crd), self.cap,
                     _lib.ptr(self.n_above), self.cap, self.ravg[t].ctypes.data_as(_lib.c_void_p), _lib.ptr(self.rot2),
                     sh))
+            if self.fgroup > 1:
+                self._enqueue_groups(t, c, beam, stream)
+                continue
             for f in range(len(self.freqs)):
                 if self.chromatic:
                     self.bmfuncs[f].launch(self.crd, self.cap, self.n_above, self.cap, beam, stream=stream,
@@ -379,21 +423,55 @@ class VisEngine:
                 else:
                     self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream)
 
+    def _enqueue_groups(self, t: int, c: int, beam: torch.Tensor, stream=None):
+        """Chunk c of time t, frequencies in groups of ``fgroup``: one grouped tau/Z,
+        product and reduction launch per group."""
+        L = _lib.lib
+        sh = _lib.stream_handle(stream)
+        A, F, X = self.nant, self.nfeed, self.nax
+        nf = len(self.freqs)
+        p0 = self.panels[0]
+        zstride = p0.nbytes
+        for f0 in range(0, nf, self.fgroup):
+            g = min(self.fgroup, nf - f0)
+            if self.pol_sky:
+                _lib.check(L.mvb_tau_z_pol_grouped(
+                    _lib.ptr(self.antpos), A, _lib.ptr(self.freqs_dev[f0:]), g, _lib.ptr(self.crd), self.cap,
+                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.coh[f0]), self.coh.shape[1], _lib.ptr(self.kept),
+                    _lib.ptr(self.rot2), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
+                    _lib.ptr(self.bmfunc.beam_index_dev), self.zcalc.mode, self.zscale, _lib.ptr(p0.data), zstride,
+                    p0.Mpad, p0.Kcap, sh))
+            else:
+                _lib.check(L.mvb_tau_z_grouped(
+                    _lib.ptr(self.antpos), A, _lib.ptr(self.freqs_dev[f0:]), g, _lib.ptr(self.crd), self.cap,
+                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f0]), self.sflux.shape[1],
+                    _lib.ptr(self.kept), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
+                    _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode, self.zscale, _lib.ptr(p0.data),
+                    zstride, p0.Mpad, p0.Kcap, sh))
+            for p in self.panels[:g]:
+                p.n_dev = self.n_above
+                p.n_host = self.cap
+                p.scale = self.zscale
+            self.matprod.enqueue_grouped(self.panels[:g], self.vis[f0:f0 + g, t], accumulate=c > 0, stream=stream,
+                                         k_chunk=self.k_chunk)
+
     def device_bytes(self) -> int:
         """Device memory this job holds once allocated."""
         if not self._allocated:
             return estimate_device_bytes(self.spec)
         tensors = [self.eci, self.antpos, self.sflux, self.topo, self.crd, self.kept, self.ws_compact, self.vis,
                    self.zcalc.z.data, self.bmfunc.interpolated_beam]
-        n = sum(t.numel() * t.element_size() for t in tensors)
+        n = sum(t.numel() * t.element_size() for t in tensors) + (len(self.panels) - 1) * self.zcalc.z.nbytes
         ws = getattr(self.matprod, "_ws", None)
         return n + (ws.numel() if ws is not None else 0)
 
     def launches_per_run(self) -> int:
-        # per frequency: tau/Z, then mvb_herk + mvb_herk_reduce or vecdot_kernel + its slice reduction
+        # per frequency (or per group of fgroup frequencies): tau/Z, then the product
+        # and its reduction (mvb_herk[_grouped] + reduce, or vecdot_kernel + its slice reduction)
         per_f = 3
+        nlaunch = len(self.freqs) if self.fgroup <= 1 else -(-len(self.freqs) // self.fgroup)
         # count + scatter + beam (+ frame), per frequency (+ its beam for a beamfits beam)
-        per_chunk = 2 + int(not self.chromatic) + (per_f + int(self.chromatic)) * len(self.freqs) + int(self.pol_sky)
+        per_chunk = 2 + int(not self.chromatic) + (per_f + int(self.chromatic)) * nlaunch + int(self.pol_sky)
         n = len(self.lsts) * (1 + self.nchunks * per_chunk)
         return n + (sum(self.bcrs_plan) if self.bcrs_plan is not None else 0)
 
@@ -486,7 +564,7 @@ class VisEngine:
             self.k_chunk = tune_k_chunk(
                 panel, self.matprod.mode, self.status,
                 run=lambda kc, st: self.matprod.enqueue(panel, scratch, accumulate=False, stream=st, k_chunk=kc))
-            self.matprod.workspace(self.zcalc.z, self.k_chunk)
+            self.matprod.workspace(self.zcalc.z, self.k_chunk, self.fgroup)
             torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream()
@@ -532,11 +610,12 @@ def estimate_device_bytes(spec: JobSpec) -> int:
     else:
         mode = _lib.Z_C64
     mpad, kcap = _lib.zpanel_shape(mode, A * F, cap * X)
-    panel = _lib.lib.mvb_zpanel_bytes(mode, mpad, kcap)
+    G = freq_group_of(spec, method, is_chromatic(spec.beams))
+    panel = G * _lib.lib.mvb_zpanel_bytes(mode, mpad, kcap)
     if method == "MatMul":
         T = mpad // _lib.TILE
         kc = spec.k_chunk or choose_k_chunk(T * (T + 1) // 2, kcap)
-        ws = _lib.lib.mvb_herk_ws_bytes(mpad, kcap, kc)
+        ws = G * _lib.lib.mvb_herk_ws_bytes(mpad, kcap, kc)
     else:
         ws = _lib.lib.mvb_vecdot_ws_bytes(npairs, F, kcap, spec.k_chunk or 4096)
     nbeam = len(spec.beams)
@@ -544,6 +623,29 @@ def estimate_device_bytes(spec: JobSpec) -> int:
     extra = (16 * Nf * N + 16 * N + 16 * cap) if pol_sky else 0  # coherency, ra/dec, frame rotations
     return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + 8 * nbeam * F * X * cap + panel + ws
                + Nf * Nt * npairs * F * F * csize + extra)
+
+
+def freq_group_of(spec: JobSpec, method: str, chromatic: bool) -> int:
+    """Frequencies per grouped launch for this job: 1 for a pair list on per-pair
+    sums (no grouped form) and for a beamfits beam (its beam changes with
+    frequency), else ``spec.freq_group`` (default DEFAULT_FREQ_GROUP), at most
+    the job's frequency count."""
+    if method != "MatMul" or chromatic:
+        return 1
+    g = DEFAULT_FREQ_GROUP if spec.freq_group is None else int(spec.freq_group)
+    if g < 1:
+        raise ValueError("freq_group must be at least 1")
+    return max(1, min(g, len(spec.freqs)))
+
+
+def fit_freq_group(spec: JobSpec, budget: float) -> JobSpec:
+    """``spec`` with the largest frequency group (at most its own) whose job fits
+    ``budget`` bytes; a group of 1 when none does (``plan_job`` then batches)."""
+    method, _ = _resolve_product(spec)
+    g = freq_group_of(spec, method, is_chromatic(spec.beams))
+    while g > 1 and estimate_device_bytes(replace(spec, freq_group=g)) > budget:
+        g //= 2
+    return replace(spec, freq_group=g)
 
 
 def plan_job(spec: JobSpec, budget: float, max_chunks: int = 100) -> tuple[int, int]:

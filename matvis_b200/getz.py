@@ -27,24 +27,43 @@ class ZPanel:
     that count times ``nax``.
     """
 
-    def __init__(self, mode: int, nant: int, nfeed: int, nax: int, nsrc_cap: int, device):
+    def __init__(self, mode: int, nant: int, nfeed: int, nax: int, nsrc_cap: int, device, data=None):
         self.mode = mode
         self.nant, self.nfeed, self.nax = nant, nfeed, nax
         self.M = nant * nfeed
         self.nsrc_cap = nsrc_cap
         self.Mpad, self.Kcap = _lib.zpanel_shape(mode, self.M, nax * nsrc_cap)
-        planes = _lib.zpanel_planes(mode)
-        dt = _lib.zpanel_dtype(mode)
-        if mode == _lib.Z_C64:
-            self.data = torch.zeros((self.M, self.Kcap), dtype=dt, device=device)
-        else:
-            kb = _lib.zpanel_kblock(mode)
-            self.data = torch.zeros((self.Kcap // kb, self.Mpad // _lib.TILE, planes, _lib.TILE, kb), dtype=dt,
-                                    device=device)
+        shape = self.data_shape(mode, self.M, self.Mpad, self.Kcap)
+        if data is None:
+            data = torch.zeros(shape, dtype=_lib.zpanel_dtype(mode), device=device)
+        elif tuple(data.shape) != shape or data.dtype != _lib.zpanel_dtype(mode) or not data.is_contiguous():
+            raise ValueError("panel storage has the wrong shape or type")
+        self.data = data
         self.n_dev = None
         self.n_host = 0
         #: power-of-two factor the panel holds Z multiplied by (fp16x3 mode)
         self.scale = 1.0
+
+    @staticmethod
+    def data_shape(mode: int, M: int, Mpad: int, Kcap: int) -> tuple:
+        if mode == _lib.Z_C64:
+            return (M, Kcap)
+        kb = _lib.zpanel_kblock(mode)
+        return (Kcap // kb, Mpad // _lib.TILE, _lib.zpanel_planes(mode), _lib.TILE, kb)
+
+    @classmethod
+    def group(cls, n: int, mode: int, nant: int, nfeed: int, nax: int, nsrc_cap: int, device) -> list["ZPanel"]:
+        """``n`` panels of one shape in one allocation, consecutive in memory (the
+        operands of one grouped tau/Z and product launch; the byte distance
+        between panels is ``panels[0].nbytes``)."""
+        M = nant * nfeed
+        Mpad, Kcap = _lib.zpanel_shape(mode, M, nax * nsrc_cap)
+        store = torch.zeros((n,) + cls.data_shape(mode, M, Mpad, Kcap), dtype=_lib.zpanel_dtype(mode), device=device)
+        return [cls(mode, nant, nfeed, nax, nsrc_cap, device, data=store[g]) for g in range(n)]
+
+    @property
+    def nbytes(self) -> int:
+        return self.data.numel() * self.data.element_size()
 
     @property
     def shape(self):

@@ -190,11 +190,44 @@ class B200MatMul(MatProd):
         self.k_chunk = k_chunk
         self._ws = None
 
-    def workspace(self, panel: ZPanel, k_chunk: int) -> torch.Tensor:
-        nbytes = _lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, k_chunk)
+    def workspace(self, panel: ZPanel, k_chunk: int, ngroup: int = 1) -> torch.Tensor:
+        """Partial-tile workspace for ``ngroup`` panels of ``panel``'s shape (kept
+        and grown as needed)."""
+        nbytes = ngroup * _lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, k_chunk)
         if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = None
             self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         return self._ws
+
+    def enqueue_grouped(self, panels: list[ZPanel], out: torch.Tensor, accumulate: bool = False, stream=None,
+                        k_chunk=None):
+        """Products of consecutive panels of one allocation (``ZPanel.group``) in
+        one launch, all with panels[0]'s column count; panel g's visibilities go
+        to ``out[g]`` (``out`` indexed along its first dimension, any stride)."""
+        ng = len(panels)
+        p0 = panels[0]
+        if ng == 1:
+            return self.enqueue(p0, out[0], accumulate=accumulate, stream=stream, k_chunk=k_chunk)
+        stride = panels[1].data.data_ptr() - p0.data.data_ptr()
+        if any(p.data.data_ptr() - p0.data.data_ptr() != g * stride for g, p in enumerate(panels)):
+            raise ValueError("grouped panels must be equally spaced in one allocation")
+        kc = k_chunk or self.resolve_k_chunk(p0)
+        ws = self.workspace(p0, kc, ng)
+        sh = stream_handle(stream)
+        check(
+            _lib.lib.mvb_herk_grouped(
+                ptr(p0.data), stride, ng, self.mode, p0.Mpad, p0.Kcap, ptr(p0.n_dev), p0.n_host, p0.nax, kc,
+                self.drain_ksteps, ptr(ws), ws.numel(), ptr(self.status), sh,
+            )
+        )
+        pairs = None if self.all_pairs else self._pairs_dev
+        check(
+            _lib.lib.mvb_herk_reduce_grouped(
+                ptr(ws), ws.numel(), ng, p0.Mpad, p0.Kcap, ptr(p0.n_dev), p0.n_host, p0.nax, kc, self.nant,
+                self.nfeed, ptr(pairs), self.npairs, ptr(out), out.stride(0) * out.element_size(),
+                1 if out.dtype == torch.complex128 else 0, 1.0 / p0.scale**2, int(accumulate), sh,
+            )
+        )
 
     def resolve_k_chunk(self, panel: ZPanel) -> int:
         if self.k_chunk is not None:

@@ -68,7 +68,7 @@ class VisServer:
     """Continuous-batching visibility server on one device."""
 
     def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 8, steps_per_turn: int = 1,
-                 reserve_fraction: float = 0.5):
+                 reserve_fraction: float = 0.5, keep_results: bool = True):
         self.device = _lib.require_cuda(device)
         free = torch.cuda.mem_get_info(self.device)[0]
         self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
@@ -81,6 +81,10 @@ class VisServer:
             del reserve
         self.max_active = max_active
         self.steps_per_turn = steps_per_turn
+        #: False: results keep the latency and term count only (a long benchmark stream)
+        self.keep_results = keep_results
+        #: kernel launches of the admitted jobs (engine.launches_per_run summed)
+        self.launches = 0
         self._pending: deque[_Job] = deque()
         self._active: list[_Job] = []
         self._finishing: list[_Job] = []
@@ -165,6 +169,7 @@ class VisServer:
                     job.engine.allocate()
                     job.engine.upload()
                     job.engine.status.zero_()
+                self.launches += job.engine.launches_per_run()
                 self._active.append(job)
         self.max_concurrent = max(self.max_concurrent, len(self._active))
 
@@ -203,8 +208,11 @@ class VisServer:
             vis = job.host
             if vis is not None and not job.spec.polarized:
                 vis = vis[..., 0, 0]
+            if not self.keep_results:
+                vis = None
             self._results[job.jid] = JobResult(jid=job.jid, vis=None if err else vis, latency_s=job.t_done - job.t_submit,
                                                queue_s=job.t_admit - job.t_submit, terms=job.terms, error=err)
+            job.spec = None
             with self._lock:
                 self.in_use -= job.footprint
             self._finishing.remove(job)
@@ -238,19 +246,24 @@ class VisServer:
             if time.perf_counter() - t0 > timeout_s:
                 raise TimeoutError("server did not drain in time")
 
-    def serve_stream(self, arrivals: list[tuple[float, JobSpec]], timeout_s: float = 3600.0) -> list[int]:
-        """Submit jobs at their arrival offsets (seconds from now) while serving."""
+    def serve_stream(self, arrivals, timeout_s: float = 3600.0) -> list[int]:
+        """Submit jobs at their arrival offsets (seconds from now) while serving.
+
+        ``arrivals``: (offset_s, JobSpec) pairs -- a list (sorted here) or any
+        iterable in non-decreasing offset order, e.g. a generator that builds
+        each job only when its turn comes, so a long stream never holds all its
+        skies in host memory at once."""
         t0 = time.perf_counter()
         ids = []
-        i = 0
-        arrivals = sorted(arrivals, key=lambda a: a[0])
-        while i < len(arrivals) or not self.idle():
+        it = iter(sorted(arrivals, key=lambda a: a[0]) if isinstance(arrivals, list) else arrivals)
+        nxt = next(it, None)
+        while nxt is not None or not self.idle():
             now = time.perf_counter() - t0
-            while i < len(arrivals) and arrivals[i][0] <= now:
-                ids.append(self.submit(arrivals[i][1], t_submit=t0 + arrivals[i][0]))
-                i += 1
-            if self.idle() and i < len(arrivals):
-                time.sleep(min(0.001, max(0.0, arrivals[i][0] - now)))
+            while nxt is not None and nxt[0] <= now:
+                ids.append(self.submit(nxt[1], t_submit=t0 + nxt[0]))
+                nxt = next(it, None)
+            if self.idle() and nxt is not None:
+                time.sleep(min(0.001, max(0.0, nxt[0] - now)))
                 continue
             self.poll()
             if not self._active and self._finishing and not self._pending:

@@ -265,18 +265,24 @@ def subset(cfg: dict, nsrc: int | None = None, nfreq: int | None = None, ntimes:
 
 def config5_jobs(njobs: int = 2000, rate_hz: float = 20.0, seed: int = 5, nsrc_max: int = 500_000,
                  nant_max: int = 512):
+    """The config-5 stream as a list (see ``config5_stream``)."""
+    return list(config5_stream(njobs, rate_hz, seed, nsrc_max, nant_max))
+
+
+def config5_stream(njobs: int = 2000, rate_hz: float = 20.0, seed: int = 5, nsrc_max: int = 500_000,
+                   nant_max: int = 512):
     """Served-form stream: Poisson arrivals (rate_hz), per job Nant log-uniform in
     [16, nant_max] (positions uniform in a 300 m disc), Nsrc log-uniform in
     [1e3, nsrc_max] isotropic with N(>S) ~ S^-1.5 fluxes, Nfreq U{1..32},
     Ntimes U{1..16}, beam either the unpolarised Gaussian or config 2's polarised
-    grid.  Returns [(arrival_s, JobSpec)]."""
+    grid.  Yields (arrival_s, JobSpec) in arrival order, building each job only
+    when it is asked for."""
     from .engine import JobSpec
     from .coordinates import point_source_crd_eq
 
     rng = rng_for(seed)
     grid_beams = dipole_beams(rng_for(2), 1)
     t = 0.0
-    out = []
     for _ in range(njobs):
         t += rng.exponential(1.0 / rate_hz)
         nant = int(round(np.exp(rng.uniform(np.log(16), np.log(nant_max)))))
@@ -292,5 +298,4 @@ def config5_jobs(njobs: int = 2000, rate_hz: float = 20.0, seed: int = 5, nsrc_m
         spec = JobSpec(antpos=antpos, eci=point_source_crd_eq(ra, dec), fluxes=np.repeat(flux[:, None], nf, axis=1),
                        freqs=freqs, lsts=lsts, latitude=HERA_LAT,
                        beams=grid_beams if pol else [GaussianBeam(sigma=0.2)], polarized=pol, precision=1)
-        out.append((t, spec))
-    return out
+        yield t, spec

@@ -38,7 +38,7 @@ from . import _lib
 from ._utils import get_desired_chunks
 from .beams import beams_at_frequency
 from .coordinates import latitude_of, lsts_of, point_source_crd_eq, radec_of
-from .engine import JobSpec, VisEngine, _norm_matprod, plan_job
+from .engine import JobSpec, VisEngine, _norm_matprod, fit_freq_group, plan_job
 
 
 logger = logging.getLogger(__name__)
@@ -155,6 +155,7 @@ def simulate_vis(
     pair_product: str = "auto",
     gemm_mode: str = "fp16x3",
     k_chunk: int | None = None,
+    freq_group: int | None = None,
     min_chunks: int = 1,
     max_memory=np.inf,
     memory_buffer: float = 0.9,
@@ -167,9 +168,11 @@ def simulate_vis(
     ``ra``/``dec`` radians; ``freqs`` Hz; ``times`` LSTs (radians).
 
     The job is sized against ``memory_buffer`` x min(``max_memory``, the device's
-    free memory): one batched job when it fits, else contiguous frequency batches
-    (and, if one frequency does not fit, more source chunks), each written into
-    its slice of one host array (``engine.plan_job``).  ``beam_spline_opts`` and
+    free memory): one batched job when it fits (with ``freq_group`` frequencies
+    per grouped launch, fewer if memory is short: ``engine.fit_freq_group``),
+    else contiguous frequency batches (and, if one frequency does not fit, more
+    source chunks), each written into its slice of one host array
+    (``engine.plan_job``).  ``beam_spline_opts`` and
     ``max_progress_reports`` are accepted for the reference's keyword set and
     have no effect; any other keyword is an error, as in the reference.
     """
@@ -195,7 +198,7 @@ def simulate_vis(
         latitude=latitude_of(telescope_loc),
         beam_idx=beam_idx, polarized=polarized, antpairs=antpairs, precision=precision, gemm_mode=gemm_mode,
         matprod=_norm_matprod(matprod_method), pair_product=pair_product, k_chunk=k_chunk, source_buffer=source_buffer,
-        nchunks=max(1, int(min_chunks)), **rot_kw,
+        nchunks=max(1, int(min_chunks)), freq_group=freq_group, **rot_kw,
     )
     # frequency-dependent (beamfits) beams are interpolated per frequency inside the
     # one batched job (the reference re-interpolates per frequency, wrapper.py:180-199)
@@ -203,7 +206,9 @@ def simulate_vis(
     dev = _lib.require_cuda(device)
     # memory the caching allocator holds but does not use is free for this job too
     free = torch.cuda.mem_get_info(dev)[0] + torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
-    nfb, nchunks = plan_job(spec, min(max_memory, free) * memory_buffer)
+    budget = min(max_memory, free) * memory_buffer
+    spec = fit_freq_group(spec, budget)
+    nfb, nchunks = plan_job(spec, budget)
     if nfb >= freqs.size and nchunks == spec.nchunks:
         vis = VisEngine(spec, device=dev).run_to_host()
         return vis if polarized else vis[..., 0, 0]

@@ -185,10 +185,10 @@ def test_simulate_vis_frequency_batches(device, caplog):
     ants = {i: tuple(p) for i, p in enumerate(cfg["antpos"])}
     kw = dict(fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"], times=cfg["lsts"],
               beams=cfg["beams"], telescope_loc=cfg["latitude"], polarized=True, beam_idx=cfg["beam_idx"],
-              precision=2)
+              precision=2, freq_group=1)
     spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"],
                            freqs=cfg["freqs"], lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"],
-                           beam_idx=cfg["beam_idx"], polarized=True, precision=2)
+                           beam_idx=cfg["beam_idx"], polarized=True, precision=2, freq_group=1)
 
     def size(n):
         return estimate_device_bytes(replace(spec, freqs=spec.freqs[:n], fluxes=spec.fluxes[:, :n]))

@@ -63,3 +63,42 @@ def test_admission_respects_budget(device):
     assert all(r.error is None for r in srv.results.values())
     with pytest.raises(ValueError, match="HBM"):
         VisServer(hbm_budget=16).submit(jobs[0])
+
+
+def test_served_jobs_share_beam_and_named_sky_copies(device):
+    """Polarised jobs with equal beam grids share one device copy; jobs naming the
+    same sky (JobSpec.sky_key) share its directions and fluxes; results equal the
+    unshared runs bit for bit."""
+    from dataclasses import replace
+
+    from matvis_b200 import devcache
+
+    cfg = wl.subset(wl.config2(nfreq=3, ntimes=2), nsrc=4000, nfreq=3, ntimes=2, nant=30, seed=4)
+    from matvis_b200.engine import job_from_arrays
+
+    base = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
+                           lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
+                           polarized=True)
+    plain = VisEngine(base).run().cpu().numpy()
+    other_times = replace(base, lsts=base.lsts + 0.3)
+    plain2 = VisEngine(other_times).run().cpu().numpy()
+    e1 = VisEngine(replace(base, sky_key="sky-A"))
+    e1.upload()
+    e2 = VisEngine(replace(other_times, sky_key="sky-A"))
+    e2.upload()
+    assert e1.eci.data_ptr() == e2.eci.data_ptr() and e1.sflux.data_ptr() == e2.sflux.data_ptr()
+    assert e1.bmfunc.grids.data_ptr() == e2.bmfunc.grids.data_ptr()
+    np.testing.assert_array_equal(e1.run().cpu().numpy(), plain)
+    np.testing.assert_array_equal(e2.run().cpu().numpy(), plain2)
+    assert devcache.CACHE.hits >= 2
+
+
+def test_served_stream_from_a_generator_without_kept_results(device):
+    """A lazily built stream (config5_stream) serves every job; keep_results=False
+    keeps latencies and term counts only."""
+    srv = VisServer(max_active=4, keep_results=False)
+    ids = srv.serve_stream(wl.config5_stream(njobs=8, seed=13, nsrc_max=20000, nant_max=96))
+    assert len(ids) == 8 and srv.launches > 0
+    summ = latency_summary(srv.results)
+    assert summ["jobs"] == 8 and summ["terms"] > 0
+    assert all(r.vis is None and r.error is None for r in srv.results.values())

@@ -493,3 +493,26 @@ def test_simulate_vis_buffer_validation(kwarg, value, errmsg):
               dec=np.full(15, -0.5), freqs=np.array([100e6]), times=np.zeros(5), beams=[], telescope_loc=-0.5)
     with pytest.raises(ValueError, match=errmsg):
         simulate_vis(**kw, **{kwarg: value})
+
+
+def test_frequency_group_fits_memory():
+    """fit_freq_group keeps the job's group when it fits, halves it while it does
+    not, and falls back to one frequency per launch (then plan_job batches)."""
+    from dataclasses import replace
+
+    from matvis_b200 import workloads as wl
+    from matvis_b200.engine import estimate_device_bytes, fit_freq_group, freq_group_of, job_from_arrays
+
+    cfg = wl.subset(wl.config2(nfreq=16, ntimes=2), nsrc=3000, nfreq=16, ntimes=2, nant=40, seed=1)
+    spec = job_from_arrays(ants=cfg["antpos"], fluxes=cfg["fluxes"], ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"],
+                           lsts=cfg["lsts"], latitude=cfg["latitude"], beams=cfg["beams"], beam_idx=cfg["beam_idx"],
+                           polarized=True)
+    assert freq_group_of(spec, "MatMul", False) == 8
+    assert freq_group_of(replace(spec, freq_group=32), "MatMul", False) == 16  # at most Nf
+    assert freq_group_of(spec, "VectorDot", False) == 1 and freq_group_of(spec, "MatMul", True) == 1
+    sizes = {g: estimate_device_bytes(replace(spec, freq_group=g)) for g in (1, 2, 4, 8)}
+    assert sizes[1] < sizes[2] < sizes[4] < sizes[8]
+    assert fit_freq_group(spec, sizes[8]).freq_group == 8
+    assert fit_freq_group(spec, sizes[8] - 1).freq_group == 4
+    assert fit_freq_group(spec, sizes[2]).freq_group == 2
+    assert fit_freq_group(spec, 1.0).freq_group == 1
