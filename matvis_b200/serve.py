@@ -9,6 +9,11 @@ Jobs (``JobSpec``) arrive at any time.  The server
   resident on the device, and gives it its own CUDA stream;
 * advances the active jobs one time step at a time, round robin, so their
   kernels overlap on the device;
+* optionally (``small_job_terms``) treats jobs below a size as a priority
+  class: they are admitted ahead of larger pending jobs and run on
+  high-priority streams, whose thread blocks the GPU dispatches first as SMs
+  free up, so a short job does not wait behind a long one; larger jobs keep
+  their arrival order;
 * hands each finished job to a copier thread, which waits for the job's last
   kernel on its own stream, copies the visibilities and the status word to the
   host (touching the result's pages first), and counts the job's terms, so the
@@ -23,6 +28,7 @@ mix.  ``latency_summary`` reports p50 / p99 and the throughput.
 
 from __future__ import annotations
 
+import os
 import queue
 import threading
 import time
@@ -34,6 +40,13 @@ import torch
 
 from . import _lib
 from .engine import JobSpec, VisEngine, estimate_device_bytes
+
+# The jobs' streams map onto the device's hardware work queues, 8 by default;
+# with more active jobs than queues, kernels of unrelated jobs serialise behind
+# each other.  32 queues measured p50 1.27 s against 2.18 s on the 2,000-job
+# config-5 stream at 8 active jobs.  Only effective before the process's first
+# CUDA call (set it in the environment otherwise).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 
 @dataclass
@@ -48,6 +61,7 @@ class _Job:
     host: np.ndarray | None = None
     status_word: int = 0
     footprint: int = 0
+    small: bool = False
     t_admit: float = 0.0
     t_done: float = 0.0
     terms: float = 0.0
@@ -67,8 +81,8 @@ class JobResult:
 class VisServer:
     """Continuous-batching visibility server on one device."""
 
-    def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 8, steps_per_turn: int = 1,
-                 reserve_fraction: float = 0.5, keep_results: bool = True):
+    def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 32, steps_per_turn: int = 1,
+                 reserve_fraction: float = 0.5, keep_results: bool = True, small_job_terms: float | None = 2e11):
         self.device = _lib.require_cuda(device)
         free = torch.cuda.mem_get_info(self.device)[0]
         self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
@@ -85,6 +99,9 @@ class VisServer:
         self.keep_results = keep_results
         #: kernel launches of the admitted jobs (engine.launches_per_run summed)
         self.launches = 0
+        #: jobs of at most this many (estimated) terms form the priority class
+        self.small_job_terms = small_job_terms
+        self._small: deque[_Job] = deque()
         self._pending: deque[_Job] = deque()
         self._active: list[_Job] = []
         self._finishing: list[_Job] = []
@@ -137,8 +154,10 @@ class VisServer:
         with self._lock:
             jid = self._next_id
             self._next_id += 1
-            self._pending.append(_Job(jid=jid, spec=spec, t_submit=time.perf_counter() if t_submit is None else t_submit,
-                                      footprint=fp))
+            job = _Job(jid=jid, spec=spec, t_submit=time.perf_counter() if t_submit is None else t_submit, footprint=fp)
+            small = self.small_job_terms is not None and estimate_terms(spec) <= self.small_job_terms
+            (self._small if small else self._pending).append(job)
+            job.small = small
         return jid
 
     def result(self, jid: int) -> JobResult | None:
@@ -150,20 +169,24 @@ class VisServer:
 
     def idle(self) -> bool:
         with self._lock:
-            return not self._pending and not self._active and not self._finishing
+            return not self._pending and not self._small and not self._active and not self._finishing
 
     # ------------------------------------------------------------ scheduling
     def _admit(self):
         with self._lock:
-            while self._pending and len(self._active) < self.max_active:
-                job = self._pending[0]
+            while len(self._active) < self.max_active:
+                # the priority class first, each class in arrival order
+                q = self._small if self._small else self._pending
+                if not q:
+                    break
+                job = q[0]
                 if self.in_use + job.footprint > self.budget:
                     break
-                self._pending.popleft()
+                q.popleft()
                 self.in_use += job.footprint
                 self.peak_in_use = max(self.peak_in_use, self.in_use)
                 job.t_admit = time.perf_counter()
-                job.stream = torch.cuda.Stream(device=self.device)
+                job.stream = torch.cuda.Stream(device=self.device, priority=-1 if job.small else 0)
                 with torch.cuda.stream(job.stream):
                     job.engine = VisEngine(job.spec, device=self.device)
                     job.engine.allocate()
@@ -271,6 +294,13 @@ class VisServer:
             if time.perf_counter() - t0 > timeout_s:
                 raise TimeoutError("serve_stream did not finish in time")
         return ids
+
+
+def estimate_terms(spec: JobSpec) -> float:
+    """Antenna-pair x source terms of a job, with half the sky above the horizon
+    (for scheduling; the reported counts are exact)."""
+    npairs = len(spec.antpos) ** 2 if spec.antpairs is None else len(spec.antpairs)
+    return float(npairs) * 0.5 * np.asarray(spec.eci).shape[1] * len(spec.freqs) * len(spec.lsts)
 
 
 def latency_summary(results: dict[int, JobResult]) -> dict:

@@ -102,3 +102,23 @@ def test_served_stream_from_a_generator_without_kept_results(device):
     summ = latency_summary(srv.results)
     assert summ["jobs"] == 8 and summ["terms"] > 0
     assert all(r.vis is None and r.error is None for r in srv.results.values())
+
+
+def test_small_jobs_form_a_priority_class(device):
+    """With one execution slot, a small job submitted after a large one is admitted
+    first and runs on a high-priority stream; both results are correct."""
+    from matvis_b200.serve import estimate_terms
+
+    big, small = _jobs()[:2]
+    if estimate_terms(big) < estimate_terms(small):
+        big, small = small, big
+    srv = VisServer(max_active=1, small_job_terms=estimate_terms(small))
+    jb = srv.submit(big)
+    js = srv.submit(small)
+    srv.poll()
+    assert [j.jid for j in srv._active + srv._finishing] == [js]
+    srv.run_until_idle()
+    assert srv.result(js).error is None and srv.result(jb).error is None
+    assert srv.result(js).queue_s <= srv.result(jb).queue_s
+    np.testing.assert_array_equal(srv.result(js).vis, (lambda a: a if small.polarized else a[..., 0, 0])(
+        VisEngine(small).run().cpu().numpy()))
