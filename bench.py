@@ -394,7 +394,8 @@ def herk_roofline(eng, args, dev) -> dict:
             if r == 2:
                 h0.record(hs)
             _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), eng.matprod.mode, panel.Mpad, panel.Kcap,
-                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, 0, _lib.ptr(ws), ws.numel(),
+                                         _lib.ptr(eng.n_above), 0, eng.nax, kc, eng.matprod.drain_ksteps, _lib.ptr(ws),
+                                         ws.numel(),
                                          _lib.ptr(eng.status), _lib.stream_handle(hs)))
         h1.record(hs)
     torch.cuda.synchronize()
@@ -563,6 +564,8 @@ def run_b200(args, rank, world, local_rank):
                                               panel.Kcap),
             "parallelism": "replicas (one job per GPU)" if world > 1 else "1 GPU",
             "precision": "FP64 rotation/horizon/phase reduction, FP32 sincos and Z, " + product,
+            "freq_group": eng.fgroup,
+            "autotune": eng.tuned,
         },
         "roofline": roofline,
         "gpu_launches": eng.launches_per_run() * args.steps,

@@ -218,10 +218,11 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
  * 64).  Their count, between ceil(K_valid / k_chunk) and 31 more, is chosen on
  * the device from K_valid so that tiles x slices fills whole waves of SMs; one
  * partial tile is written per (k-slice, tile).
- * drain_ksteps (1, 2 or 4; 0 = default: 1 for MVB_GEMM_BF16_6, else 2) is the
- * number of 32-byte k-steps summed in one TMEM block before the block is added
- * to FP32 registers: the tensor core rounds its accumulator toward zero at every
- * instruction, so short blocks bound that drift.
+ * drain_ksteps (1, 2 or 4; 0 = default 2) is the number of 32-byte k-steps
+ * summed in one TMEM block before the block is added to FP32 registers: the
+ * tensor core rounds its accumulator toward zero at every instruction, so short
+ * blocks bound that drift; a block's products are issued in ascending
+ * magnitude (the hi x hi products last).
  * Replaces GPUMatMul.compute -> zdotz -> cublas.c/zgemm (gpu/matprod.py:31-36,
  * gpu/_cublas.py:7-65) and CPUMatMul.compute's z.conj().dot(z.T)
  * (cpu/matprod.py:11-32); computes only the upper-triangle tiles. */

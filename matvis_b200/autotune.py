@@ -1,17 +1,25 @@
-"""Autotuner for the Hermitian product's k-slice length.
+"""Autotuner for the Hermitian product: k-slice length and drain interval, timed
+on the job's own Z panel; frequencies per grouped launch sized to memory.
 
-The k-slice (``k_chunk``) sets how many source columns one work unit of
-``mvb_herk`` accumulates before its partial tile is written: short slices give
-more units (better balance across the SMs) but more partial-tile traffic and a
-longer FP64 reduction; long slices the reverse.  Every candidate keeps the
-accumulation error below 1e-6 (each 32-byte k-step is summed in a fresh TMEM
-block and slices are reduced in FP64), so the choice is speed only.
+* ``k_chunk`` -- how many source columns one work unit of ``mvb_herk``
+  accumulates before its partial tile is written: short slices give more units
+  (better balance across the SMs) but more partial-tile traffic and a longer
+  FP64 reduction; long slices the reverse.
+* ``drain_ksteps`` (KD) -- how many 32-byte k-steps the tensor core sums in one
+  TMEM block before the epilogue adds the block to FP32 registers.  Fewer drains
+  leave the UMMAs more of the SM, but the accumulator is truncated toward zero
+  at every instruction, so the error grows with KD.  The block's products are
+  issued in ascending magnitude (cross terms first), and the errors measured on a
+  whole config-2 slice against the FP64 oracle (``MEASURED_ERROR``) decide which
+  KD are candidates: those under ``ERROR_BUDGET``.
+* frequencies per grouped launch (``fit_freq_group`` in the engine): the job time
+  measured the same for 1 to 16 frequencies per launch (1.69-1.72 s for the
+  config-2 job), so the group is sized by memory, not timed.
 
-``tune_k_chunk`` times each candidate on the job's own Z panel (a few launches,
-CUDA events on a side stream) -- the product together with its reduction when
-the caller passes ``run``, since shorter slices also mean more partial tiles to
-reduce -- and caches the winner per (mode, Mpad, K bucket) for the life of the
-process.
+``tune_product`` times every candidate pair (a few launches each, CUDA events
+on a side stream) -- the product together with its reduction when the caller
+passes ``run`` -- and caches the winner per (mode, Mpad, K bucket, device) for
+the life of the process.  ``last_choice`` reports the latest decision.
 """
 
 from __future__ import annotations
@@ -20,8 +28,22 @@ import torch
 
 from . import _lib
 
-CANDIDATES = (1024, 2048, 4096)
-_cache: dict[tuple, int] = {}
+KC_CANDIDATES = (1024, 2048, 4096, 8192)
+KD_CANDIDATES = (1, 2, 4)
+#: max |V - V_oracle| / sqrt(|V_ii| |V_jj|) measured on a whole config-2 slice
+#: (196,608 sources, 350 antennas, complex128 output, k_chunk 4096) per split
+#: mode and drain interval; product time per slice in the comment (one B200)
+MEASURED_ERROR = {
+    _lib.GEMM_F16_3: {1: 2.82e-7, 2: 3.62e-7, 4: 7.01e-7},   # 1.32 / 1.17 / 1.29 ms
+    _lib.GEMM_TF32_3: {1: 2.34e-7, 2: 2.86e-7, 4: 4.25e-7},  # 2.60 / 2.16 / 2.58 ms
+    _lib.GEMM_BF16_6: {1: 2.23e-7, 2: 2.91e-7, 4: 4.94e-7},  # 2.08 / 1.95 / 2.27 ms
+    _lib.GEMM_BF16_3: {1: 3.5e-6, 2: 3.5e-6, 4: 3.5e-6},     # the 2-term bf16 split itself misses the bar
+}
+#: largest accepted measured error of a drain interval (the bar is 1e-6)
+ERROR_BUDGET = 6e-7
+_cache: dict[tuple, tuple[int, int]] = {}
+#: the latest decision: candidates timed (ms per launch) and the winner
+last_choice: dict = {}
 
 
 def _bucket(k: int) -> int:
@@ -31,40 +53,64 @@ def _bucket(k: int) -> int:
     return b
 
 
-def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidates=CANDIDATES, run=None) -> int:
-    """Fastest k_chunk for this panel shape (panel.n_dev / n_host give the valid K).
+def drain_candidates(mode: int, kd_candidates=KD_CANDIDATES) -> list[int]:
+    """Drain intervals whose measured error fits ERROR_BUDGET (0 = the mode's
+    default, always allowed); the lowest-error one if none does."""
+    meas = MEASURED_ERROR.get(mode, {})
+    ok = [d for d in kd_candidates if d == 0 or meas.get(d, float("inf")) <= ERROR_BUDGET]
+    return ok or [min(meas, key=meas.get, default=1)]
 
-    ``run(k_chunk, stream)``, if given, enqueues everything that depends on the
-    k-slice (product and reduction); otherwise the product alone is timed."""
+
+def tune_product(panel, mode: int, status: torch.Tensor, run=None, reps: int = 3, kc_candidates=KC_CANDIDATES,
+                 kd_candidates=KD_CANDIDATES) -> tuple[int, int]:
+    """Fastest (k_chunk, drain_ksteps) for this panel shape (panel.n_dev / n_host
+    give the valid K).
+
+    ``run(k_chunk, drain_ksteps, stream)``, if given, enqueues everything that
+    depends on the two (product and reduction); otherwise the product alone is
+    timed."""
+    global last_choice
     kvalid = panel.n_host * panel.nax if panel.n_dev is None else int(panel.n_dev.item()) * panel.nax
-    key = (mode, panel.Mpad, _bucket(max(kvalid, 1)), torch.cuda.current_device())
+    kcs = [c for c in kc_candidates if c <= max(kvalid, kc_candidates[0])] or [kc_candidates[0]]
+    kds = drain_candidates(mode, kd_candidates)
+    key = (mode, panel.Mpad, _bucket(max(kvalid, 1)), torch.cuda.current_device(), tuple(kcs), tuple(kds))
     if key in _cache:
         return _cache[key]
-    cands = [c for c in candidates if c <= max(kvalid, candidates[0])] or [candidates[0]]
     ws = None
     if run is None:
-        nbytes = max(_lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, c) for c in cands)
+        nbytes = max(_lib.lib.mvb_herk_ws_bytes(panel.Mpad, panel.Kcap, c) for c in kcs)
         ws = torch.empty(nbytes, dtype=torch.uint8, device=panel.data.device)
     s = torch.cuda.Stream(device=panel.data.device)
     s.wait_stream(torch.cuda.current_stream())
-    best, best_ms = cands[0], float("inf")
+    best, best_ms = (kcs[0], kds[0]), float("inf")
+    timed = {}
     with torch.cuda.stream(s):
-        for c in cands:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            for r in range(reps + 1):
-                if r == 1:
-                    e0.record(s)
-                if run is not None:
-                    run(c, s)
-                    continue
-                _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), mode, panel.Mpad, panel.Kcap, _lib.ptr(panel.n_dev),
-                                             panel.n_host, panel.nax, c, 0, _lib.ptr(ws), ws.numel(), _lib.ptr(status),
-                                             _lib.stream_handle(s)))
-            e1.record(s)
-            e1.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            if ms < best_ms:
-                best, best_ms = c, ms
+        for kd in kds:
+            for c in kcs:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                for r in range(reps + 1):
+                    if r == 1:
+                        e0.record(s)
+                    if run is not None:
+                        run(c, kd, s)
+                        continue
+                    _lib.check(_lib.lib.mvb_herk(_lib.ptr(panel.data), mode, panel.Mpad, panel.Kcap,
+                                                 _lib.ptr(panel.n_dev), panel.n_host, panel.nax, c, kd, _lib.ptr(ws),
+                                                 ws.numel(), _lib.ptr(status), _lib.stream_handle(s)))
+                e1.record(s)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                timed[f"k_chunk={c},drain_ksteps={kd}"] = round(ms, 4)
+                if ms < best_ms:
+                    best, best_ms = (c, kd), ms
     torch.cuda.current_stream().wait_stream(s)
     _cache[key] = best
+    last_choice = {"k_chunk": best[0], "drain_ksteps": best[1], "ms": round(best_ms, 4), "timed_ms": timed,
+                   "shape": {"Mpad": panel.Mpad, "K": kvalid, "mode": mode}}
     return best
+
+
+def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidates=KC_CANDIDATES, run=None) -> int:
+    """k-slice length alone (the mode's default drain interval)."""
+    r = None if run is None else (lambda c, kd, st: run(c, st))
+    return tune_product(panel, mode, status, run=r, reps=reps, kc_candidates=candidates, kd_candidates=(0,))[0]

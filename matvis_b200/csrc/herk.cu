@@ -18,10 +18,15 @@
 // Accuracy.  The tensor core rounds its FP32 accumulator toward zero at every
 // UMMA, so a long in-TMEM sum drifts by about one ulp per instruction (3e-5
 // relative after 2,048 columns).  Each group of KD k-steps (32-byte column
-// blocks) is therefore accumulated into a FRESH TMEM block, products in ascending order of
-// magnitude -- BF16_6 {11, 02, 20, 01, 10, 00}, BF16_3 / TF32_3 {01, 10, 00} -- so
-// only the final hi x hi UMMAs round at full magnitude, and the block is drained
-// by the epilogue warps into FP32 registers with round-to-nearest adds.  One
+// blocks; KD = 2 by default, one stage) is therefore accumulated into a FRESH
+// TMEM block, products in ascending order of magnitude -- BF16_6 {11, 02, 20, 01,
+// 10, 00}, BF16_3 / TF32_3 / F16_3 {01, 10, 00}, each product over all the
+// block's k-steps before the next -- so only the final hi x hi UMMAs round at
+// full magnitude, and the block is drained by the epilogue warps into FP32
+// registers with round-to-nearest adds.  (Issuing the cross terms of both
+// k-steps of a stage before its hi x hi products, instead of k-step by k-step,
+// measured 3.6e-7 against 5.0e-7 on a whole config-2 slice and a 4 % shorter
+// product.)  One
 // k-slice (k_chunk columns) of register sums is one partial tile; slices are
 // summed in float-float (TwoSum, ~2^-44) and rounded to FP64 by herk_reduce_*.
 //
@@ -76,6 +81,7 @@ struct HerkCfg {
   static constexpr int OPER_BYTES = 2 * P * kPlaneBytes;
   static constexpr int STAGE_BYTES = 2 * OPER_BYTES;
   static constexpr int STAGES = kSmemBudget / STAGE_BYTES;
+  static_assert(STAGES >= 2, "a drained block of four k-steps holds two stages");
   static constexpr int NPROD = P == 3 ? 6 : 3;
   // UMMA operand format: 0 = F16, 1 = BF16, 2 = TF32
   static constexpr uint32_t FMT = MODE == MVB_GEMM_TF32_3 ? 2u : (MODE == MVB_GEMM_F16_3 ? 0u : 1u);
@@ -253,6 +259,67 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
       bool ok = true;
+      if constexpr (KD == 2 || KD == 4) {
+        // a TMEM block is KD / 2 whole stages (two k-steps each): products
+        // ordered by magnitude across the block's k-steps -- every cross term,
+        // then the hi x hi products -- so that the block's large partial sum
+        // exists only for its last instructions (the accumulator is truncated
+        // toward zero at each)
+        constexpr int SPB = KD / 2;
+        for (int ks = 0; ks < nks; ks += KD) {
+          const int nk = min(KD, nks - ks);
+          const int nst = (nk + 1) / 2;
+          uint32_t slot[SPB];
+          if (!mbar_wait(&dempty_bar[buf], ((dph >> buf) & 1u) ^ 1u, wait_ns)) ok = false;
+#pragma unroll
+          for (int j = 0; j < SPB; ++j) {
+            if (j >= nst || !ok) break;
+            if (!mbar_wait(&full_bar[st], ph, wait_ns)) {
+              ok = false;
+              break;
+            }
+            slot[j] = st;
+            if (++st == C::STAGES) {
+              st = 0;
+              ph ^= 1;
+            }
+          }
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t d = tbase + buf * 256;
+#pragma unroll
+          for (int q = 0; q < C::NPROD; ++q) {
+            uint32_t pa, pb;
+            product_terms(C::NPROD, q, pa, pb);
+#pragma unroll
+            for (int kk = 0; kk < KD; ++kk) {
+              if (kk >= nk) break;
+              const uint32_t a_base =
+                  smem_u32(smem + (size_t)slot[kk >> 1] * C::STAGE_BYTES) + (uint32_t)(kk & 1) * 32;
+              const uint32_t b_base = diag ? a_base : a_base + C::OPER_BYTES;
+              const uint64_t a_re = umma_desc_sw64(a_base + (2 * pa) * kPlaneBytes);
+              const uint64_t a_im = umma_desc_sw64(a_base + (2 * pa + 1) * kPlaneBytes);
+              const uint64_t b_re = umma_desc_sw64(b_base + (2 * pb) * kPlaneBytes);
+              const uint64_t b_im = umma_desc_sw64(b_base + (2 * pb + 1) * kPlaneBytes);
+              umma<MODE>(d, a_re, b_re, C::ID256, (q > 0 || kk > 0) ? 1u : 0u);
+              umma<MODE>(d, a_im, b_im, C::ID128, 1u);
+              umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < SPB; ++j)
+            if (j < nst) tc_commit(&empty_bar[slot[j]]);  // the block's stages are consumed
+          tc_commit(&dfull_bar[buf]);                      // the block is complete
+          dph ^= 1u << buf;
+          buf ^= 1u;
+        }
+        if (!ok) {
+          atomicOr(status, MVB_DEV_TIMEOUT);
+          abort_flag = 1;
+          break;
+        }
+        continue;
+      }
       // k-steps in order; a TMEM block holds KD of them, a stage (one 64-byte
       // k-block) two: the block and stage boundaries are independent
       for (int ks = 0; ks < nks; ++ks) {
@@ -594,8 +661,8 @@ static int herk_impl(const char *who, const void *z, int64_t zstride, int ngroup
   if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "%s: ws must be 16-byte aligned", who);
   if (drain_ksteps < 0 || drain_ksteps > 4 || drain_ksteps == 3)
     return fail(MVB_ERR_ARG, "%s: drain_ksteps must be 0, 1, 2 or 4", who);
-  // default: 6-product mode drains every k-step, 3-product modes every 2
-  const int kd = drain_ksteps ? drain_ksteps : (mode == MVB_GEMM_BF16_6 ? 1 : 2);
+  // default: a block per stage (two k-steps), the fastest interval in every mode
+  const int kd = drain_ksteps ? drain_ksteps : 2;
   cudaStream_t s = as_stream(stream);
   float *part = static_cast<float *>(ws);
 #define MVB_HERK(M)                                                                                                \

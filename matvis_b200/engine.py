@@ -40,7 +40,8 @@ from .coordinates import (
     point_source_crd_eq,
 )
 from .getz import ZMatrixCalc, ZPanel
-from .autotune import tune_k_chunk
+from . import autotune
+from .autotune import KD_CANDIDATES, tune_product
 from .matprod import B200MatMul, B200VectorDot, choose_k_chunk, pair_product
 
 #: k-slice of the Hermitian product without autotuning: the tuner's choice for
@@ -248,6 +249,8 @@ class VisEngine:
         self._graph = None
         self._allocated = False
         self._uploaded = False
+        #: the autotuner's decision for this job (set by capture())
+        self.tuned: dict | None = None
 
     # ------------------------------------------------------------------ setup
     def allocate(self):
@@ -559,12 +562,23 @@ class VisEngine:
         self.enqueue()  # warm-up: function attributes, lazy module loading
         torch.cuda.synchronize()
         if self.method == "MatMul" and not self.spec.k_chunk:
-            # the panel holds the last slice: time the k-slice candidates on it
+            # the panel holds the last slice: time the (k-slice, drain interval) candidates on it
             panel, scratch = self.zcalc.z, torch.empty_like(self.vis[0, 0])
-            self.k_chunk = tune_k_chunk(
-                panel, self.matprod.mode, self.status,
-                run=lambda kc, st: self.matprod.enqueue(panel, scratch, accumulate=False, stream=st, k_chunk=kc))
-            self.matprod.workspace(self.zcalc.z, self.k_chunk, self.fgroup)
+            mp = self.matprod
+            kd0 = mp.drain_ksteps
+
+            def run(kc, kd, st):
+                mp.drain_ksteps = kd
+                mp.enqueue(panel, scratch, accumulate=False, stream=st, k_chunk=kc)
+
+            try:
+                self.k_chunk, kd = tune_product(panel, mp.mode, self.status, run=run,
+                                                kd_candidates=(kd0,) if kd0 else KD_CANDIDATES)
+            finally:
+                mp.drain_ksteps = kd0
+            mp.drain_ksteps = kd
+            self.tuned = dict(autotune.last_choice) or {"k_chunk": self.k_chunk, "drain_ksteps": kd, "cached": True}
+            mp.workspace(self.zcalc.z, self.k_chunk, self.fgroup)
             torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream()

@@ -103,3 +103,25 @@ def test_job_with_frequency_groups_vs_oracle(device, group):
                            latitude=cfg["latitude"], beams=beams, polarized=True, beam_idx=cfg["beam_idx"])
     err = orc.cosine_error_metric(vis, ref, 2)
     assert err <= 1e-6, err
+
+
+def test_autotuner_reports_its_choice(device):
+    """capture() times (k_chunk, drain interval) candidates on the job's panel and
+    records the winner; the captured job still meets the parity bar."""
+    from matvis_b200 import autotune
+
+    cfg = wl.subset(wl.config2(nfreq=4, ntimes=2), nsrc=20000, nfreq=2, ntimes=1, seed=2)
+    eng = VisEngine(_spec(cfg, precision=2))
+    eng.upload()
+    eng.run()
+    autotune._cache.clear()
+    eng.capture()
+    t = eng.tuned
+    assert t["k_chunk"] in autotune.KC_CANDIDATES and t["drain_ksteps"] in (1, 2)
+    assert len(t["timed_ms"]) >= 2 and min(t["timed_ms"].values()) == t["ms"]
+    vis = eng.run().cpu().numpy()
+    beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in cfg["beams"]]
+    ref = orc.simulate_vis(ants={i: tuple(p) for i, p in enumerate(cfg["antpos"])}, fluxes=cfg["fluxes"],
+                           ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"], lsts=cfg["lsts"],
+                           latitude=cfg["latitude"], beams=beams, polarized=True, beam_idx=cfg["beam_idx"])
+    assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6

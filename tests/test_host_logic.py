@@ -516,3 +516,18 @@ def test_frequency_group_fits_memory():
     assert fit_freq_group(spec, sizes[8] - 1).freq_group == 4
     assert fit_freq_group(spec, sizes[2]).freq_group == 2
     assert fit_freq_group(spec, 1.0).freq_group == 1
+
+
+def test_autotuner_drain_candidates_stay_within_the_error_budget():
+    """The drain interval is tuned only among intervals whose measured error (whole
+    config-2 slice against the FP64 oracle) fits the budget: fp16x3 drains every 1
+    or 2 k-steps, tf32x3 and bf16x6 every 1, 2 or 4; bf16x3, which misses the bar
+    at any interval, keeps its most accurate one."""
+    from matvis_b200 import _lib
+    from matvis_b200.autotune import ERROR_BUDGET, drain_candidates
+
+    assert drain_candidates(_lib.GEMM_F16_3) == [1, 2]
+    assert drain_candidates(_lib.GEMM_TF32_3) == drain_candidates(_lib.GEMM_BF16_6) == [1, 2, 4]
+    assert drain_candidates(_lib.GEMM_BF16_3) == [1]
+    assert drain_candidates(_lib.GEMM_F16_3, (0,)) == [0]
+    assert ERROR_BUDGET < 1e-6
