@@ -366,8 +366,12 @@ class VisEngine:
         for t in range(len(self.lsts)):
             self.enqueue_time(t, stream)
 
-    def enqueue_time(self, t: int, stream=None):
-        """Enqueue the kernels of time index t (all chunks and frequencies)."""
+    def enqueue_time(self, t: int, stream=None, after=None):
+        """Enqueue the kernels of time index t (all chunks and frequencies).
+
+        ``after(f0, g)``, if given, is called once the launches that complete
+        frequencies f0 .. f0 + g - 1 of this time are enqueued (for a results
+        copy that can start as soon as they have run)."""
         L = _lib.lib
         sh = _lib.stream_handle(stream)
         chk = _lib.check
@@ -397,8 +401,9 @@ class VisEngine:
                     _lib.ptr(self.radec), self.nsrc, _lib.ptr(self.kept), _lib.ptr(self.crd), self.cap,
                     _lib.ptr(self.n_above), self.cap, self.ravg[t].ctypes.data_as(_lib.c_void_p), _lib.ptr(self.rot2),
                     sh))
+            last = c == self.nchunks - 1
             if self.fgroup > 1:
-                self._enqueue_groups(t, c, beam, stream)
+                self._enqueue_groups(t, c, beam, stream, after if last else None)
                 continue
             for f in range(len(self.freqs)):
                 if self.chromatic:
@@ -425,8 +430,10 @@ class VisEngine:
                     self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream, k_chunk=self.k_chunk)
                 else:
                     self.matprod.enqueue(panel, out, accumulate=c > 0, stream=stream)
+                if last and after is not None:
+                    after(f, 1)
 
-    def _enqueue_groups(self, t: int, c: int, beam: torch.Tensor, stream=None):
+    def _enqueue_groups(self, t: int, c: int, beam: torch.Tensor, stream=None, after=None):
         """Chunk c of time t, frequencies in groups of ``fgroup``: one grouped tau/Z,
         product and reduction launch per group."""
         L = _lib.lib
@@ -457,6 +464,8 @@ class VisEngine:
                 p.scale = self.zscale
             self.matprod.enqueue_grouped(self.panels[:g], self.vis[f0:f0 + g, t], accumulate=c > 0, stream=stream,
                                          k_chunk=self.k_chunk)
+            if after is not None:
+                after(f0, g)
 
     def device_bytes(self) -> int:
         """Device memory this job holds once allocated."""
@@ -495,11 +504,11 @@ class VisEngine:
     def run_to_host(self, out: np.ndarray | None = None) -> np.ndarray:
         """Run the job and return the visibilities in host memory (``out`` if given).
 
-        As soon as the kernels of a time step have run, a helper thread copies
-        that step's visibilities (all frequencies) into ``out`` on its own
+        As soon as the kernels of a group of frequencies of a time step have
+        run, a helper thread copies those visibilities into ``out`` on its own
         stream, so the device -> host copy, and the first touch of freshly
         allocated host pages (slower than the copy itself), overlap the compute
-        of the later time steps.
+        that follows; only the last group's copy runs after the compute.
         """
         if not self._uploaded:
             self.upload()
@@ -525,13 +534,13 @@ class VisEngine:
                 torch.cuda.set_device(dev)
                 with torch.cuda.stream(side):
                     while (item := steps.get()) is not None:
-                        t, done = item
-                        # touch the destination pages while the step still computes, so that
-                        # the copy after it is not held up by first-touch page faults
-                        for f in range(nf):
+                        t, f0, g, done = item
+                        # touch the destination pages while the group still computes, so
+                        # that the copy after it is not held up by first-touch page faults
+                        for f in range(f0, f0 + g):
                             out[f, t].reshape(-1)[::page] = 0
                         side.wait_event(done)
-                        for f in range(nf):
+                        for f in range(f0, f0 + g):
                             host[f, t].copy_(self.vis[f, t])
             except BaseException as exc:  # re-raised on the calling thread
                 errors.append(exc)
@@ -542,10 +551,12 @@ class VisEngine:
         worker.start()
         try:
             for t in range(nt):
-                self.enqueue_time(t)
-                done = torch.cuda.Event()
-                done.record(main)
-                steps.put((t, done))
+                def after(f0, g, t=t):
+                    done = torch.cuda.Event()
+                    done.record(main)
+                    steps.put((t, f0, g, done))
+
+                self.enqueue_time(t, after=after)
         finally:
             steps.put(None)
             worker.join()
