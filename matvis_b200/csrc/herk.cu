@@ -10,10 +10,12 @@
 //   Im V[m, n] = sum_k Zr[m,k] Zi[n,k] - Zi[m,k] Zr[n,k]
 // A 128 x 128 complex tile (I, J), I <= J, lives in one 128 x 256 FP32 TMEM
 // block D (columns 0..127 real, 128..255 imaginary) filled by three UMMAs per
-// k-step and split-term product (pa, pb):
-//   D[:,   0:256] += Zr_I^pa . [Zr_J^pb ; Zi_J^pb]^T     (N = 256)
+// k-step and split-term product (pa, pb), issued in this order:
 //   D[:,   0:128] += Zi_I^pa . Zi_J^pb^T                  (N = 128)
 //   D[:, 128:256] += Zi_I^pa . (-Zr_J^pb)^T               (N = 128, negate-B bit)
+//   D[:,   0:256] += Zr_I^pa . [Zr_J^pb ; Zi_J^pb]^T     (N = 256)
+// (with the N = 256 product first the whole-slice error measured 3.6e-7
+// against 3.0e-7 at the same speed)
 //
 // Accuracy.  The tensor core rounds its FP32 accumulator toward zero at every
 // UMMA, so a long in-TMEM sum drifts by about one ulp per instruction (3e-5
@@ -301,9 +303,12 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
               const uint64_t a_im = umma_desc_sw64(a_base + (2 * pa + 1) * kPlaneBytes);
               const uint64_t b_re = umma_desc_sw64(b_base + (2 * pb) * kPlaneBytes);
               const uint64_t b_im = umma_desc_sw64(b_base + (2 * pb + 1) * kPlaneBytes);
-              umma<MODE>(d, a_re, b_re, C::ID256, (q > 0 || kk > 0) ? 1u : 0u);
-              umma<MODE>(d, a_im, b_im, C::ID128, 1u);
-              umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+              // the two N = 128 products first: the block's real and imaginary
+              // halves each start from Zi terms, then take the Zr terms
+              const uint32_t acc = (q > 0 || kk > 0) ? 1u : 0u;
+              umma<MODE>(d, a_im, b_im, C::ID128, acc);
+              umma<MODE>(d + 128, a_im, b_re, C::ID128N, acc);
+              umma<MODE>(d, a_re, b_re, C::ID256, 1u);
             }
           }
 #pragma unroll
@@ -313,13 +318,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           dph ^= 1u << buf;
           buf ^= 1u;
         }
-        if (!ok) {
-          atomicOr(status, MVB_DEV_TIMEOUT);
-          abort_flag = 1;
-          break;
-        }
-        continue;
-      }
+      } else {
       // k-steps in order; a TMEM block holds KD of them, a stage (one 64-byte
       // k-block) two: the block and stage boundaries are independent
       for (int ks = 0; ks < nks; ++ks) {
@@ -349,9 +348,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           const uint64_t a_im = umma_desc_sw64(a_base + (2 * pa + 1) * kPlaneBytes);
           const uint64_t b_re = umma_desc_sw64(b_base + (2 * pb) * kPlaneBytes);
           const uint64_t b_im = umma_desc_sw64(b_base + (2 * pb + 1) * kPlaneBytes);
-          umma<MODE>(d, a_re, b_re, C::ID256, (ks % KD != 0 || q > 0) ? 1u : 0u);
-          umma<MODE>(d, a_im, b_im, C::ID128, 1u);
-          umma<MODE>(d + 128, a_im, b_re, C::ID128N, 1u);
+          const uint32_t acc = (ks % KD != 0 || q > 0) ? 1u : 0u;
+          umma<MODE>(d, a_im, b_im, C::ID128, acc);
+          umma<MODE>(d + 128, a_im, b_re, C::ID128N, acc);
+          umma<MODE>(d, a_re, b_re, C::ID256, 1u);
         }
         if ((ks & 1) == 1 || ks == nks - 1) {  // the stage is consumed
           tc_commit(&empty_bar[st]);
@@ -365,6 +365,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           dph ^= 1u << buf;
           buf ^= 1u;
         }
+      }
       }
       if (!ok) {
         atomicOr(status, MVB_DEV_TIMEOUT);

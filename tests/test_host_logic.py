@@ -520,14 +520,16 @@ def test_frequency_group_fits_memory():
 
 def test_autotuner_drain_candidates_stay_within_the_error_budget():
     """The drain interval is tuned only among intervals whose measured error (whole
-    config-2 slice against the FP64 oracle) fits the budget: fp16x3 drains every 1
-    or 2 k-steps, tf32x3 and bf16x6 every 1, 2 or 4; bf16x3, which misses the bar
-    at any interval, keeps its most accurate one."""
+    config-2 slice against the FP64 oracle) fits the budget: every interval for
+    fp16x3, tf32x3 and bf16x6, none for bf16x3, which misses the bar at any
+    interval and keeps its most accurate one."""
     from matvis_b200 import _lib
-    from matvis_b200.autotune import ERROR_BUDGET, drain_candidates
+    from matvis_b200.autotune import ERROR_BUDGET, MEASURED_ERROR, drain_candidates
 
-    assert drain_candidates(_lib.GEMM_F16_3) == [1, 2]
-    assert drain_candidates(_lib.GEMM_TF32_3) == drain_candidates(_lib.GEMM_BF16_6) == [1, 2, 4]
+    for m in (_lib.GEMM_F16_3, _lib.GEMM_TF32_3, _lib.GEMM_BF16_6):
+        assert drain_candidates(m) == [1, 2, 4]
+    assert drain_candidates(_lib.GEMM_F16_3, (1, 2, 4, 8)) == [1, 2, 4]  # unmeasured intervals are not candidates
+    assert max(MEASURED_ERROR[_lib.GEMM_F16_3].values()) <= ERROR_BUDGET
     assert drain_candidates(_lib.GEMM_BF16_3) == [1]
     assert drain_candidates(_lib.GEMM_F16_3, (0,)) == [0]
     assert ERROR_BUDGET < 1e-6
