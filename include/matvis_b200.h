@@ -239,6 +239,30 @@ int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t 
 int mvb_herk_grouped(const void *z, size_t z_stride, int ngroup, int mode, int64_t Mpad, int64_t Kcap,
                      const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int drain_ksteps, void *ws,
                      size_t ws_bytes, int32_t *status, void *stream);
+/* One group of mvb_herk_batch: ngroup panels of one shape, z_stride bytes apart,
+ * with the arguments mvb_herk_grouped takes for them. */
+typedef struct {
+  const void *z;
+  size_t z_stride;
+  int ngroup;
+  int64_t Mpad, Kcap;
+  const int32_t *n_dev;
+  int64_t n_host;
+  int kmul, k_chunk;
+  void *ws;
+  size_t ws_bytes;
+  int32_t *status;
+} mvb_herk_group;
+/* The products of several panel groups of different shapes -- the current
+ * frequency groups of several jobs of a server -- in one launch on the
+ * persistent CTAs (at most 32 panels in all).  Every group is planned and
+ * summed exactly as its own mvb_herk_grouped call, so the partial tiles in its
+ * ws, and the visibilities mvb_herk_reduce_grouped then writes from them, are
+ * bit-identical to that call's.  A bounded wait that runs out sets
+ * MVB_DEV_TIMEOUT in every group's status word.  Replaces the per-job GPUMatMul
+ * calls of jobs run side by side (gpu/matprod.py:31-36); the reference runs one
+ * job at a time. */
+int mvb_herk_batch(const mvb_herk_group *groups, int ngroups, int mode, int drain_ksteps, void *stream);
 /* Sums the FP32 partial tiles over k-slices in float-float (TwoSum, about
  * 2^-44 relative), rounds to FP64 and writes the visibilities in the
  * reference layout out[pair, p, q] = V[ant_i*F + q, ant_j*F + p]

@@ -94,6 +94,7 @@ _SIGNATURES = {
     "mvb_set_wait_limit_ns": (ctypes.c_uint64, [ctypes.c_uint64]),
     "mvb_herk_grouped": (c_int, [_p, c_size_t, c_int, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, _p,
                                  c_size_t, _p, _p]),
+    "mvb_herk_batch": (c_int, [_p, c_int, c_int, c_int, _p]),
     "mvb_herk_reduce_grouped": (
         c_int,
         [_p, c_size_t, c_int, c_int64, c_int64, _p, c_int64, c_int, c_int, c_int, c_int, _p, c_int64, _p, c_size_t,
@@ -116,6 +117,18 @@ _SIGNATURES = {
         [_p, c_int64, _p, c_int64, c_int, c_int, _p, c_int64, c_int, _p, c_size_t, _p, c_int, c_int, _p],
     ),
 }
+
+
+class HerkGroup(ctypes.Structure):
+    """``mvb_herk_group`` of the C header: one panel group of mvb_herk_batch."""
+
+    _fields_ = [("z", c_void_p), ("z_stride", c_size_t), ("ngroup", c_int), ("Mpad", c_int64), ("Kcap", c_int64),
+                ("n_dev", c_void_p), ("n_host", c_int64), ("kmul", c_int), ("k_chunk", c_int), ("ws", c_void_p),
+                ("ws_bytes", c_size_t), ("status", c_void_p)]
+
+
+#: panels one mvb_herk_batch launch can hold
+MAX_BATCH_PANELS = 32
 
 
 def _load() -> ctypes.CDLL:

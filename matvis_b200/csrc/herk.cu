@@ -165,12 +165,33 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
     umma_bf16(d, a, b, idesc, acc);
 }
 
+// A launch's work units come either from one panel shape repeated ngroup
+// times (the frequencies of a job's time step), or from a table of panels of
+// different shapes (the panel groups of several jobs, mvb_herk_batch).  A table
+// entry is one panel: its k-slice plan fills waves for plan_tiles tiles and its
+// partial tiles sit at index in its group's workspace, so that each group's
+// sums equal those of its own grouped launch.
+constexpr int kMaxBatchPanels = 32;
+struct HerkPanel {
+  const uint8_t *panel;
+  const int32_t *n_dev;
+  float *partials;  // the group's workspace
+  int32_t *status;
+  int64_t n_host, Kcap;
+  int T, kmul, k_chunk, plan_tiles, index;
+};
+struct HerkTable {
+  HerkPanel p[kMaxBatchPanels];
+  int n;
+};
+
 // KD: k-steps accumulated in one TMEM block before it is drained (1, 2 or 4).
 template <int MODE, int KD>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const uint8_t *__restrict__ zpanels, int64_t zstride, int ngroup, int T, int n_tiles,
                 const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm,
-                float *__restrict__ partials, int32_t *__restrict__ status, uint64_t wait_ns) {
+                float *__restrict__ partials, int32_t *__restrict__ status, uint64_t wait_ns,
+                const __grid_constant__ HerkTable table) {
   using C = HerkCfg<MODE>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[C::STAGES];
@@ -181,14 +202,76 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
 
+  __shared__ int s_first[kMaxBatchPanels + 1];  // a table's first unit per panel
+  __shared__ int s_nsplit[kMaxBatchPanels];
+  __shared__ int64_t s_kc[kMaxBatchPanels], s_kvalid[kMaxBatchPanels];
+
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t kvalid = valid_k(n_dev, n_host, kmul, Kcap);
-  int nsplit;
-  int64_t kc;
-  plan_splits(kvalid, n_tiles * ngroup, k_chunk, nsm, nsplit, kc);
-  const int per_panel = n_tiles * nsplit;
-  const int n_units = per_panel * ngroup;
+  const bool tabled = table.n > 0;
+  int64_t kvalid = 0, kc = 0;
+  int per_panel = 0, n_units;
+  if (tabled) {
+    if (warp == 0) {  // every lane plans (plan_splits is warp-wide); lane 0 records
+      int acc = 0;
+      for (int q = 0; q < table.n; ++q) {
+        const HerkPanel &e = table.p[q];
+        const int64_t kv = valid_k(e.n_dev, e.n_host, e.kmul, e.Kcap);
+        int ns;
+        int64_t kcq;
+        plan_splits(kv, e.plan_tiles, e.k_chunk, nsm, ns, kcq);
+        if (lane == 0) {
+          s_first[q] = acc;
+          s_nsplit[q] = ns;
+          s_kc[q] = kcq;
+          s_kvalid[q] = kv;
+        }
+        acc += ns * (e.T * (e.T + 1) / 2);
+      }
+      if (lane == 0) s_first[table.n] = acc;
+    }
+    __syncthreads();
+    n_units = s_first[table.n];
+  } else {
+    kvalid = valid_k(n_dev, n_host, kmul, Kcap);
+    int nsplit;
+    plan_splits(kvalid, n_tiles * ngroup, k_chunk, nsm, nsplit, kc);
+    per_panel = n_tiles * nsplit;
+    n_units = per_panel * ngroup;
+  }
   if ((int)blockIdx.x >= n_units) return;  // uniform over the CTA
+
+  // Where unit u is: its panel and block count, tile, columns and partial tile.
+  auto place = [&](int u, const uint8_t *&zpanel, float *&partial, int &Tu, int &I, int &J, int64_t &k0,
+                   int64_t &klen) {
+    if (tabled) {
+      int q = 0;
+      while (q + 1 < table.n && s_first[q + 1] <= u) ++q;
+      const HerkPanel &e = table.p[q];
+      const int nt = e.T * (e.T + 1) / 2;
+      const int r = u - s_first[q];
+      Tu = e.T;
+      decode_tile(r % nt, e.T, I, J);
+      zpanel = e.panel;
+      partial = e.partials + ((size_t)e.index * s_nsplit[q] * nt + r) * (256 * 128);
+      k0 = (int64_t)(r / nt) * s_kc[q];
+      klen = min(s_kc[q], s_kvalid[q] - k0);
+    } else {
+      const int r = u % per_panel;
+      Tu = T;
+      decode_tile(r % n_tiles, T, I, J);
+      zpanel = zpanels + (int64_t)(u / per_panel) * zstride;
+      partial = partials + (size_t)u * (256 * 128);
+      k0 = (int64_t)(r / n_tiles) * kc;
+      klen = min(kc, kvalid - k0);
+    }
+  };
+  // a bounded wait ran out: every status word of the launch learns it
+  auto flag_timeout = [&]() {
+    if (status) atomicOr(status, MVB_DEV_TIMEOUT);
+    if (tabled)
+      for (int q = 0; q < table.n; ++q)
+        if (table.p[q].status) atomicOr(table.p[q].status, MVB_DEV_TIMEOUT);
+  };
 
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 
@@ -219,18 +302,17 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     // ---------------- bulk-copy producer ----------------
     uint32_t st = 0, ph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      const int g = u / per_panel, s = (u % per_panel) / n_tiles, t = u % n_tiles;
-      const uint8_t *zpanel = zpanels + (int64_t)g * zstride;
-      int I, J;
-      decode_tile(t, T, I, J);
-      const int64_t k0 = (int64_t)s * kc;
-      const int64_t klen = min(kc, kvalid - k0);
+      const uint8_t *zpanel;
+      float *partial;
+      int Tu, I, J;
+      int64_t k0, klen;
+      place(u, zpanel, partial, Tu, I, J, k0, klen);
       const int nkb = (int)((klen + C::KB - 1) / C::KB);
       const bool diag = I == J;
       const uint32_t bytes = diag ? C::OPER_BYTES : 2 * C::OPER_BYTES;
       for (int kbi = 0; kbi < nkb; ++kbi) {
         if (!mbar_wait(&empty_bar[st], ph ^ 1, wait_ns)) {
-          atomicOr(status, MVB_DEV_TIMEOUT);
+          flag_timeout();
           abort_flag = 1;
           break;
         }
@@ -239,9 +321,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         // k-block index: k0 is a multiple of 64 elements, a k-block 64 bytes;
         // operand (kb, R) starts at ((kb T + R) 2P) planes of 8 KB
         const int64_t kb = (k0 + (int64_t)kbi * C::KB) / C::KB;
-        bulk_load(a, zpanel + (kb * T + I) * (int64_t)C::OPER_BYTES, C::OPER_BYTES, &full_bar[st]);
+        bulk_load(a, zpanel + (kb * Tu + I) * (int64_t)C::OPER_BYTES, C::OPER_BYTES, &full_bar[st]);
         if (!diag)
-          bulk_load(a + C::OPER_BYTES, zpanel + (kb * T + J) * (int64_t)C::OPER_BYTES, C::OPER_BYTES, &full_bar[st]);
+          bulk_load(a + C::OPER_BYTES, zpanel + (kb * Tu + J) * (int64_t)C::OPER_BYTES, C::OPER_BYTES, &full_bar[st]);
         ++issued;
         if (++st == C::STAGES) {
           st = 0;
@@ -253,11 +335,11 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     // ---------------- UMMA issuer: one fresh TMEM block per KD k-steps ----------------
     uint32_t st = 0, ph = 0, buf = 0, dph = 0;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      const int s = (u % per_panel) / n_tiles, t = u % n_tiles;
-      int I, J;
-      decode_tile(t, T, I, J);
-      const int64_t k0 = (int64_t)s * kc;
-      const int64_t klen = min(kc, kvalid - k0);
+      const uint8_t *zpanel;
+      float *partial;
+      int Tu, I, J;
+      int64_t k0, klen;
+      place(u, zpanel, partial, Tu, I, J, k0, klen);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       const bool diag = I == J;
       bool ok = true;
@@ -368,7 +450,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       }
       }
       if (!ok) {
-        atomicOr(status, MVB_DEV_TIMEOUT);
+        flag_timeout();
         abort_flag = 1;
         break;
       }
@@ -383,9 +465,11 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 #pragma unroll
     for (int j = 0; j < 64; ++j) acc[j] = 0.f;
     for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
-      const int s = (u % per_panel) / n_tiles;
-      const int64_t k0 = (int64_t)s * kc;
-      const int64_t klen = min(kc, kvalid - k0);
+      const uint8_t *zpanel;
+      float *partial;
+      int Tu, I, J;
+      int64_t k0, klen;
+      place(u, zpanel, partial, Tu, I, J, k0, klen);
       const int nks = (int)((klen + C::KSTEP - 1) / C::KSTEP);
       bool ok = true;
       for (int g0 = 0; g0 < nks; g0 += KD) {
@@ -409,11 +493,11 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         buf ^= 1u;
       }
       if (!ok) {
-        if (lane == 0) atomicOr(status, MVB_DEV_TIMEOUT);
+        if (lane == 0) flag_timeout();
         abort_flag = 1;
         break;
       }
-      float *dst = partials + (size_t)u * (256 * 128) + (size_t)quarter * 64 * 128;
+      float *dst = partial + (size_t)quarter * 64 * 128;
 #pragma unroll
       for (int j = 0; j < 64; ++j) {
         dst[j * 128 + row] = acc[j];
@@ -612,14 +696,23 @@ int set_smem_once(const void *fn, int bytes, int slot) {
 // mvb_set_wait_limit_ns); read at each launch.
 static std::atomic<uint64_t> g_wait_limit_ns{kWaitLimitNs};
 
+// table.n > 0: the units come from the table (z, ngroup, shape and status arguments unused).
 template <int MODE, int KD>
 static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
-                       int64_t n_host, int kmul, int k_chunk, float *partials, int32_t *status, cudaStream_t s) {
+                       int64_t n_host, int kmul, int k_chunk, float *partials, int32_t *status, cudaStream_t s,
+                       const HerkTable &table) {
   using C = HerkCfg<MODE>;
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
   const int nsm = num_sms();
-  const int64_t max_units = (int64_t)ngroup * n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
+  int64_t max_units = (int64_t)ngroup * n_tiles * (ceil_div(Kcap, k_chunk) + kPlanExtra);
+  if (table.n > 0) {
+    max_units = 0;
+    for (int q = 0; q < table.n; ++q) {
+      const HerkPanel &e = table.p[q];
+      max_units += (int64_t)(e.T * (e.T + 1) / 2) * (ceil_div(e.Kcap, e.k_chunk) + kPlanExtra);
+    }
+  }
   const int grid = (int)std::min<int64_t>(max_units, nsm);
   const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
   // slots 16 + 3 * MODE + {0, 1, 2} for KD = {1, 2, 4}
@@ -629,7 +722,7 @@ static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad,
   if (grid <= 0) return MVB_OK;
   herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T, n_tiles,
                                                          n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials, status,
-                                                         g_wait_limit_ns.load(std::memory_order_relaxed));
+                                                         g_wait_limit_ns.load(std::memory_order_relaxed), table);
   return check_launch("herk_kernel");
 }
 
@@ -648,9 +741,10 @@ static int check_herk_shape(const char *who, int ngroup, int64_t Mpad, int64_t K
   return MVB_OK;
 }
 
-static int herk_impl(const char *who, const void *z, int64_t zstride, int ngroup, int mode, int64_t Mpad, int64_t Kcap,
-                     const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int drain_ksteps, void *ws,
-                     size_t ws_bytes, int32_t *status, void *stream) {
+// The checks of one product (a group of ngroup panels of one shape).
+static int check_herk_group(const char *who, const void *z, int64_t zstride, int ngroup, int mode, int64_t Mpad,
+                            int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, const void *ws,
+                            size_t ws_bytes, const int32_t *status) {
   if (!z || !ws || !status) return fail(MVB_ERR_ARG, "%s: bad arguments", who);
   int rc = check_herk_shape(who, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk);
   if (rc) return rc;
@@ -660,16 +754,30 @@ static int herk_impl(const char *who, const void *z, int64_t zstride, int ngroup
   if (ws_bytes / (size_t)ngroup < mvb_herk_ws_bytes(Mpad, Kcap, k_chunk))
     return fail(MVB_ERR_ARG, "%s: workspace too small", who);
   if (reinterpret_cast<uintptr_t>(ws) % 16) return fail(MVB_ERR_ARG, "%s: ws must be 16-byte aligned", who);
+  return MVB_OK;
+}
+
+static int herk_impl(const char *who, const void *z, int64_t zstride, int ngroup, int mode, int64_t Mpad, int64_t Kcap,
+                     const int32_t *n_dev, int64_t n_host, int kmul, int k_chunk, int drain_ksteps, void *ws,
+                     size_t ws_bytes, int32_t *status, void *stream, const HerkTable &table = HerkTable{}) {
+  if (table.n == 0) {
+    int rc = check_herk_group(who, z, zstride, ngroup, mode, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, ws, ws_bytes,
+                              status);
+    if (rc) return rc;
+  }
   if (drain_ksteps < 0 || drain_ksteps > 4 || drain_ksteps == 3)
     return fail(MVB_ERR_ARG, "%s: drain_ksteps must be 0, 1, 2 or 4", who);
   // default: a block per stage (two k-steps), the fastest interval in every mode
   const int kd = drain_ksteps ? drain_ksteps : 2;
   cudaStream_t s = as_stream(stream);
   float *part = static_cast<float *>(ws);
-#define MVB_HERK(M)                                                                                                \
-  return kd == 1   ? launch_herk<M, 1>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
-         : kd == 2 ? launch_herk<M, 2>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s) \
-                   : launch_herk<M, 4>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s)
+#define MVB_HERK(M)                                                                                                 \
+  return kd == 1   ? launch_herk<M, 1>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s, \
+                                       table)                                                                       \
+         : kd == 2 ? launch_herk<M, 2>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s, \
+                                       table)                                                                       \
+                   : launch_herk<M, 4>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s, \
+                                       table)
   switch (mode) {
     case MVB_GEMM_BF16_3: MVB_HERK(MVB_GEMM_BF16_3);
     case MVB_GEMM_BF16_6: MVB_HERK(MVB_GEMM_BF16_6);
@@ -754,6 +862,38 @@ extern "C" int mvb_herk_grouped(const void *z, size_t z_stride, int ngroup, int 
   if (z_stride > (size_t)INT64_MAX) return fail(MVB_ERR_ARG, "mvb_herk_grouped: bad arguments");
   return herk_impl("mvb_herk_grouped", z, (int64_t)z_stride, ngroup, mode, Mpad, Kcap, n_dev, n_host, kmul, k_chunk,
                    drain_ksteps, ws, ws_bytes, status, stream);
+}
+
+extern "C" int mvb_herk_batch(const mvb_herk_group *groups, int ngroups, int mode, int drain_ksteps, void *stream) {
+  if (!groups || ngroups <= 0) return fail(MVB_ERR_ARG, "mvb_herk_batch: bad arguments");
+  HerkTable table{};
+  for (int g = 0; g < ngroups; ++g) {
+    const mvb_herk_group &e = groups[g];
+    if (e.z_stride > (size_t)INT64_MAX) return fail(MVB_ERR_ARG, "mvb_herk_batch: bad arguments");
+    int rc = check_herk_group("mvb_herk_batch", e.z, (int64_t)e.z_stride, e.ngroup, mode, e.Mpad, e.Kcap, e.n_dev,
+                              e.n_host, e.kmul, e.k_chunk, e.ws, e.ws_bytes, e.status);
+    if (rc) return rc;
+    if (table.n + e.ngroup > kMaxBatchPanels)
+      return fail(MVB_ERR_ARG, "mvb_herk_batch: more than %d panels in one launch", kMaxBatchPanels);
+    const int T = (int)(e.Mpad / 128);
+    for (int j = 0; j < e.ngroup; ++j) {
+      HerkPanel &p = table.p[table.n++];
+      p.panel = static_cast<const uint8_t *>(e.z) + (int64_t)j * (int64_t)e.z_stride;
+      p.n_dev = e.n_dev;
+      p.partials = static_cast<float *>(e.ws);
+      p.status = e.status;
+      p.n_host = e.n_host;
+      p.Kcap = e.Kcap;
+      p.T = T;
+      p.kmul = e.kmul;
+      p.k_chunk = e.k_chunk;
+      p.plan_tiles = e.ngroup * (T * (T + 1) / 2);
+      p.index = j;
+    }
+  }
+  const mvb_herk_group &e0 = groups[0];
+  return herk_impl("mvb_herk_batch", e0.z, 0, 1, mode, e0.Mpad, e0.Kcap, e0.n_dev, e0.n_host, e0.kmul, e0.k_chunk,
+                   drain_ksteps, e0.ws, e0.ws_bytes, nullptr, stream, table);
 }
 
 extern "C" int mvb_herk_reduce(const void *ws, size_t ws_bytes, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,

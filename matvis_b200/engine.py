@@ -301,10 +301,10 @@ class VisEngine:
             # G panels of one allocation: the operands of one grouped launch
             self.panels = ZPanel.group(self.fgroup, zmode, A, self.nfeed, self.nax, self.cap, dev)
             self.zcalc.z = self.panels[0]
-            self.freqs_dev = torch.as_tensor(self.freqs, dtype=torch.float64, device=dev)
         else:
             self.zcalc.setup()
             self.panels = [self.zcalc.z]
+        self.freqs_dev = torch.as_tensor(self.freqs, dtype=torch.float64, device=dev)
         self.npairs = self.matprod.npairs
         self.vis = torch.zeros((len(self.freqs), len(self.lsts), self.npairs, self.nfeed, self.nfeed), dtype=self.ctype,
                                device=dev)
@@ -378,32 +378,16 @@ class VisEngine:
         A = self.nant
         F, X = self.nfeed, self.nax
         panel = self.zcalc.z
-        R = np.ascontiguousarray(self.rot[t])
-        src = self.eci
-        if self.bcrs_plan is not None:
-            if self.bcrs_plan[t]:
-                a = self.astrom_packed[t]
-                chk(L.mvb_bcrs(_lib.ptr(self.eci), self.nsrc, a.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.bcrs), sh))
-            src = self.bcrs
-        chk(L.mvb_rotate(_lib.ptr(src), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
         for c in range(self.nchunks):
-            c0 = min(c * self.chunk_size, self.nsrc)
-            c1 = min((c + 1) * self.chunk_size, self.nsrc)
-            chk(L.mvb_horizon_compact(
-                _lib.ptr(self.topo), self.nsrc, c0, c1, None, _lib.ptr(self.crd), _lib.ptr(self.kept), None,
-                _lib.ptr(self.n_above), self.cap, _lib.ptr(self.status), _lib.ptr(self.ws_compact),
-                self.ws_compact.numel(), sh))
-            beam = self.bmfunc.interpolated_beam
-            if not self.chromatic:  # time-only: once for all frequencies
-                self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, beam, stream=stream, status=self.status)
-            if self.pol_sky:
-                chk(L.mvb_coherency_rotation(
-                    _lib.ptr(self.radec), self.nsrc, _lib.ptr(self.kept), _lib.ptr(self.crd), self.cap,
-                    _lib.ptr(self.n_above), self.cap, self.ravg[t].ctypes.data_as(_lib.c_void_p), _lib.ptr(self.rot2),
-                    sh))
+            beam = self.chunk_prologue(t, c, stream)
             last = c == self.nchunks - 1
             if self.fgroup > 1:
-                self._enqueue_groups(t, c, beam, stream, after if last else None)
+                for f0 in range(0, len(self.freqs), self.fgroup):
+                    g = self.tau_z_group(t, f0, beam, stream)
+                    self.matprod.enqueue_grouped(self.panels[:g], self.vis[f0:f0 + g, t], accumulate=c > 0,
+                                                 stream=stream, k_chunk=self.k_chunk)
+                    if last and after is not None:
+                        after(f0, g)
                 continue
             for f in range(len(self.freqs)):
                 if self.chromatic:
@@ -433,39 +417,75 @@ class VisEngine:
                 if last and after is not None:
                     after(f, 1)
 
-    def _enqueue_groups(self, t: int, c: int, beam: torch.Tensor, stream=None, after=None):
-        """Chunk c of time t, frequencies in groups of ``fgroup``: one grouped tau/Z,
-        product and reduction launch per group."""
+    def chunk_prologue(self, t: int, c: int, stream=None) -> torch.Tensor:
+        """The kernels of time t and source chunk c that every frequency shares:
+        for c = 0 the apparent-place refresh and the rotation; then the horizon
+        selection of the chunk, the beam (an achromatic one: once for all
+        frequencies) and the polarised sky's frame rotation.  Returns the beam
+        buffer."""
+        L = _lib.lib
+        sh = _lib.stream_handle(stream)
+        chk = _lib.check
+        if c == 0:
+            R = np.ascontiguousarray(self.rot[t])
+            src = self.eci
+            if self.bcrs_plan is not None:
+                if self.bcrs_plan[t]:
+                    a = self.astrom_packed[t]
+                    chk(L.mvb_bcrs(_lib.ptr(self.eci), self.nsrc, a.ctypes.data_as(_lib.c_void_p),
+                                   _lib.ptr(self.bcrs), sh))
+                src = self.bcrs
+            chk(L.mvb_rotate(_lib.ptr(src), self.nsrc, R.ctypes.data_as(_lib.c_void_p), _lib.ptr(self.topo), sh))
+        c0 = min(c * self.chunk_size, self.nsrc)
+        c1 = min((c + 1) * self.chunk_size, self.nsrc)
+        chk(L.mvb_horizon_compact(
+            _lib.ptr(self.topo), self.nsrc, c0, c1, None, _lib.ptr(self.crd), _lib.ptr(self.kept), None,
+            _lib.ptr(self.n_above), self.cap, _lib.ptr(self.status), _lib.ptr(self.ws_compact),
+            self.ws_compact.numel(), sh))
+        beam = self.bmfunc.interpolated_beam
+        if not self.chromatic:  # time-only: once for all frequencies
+            self.bmfunc.launch(self.crd, self.cap, self.n_above, self.cap, beam, stream=stream, status=self.status)
+        if self.pol_sky:
+            chk(L.mvb_coherency_rotation(
+                _lib.ptr(self.radec), self.nsrc, _lib.ptr(self.kept), _lib.ptr(self.crd), self.cap,
+                _lib.ptr(self.n_above), self.cap, self.ravg[t].ctypes.data_as(_lib.c_void_p), _lib.ptr(self.rot2),
+                sh))
+        return beam
+
+    def tau_z_group(self, t: int, f0: int, beam: torch.Tensor, stream=None) -> int:
+        """One grouped tau/Z launch: frequencies f0 .. f0 + g - 1 (g = fgroup or
+        what is left) of the current chunk into ``panels[:g]``.  Returns g."""
         L = _lib.lib
         sh = _lib.stream_handle(stream)
         A, F, X = self.nant, self.nfeed, self.nax
-        nf = len(self.freqs)
+        g = min(self.fgroup, len(self.freqs) - f0)
         p0 = self.panels[0]
         zstride = p0.nbytes
-        for f0 in range(0, nf, self.fgroup):
-            g = min(self.fgroup, nf - f0)
-            if self.pol_sky:
-                _lib.check(L.mvb_tau_z_pol_grouped(
-                    _lib.ptr(self.antpos), A, _lib.ptr(self.freqs_dev[f0:]), g, _lib.ptr(self.crd), self.cap,
-                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.coh[f0]), self.coh.shape[1], _lib.ptr(self.kept),
-                    _lib.ptr(self.rot2), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
-                    _lib.ptr(self.bmfunc.beam_index_dev), self.zcalc.mode, self.zscale, _lib.ptr(p0.data), zstride,
-                    p0.Mpad, p0.Kcap, sh))
-            else:
-                _lib.check(L.mvb_tau_z_grouped(
-                    _lib.ptr(self.antpos), A, _lib.ptr(self.freqs_dev[f0:]), g, _lib.ptr(self.crd), self.cap,
-                    _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f0]), self.sflux.shape[1],
-                    _lib.ptr(self.kept), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
-                    _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode, self.zscale, _lib.ptr(p0.data),
-                    zstride, p0.Mpad, p0.Kcap, sh))
-            for p in self.panels[:g]:
-                p.n_dev = self.n_above
-                p.n_host = self.cap
-                p.scale = self.zscale
-            self.matprod.enqueue_grouped(self.panels[:g], self.vis[f0:f0 + g, t], accumulate=c > 0, stream=stream,
-                                         k_chunk=self.k_chunk)
-            if after is not None:
-                after(f0, g)
+        if self.pol_sky:
+            _lib.check(L.mvb_tau_z_pol_grouped(
+                _lib.ptr(self.antpos), A, _lib.ptr(self.freqs_dev[f0:]), g, _lib.ptr(self.crd), self.cap,
+                _lib.ptr(self.n_above), self.cap, _lib.ptr(self.coh[f0]), self.coh.shape[1], _lib.ptr(self.kept),
+                _lib.ptr(self.rot2), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
+                _lib.ptr(self.bmfunc.beam_index_dev), self.zcalc.mode, self.zscale, _lib.ptr(p0.data), zstride,
+                p0.Mpad, p0.Kcap, sh))
+        else:
+            _lib.check(L.mvb_tau_z_grouped(
+                _lib.ptr(self.antpos), A, _lib.ptr(self.freqs_dev[f0:]), g, _lib.ptr(self.crd), self.cap,
+                _lib.ptr(self.n_above), self.cap, _lib.ptr(self.sflux[f0]), self.sflux.shape[1],
+                _lib.ptr(self.kept), _lib.ptr(beam), beam.shape[-1], beam.shape[0],
+                _lib.ptr(self.bmfunc.beam_index_dev), F, X, self.zcalc.mode, self.zscale, _lib.ptr(p0.data),
+                zstride, p0.Mpad, p0.Kcap, sh))
+        for p in self.panels[:g]:
+            p.n_dev = self.n_above
+            p.n_host = self.cap
+            p.scale = self.zscale
+        return g
+
+    @property
+    def batchable(self) -> bool:
+        """Whether the job's products can share a launch with other jobs'
+        (mvb_herk_batch): the Hermitian product with an achromatic beam."""
+        return self.method == "MatMul" and not self.chromatic
 
     def device_bytes(self) -> int:
         """Device memory this job holds once allocated."""

@@ -220,12 +220,36 @@ class B200MatMul(MatProd):
                 self.drain_ksteps, ptr(ws), ws.numel(), ptr(self.status), sh,
             )
         )
+        self.reduce_grouped(panels, out, accumulate=accumulate, stream=stream, k_chunk=kc)
+
+    def batch_group(self, panels: list[ZPanel], k_chunk: int) -> _lib.HerkGroup:
+        """The ``mvb_herk_batch`` entry for the products of ``panels`` (consecutive
+        panels of one allocation, all with panels[0]'s column count): run in a
+        batch with other jobs' groups, its partial tiles equal those of
+        enqueue_grouped's product, and ``reduce_grouped`` then writes the same
+        visibilities."""
+        p0 = panels[0]
+        ng = len(panels)
+        stride = panels[1].data.data_ptr() - p0.data.data_ptr() if ng > 1 else 0
+        ws = self.workspace(p0, k_chunk, ng)
+        return _lib.HerkGroup(z=p0.data.data_ptr(), z_stride=stride, ngroup=ng, Mpad=p0.Mpad, Kcap=p0.Kcap,
+                              n_dev=None if p0.n_dev is None else p0.n_dev.data_ptr(), n_host=p0.n_host,
+                              kmul=p0.nax, k_chunk=k_chunk, ws=ws.data_ptr(), ws_bytes=ws.numel(),
+                              status=self.status.data_ptr())
+
+    def reduce_grouped(self, panels: list[ZPanel], out: torch.Tensor, accumulate: bool = False, stream=None,
+                       k_chunk=None):
+        """The reduction of the grouped product of ``panels`` (after mvb_herk_grouped
+        or a batch holding their group): panel g's visibilities to ``out[g]``."""
+        p0 = panels[0]
+        kc = k_chunk or self.resolve_k_chunk(p0)
+        ws = self.workspace(p0, kc, len(panels))
         pairs = None if self.all_pairs else self._pairs_dev
         check(
             _lib.lib.mvb_herk_reduce_grouped(
-                ptr(ws), ws.numel(), ng, p0.Mpad, p0.Kcap, ptr(p0.n_dev), p0.n_host, p0.nax, kc, self.nant,
+                ptr(ws), ws.numel(), len(panels), p0.Mpad, p0.Kcap, ptr(p0.n_dev), p0.n_host, p0.nax, kc, self.nant,
                 self.nfeed, ptr(pairs), self.npairs, ptr(out), out.stride(0) * out.element_size(),
-                1 if out.dtype == torch.complex128 else 0, 1.0 / p0.scale**2, int(accumulate), sh,
+                1 if out.dtype == torch.complex128 else 0, 1.0 / p0.scale**2, int(accumulate), stream_handle(stream),
             )
         )
 

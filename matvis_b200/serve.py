@@ -7,8 +7,13 @@ Jobs (``JobSpec``) arrive at any time.  The server
   others are on the GPU are admitted as soon as slots and memory free up;
 * keeps every admitted job's sky, beams, Z panel and partial visibilities
   resident on the device, and gives it its own CUDA stream;
-* advances the active jobs one time step at a time, round robin, so their
-  kernels overlap on the device;
+* advances the active jobs round robin, so their kernels overlap on the
+  device: each turn, every job's next group of frequencies gets its tau/Z on
+  the job's stream, and the Hermitian products of all those groups run in one
+  launch (``mvb_herk_batch``, up to 32 panels) on a shared stream, ordered
+  against the jobs' streams by events; each job then reduces its own group
+  (jobs whose product cannot be batched -- pair lists on per-pair sums, beamfits
+  beams -- advance a time step per turn on their own stream);
 * optionally (``small_job_terms``) treats jobs below a size as a priority
   class: they are admitted ahead of larger pending jobs and run on
   high-priority streams, whose thread blocks the GPU dispatches first as SMs
@@ -62,6 +67,9 @@ class _Job:
     status_word: int = 0
     footprint: int = 0
     small: bool = False
+    #: next (time, source chunk, first frequency) of a batched job, and its beam buffer
+    cursor: tuple = (0, 0, 0)
+    beam: torch.Tensor | None = None
     t_admit: float = 0.0
     t_done: float = 0.0
     terms: float = 0.0
@@ -82,7 +90,8 @@ class VisServer:
     """Continuous-batching visibility server on one device."""
 
     def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 32, steps_per_turn: int = 1,
-                 reserve_fraction: float = 0.5, keep_results: bool = True, small_job_terms: float | None = 2e11):
+                 reserve_fraction: float = 0.5, keep_results: bool = True, small_job_terms: float | None = 2e11,
+                 batch_products: bool = True):
         self.device = _lib.require_cuda(device)
         free = torch.cuda.mem_get_info(self.device)[0]
         self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
@@ -102,6 +111,13 @@ class VisServer:
         #: jobs of at most this many (estimated) terms form the priority class
         self.small_job_terms = small_job_terms
         self._small: deque[_Job] = deque()
+        #: run the products of the active jobs' current frequency groups in shared launches
+        self.batch_products = batch_products
+        self._batch_streams = {False: torch.cuda.Stream(device=self.device),
+                               True: torch.cuda.Stream(device=self.device, priority=-1)}
+        #: product launches (mvb_herk_batch) and the panel groups they carried
+        self.batch_launches = 0
+        self.batched_groups = 0
         self._pending: deque[_Job] = deque()
         self._active: list[_Job] = []
         self._finishing: list[_Job] = []
@@ -198,8 +214,23 @@ class VisServer:
 
     def _advance(self):
         still = []
+        batch = []
         for job in self._active:
             eng = job.engine
+            if self.batch_products and eng.batchable:
+                # this turn: the job's next frequency group up to its product
+                t, c, f0 = job.cursor
+                if t >= len(eng.lsts):  # no time steps at all
+                    self._finish(job)
+                    continue
+                with torch.cuda.stream(job.stream):
+                    if f0 == 0:
+                        job.beam = eng.chunk_prologue(t, c, stream=job.stream)
+                    g = eng.tau_z_group(t, f0, job.beam, stream=job.stream)
+                    ready = torch.cuda.Event()
+                    ready.record(job.stream)
+                batch.append((job, g, ready))
+                continue
             nt = len(eng.lsts)
             with torch.cuda.stream(job.stream):
                 for _ in range(self.steps_per_turn):
@@ -208,13 +239,69 @@ class VisServer:
                     eng.enqueue_time(job.next_t, stream=job.stream)
                     job.next_t += 1
                 if job.next_t >= nt:
-                    job.done_event = torch.cuda.Event()
-                    job.done_event.record(job.stream)
-                    self._finishing.append(job)
-                    self._to_copy.put(job)
+                    self._finish(job)
                     continue
             still.append(job)
-        self._active = still
+        self._active = still + (self._launch_batches(batch) if batch else [])
+
+    def _finish(self, job: _Job):
+        """The job's last kernel is enqueued: hand it to the copier."""
+        job.done_event = torch.cuda.Event()
+        job.done_event.record(job.stream)
+        self._finishing.append(job)
+        self._to_copy.put(job)
+
+    def _launch_batches(self, batch: list) -> list:
+        """The products of this turn's groups, in launches of at most 32 panels
+        per (split mode, drain interval, priority class); then each job's
+        reduction on its own stream.  Returns the jobs still active."""
+        packs: dict = {}
+        for item in batch:
+            eng = item[0].engine
+            packs.setdefault((eng.matprod.mode, eng.matprod.drain_ksteps, item[0].small), []).append(item)
+        still = []
+        for (mode, kd, small), items in packs.items():
+            while items:
+                take, n = [], 0
+                while items and n + items[0][1] <= _lib.MAX_BATCH_PANELS:
+                    take.append(items.pop(0))
+                    n += take[-1][1]
+                bs = self._batch_streams[small]
+                groups = (_lib.HerkGroup * len(take))()
+                for i, (job, g, ready) in enumerate(take):
+                    bs.wait_event(ready)
+                    eng = job.engine
+                    groups[i] = eng.matprod.batch_group(eng.panels[:g], eng.k_chunk)
+                _lib.check(_lib.lib.mvb_herk_batch(_lib.c_void_p(_lib.ctypes.addressof(groups)), len(take), mode, kd,
+                                                   _lib.stream_handle(bs)))
+                done = torch.cuda.Event()
+                done.record(bs)
+                self.batch_launches += 1
+                self.batched_groups += len(take)
+                for job, g, _ in take:
+                    if self._reduce_and_step(job, g, done):
+                        still.append(job)
+        return still
+
+    def _reduce_and_step(self, job: _Job, g: int, done: torch.cuda.Event) -> bool:
+        """The job's reduction of its batched group, then its cursor moves on;
+        False once the job has enqueued its last kernel."""
+        eng = job.engine
+        t, c, f0 = job.cursor
+        job.stream.wait_event(done)
+        with torch.cuda.stream(job.stream):
+            eng.matprod.reduce_grouped(eng.panels[:g], eng.vis[f0:f0 + g, t], accumulate=c > 0, stream=job.stream,
+                                       k_chunk=eng.k_chunk)
+        f0 += g
+        if f0 >= len(eng.freqs):
+            f0, c = 0, c + 1
+            if c >= eng.nchunks:
+                c, t = 0, t + 1
+        job.cursor = (t, c, f0)
+        if t >= len(eng.lsts):
+            self._finish(job)
+            return False
+        return True
 
     def _retire(self):
         while True:

@@ -185,3 +185,36 @@ def test_pair_lists_are_range_checked_on_the_host():
         B200MatMul(1, 1, 3, np.array([[0, 3]]))
     with pytest.raises(ValueError, match="shape"):
         B200MatMul(1, 1, 3, np.array([[0, 1, 2]]))
+
+
+def test_herk_group_struct_layout():
+    """The ctypes mirror of mvb_herk_group has the C layout (x86-64 alignment):
+    pointers and 64-bit fields on 8-byte boundaries, 88 bytes in all."""
+    from matvis_b200 import _lib
+
+    G = _lib.HerkGroup
+    assert ctypes.sizeof(G) == 88
+    assert [getattr(G, f).offset for f in ("z", "z_stride", "ngroup", "Mpad", "Kcap", "n_dev", "n_host", "kmul",
+                                            "k_chunk", "ws", "ws_bytes", "status")] == [0, 8, 16, 24, 32, 40, 48, 56,
+                                                                                         60, 64, 72, 80]
+    text = HEADER.read_text()
+    assert "} mvb_herk_group;" in text
+
+
+def test_herk_batch_checks_without_gpu():
+    """Every group is checked as mvb_herk_grouped checks it, and the panel total is
+    bounded, before any CUDA call."""
+    from matvis_b200 import _lib
+
+    fake = 256
+    need = _lib.lib.mvb_herk_ws_bytes(768, 4096, 2048)
+    g = _lib.HerkGroup(z=fake, z_stride=0, ngroup=1, Mpad=768, Kcap=4096, n_dev=None, n_host=2048, kmul=2,
+                       k_chunk=2048, ws=fake, ws_bytes=need - 16, status=fake)
+    arr = (_lib.HerkGroup * 1)(g)
+    assert _lib.lib.mvb_herk_batch(ctypes.cast(arr, ctypes.c_void_p), 1, _lib.GEMM_F16_3, 0, None) == _lib.MVB_ERR_ARG
+    assert b"workspace" in _lib.lib.mvb_last_error()
+    g.ws_bytes = 40 * need
+    g.ngroup, g.z_stride = 33, _lib.lib.mvb_zpanel_bytes(_lib.GEMM_F16_3, 768, 4096)
+    arr = (_lib.HerkGroup * 1)(g)
+    assert _lib.lib.mvb_herk_batch(ctypes.cast(arr, ctypes.c_void_p), 1, _lib.GEMM_F16_3, 0, None) == _lib.MVB_ERR_ARG
+    assert b"32 panels" in _lib.lib.mvb_last_error()

@@ -125,3 +125,47 @@ def test_autotuner_reports_its_choice(device):
                            ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"], lsts=cfg["lsts"],
                            latitude=cfg["latitude"], beams=beams, polarized=True, beam_idx=cfg["beam_idx"])
     assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6
+
+
+def test_batched_products_of_different_shapes_equal_their_own_launches(device):
+    """mvb_herk_batch over three panel groups of different shapes (rows, columns,
+    panels per group) leaves in each group's workspace exactly the partial tiles
+    of that group's own mvb_herk_grouped call, and the reductions agree bit for bit."""
+    rng = np.random.default_rng(21)
+    shapes = [(40, 2, 9000, 3), (150, 2, 24000, 1), (70, 1, 15000, 2)]  # (nant, nfeed, K, panels)
+    items = []
+    for nant, nfeed, K, G in shapes:
+        mp = B200MatMul(1, nfeed, nant, None, precision=2, gemm_mode="fp16x3", k_chunk=2048)
+        mp.setup()
+        panels = ZPanel.group(G, mp.mode, nant, nfeed, 1, K, device)
+        for p in panels:
+            z = rng.normal(size=(nant * nfeed, K)) + 1j * rng.normal(size=(nant * nfeed, K))
+            zt = torch.as_tensor(z.astype(np.complex64), device=device)
+            _lib.check(_lib.lib.mvb_z_pack(_lib.ptr(zt), 0, nant * nfeed, K, K, mp.mode, 1.0, _lib.ptr(p.data),
+                                           p.Mpad, p.Kcap, _lib.stream_handle()))
+            p.scale, p.n_dev, p.n_host = 1.0, None, K
+        items.append((mp, panels, G, nant, nfeed))
+    # each group alone
+    alone_ws, alone_out = [], []
+    for mp, panels, G, nant, nfeed in items:
+        out = torch.zeros((G, nant * nant, nfeed, nfeed), dtype=torch.complex128, device=device)
+        mp.workspace(panels[0], 2048, G).zero_()
+        mp.enqueue_grouped(panels, out, k_chunk=2048)
+        torch.cuda.synchronize()
+        alone_ws.append(mp.workspace(panels[0], 2048, G).clone())
+        alone_out.append(out.cpu().numpy())
+        mp.workspace(panels[0], 2048, G).zero_()
+    # all three in one launch
+    groups = (_lib.HerkGroup * 3)()
+    for i, (mp, panels, G, _, _) in enumerate(items):
+        groups[i] = mp.batch_group(panels, 2048)
+    _lib.check(_lib.lib.mvb_herk_batch(_lib.c_void_p(_lib.ctypes.addressof(groups)), 3, _lib.GEMM_F16_3, 0,
+                                       _lib.stream_handle()))
+    for i, (mp, panels, G, nant, nfeed) in enumerate(items):
+        out = torch.zeros((G, nant * nant, nfeed, nfeed), dtype=torch.complex128, device=device)
+        mp.reduce_grouped(panels, out, k_chunk=2048)
+        torch.cuda.synchronize()
+        _lib.check_status_word(mp.status, f"batched group {i}")
+        # the whole workspace (zeroed before either run) holds the same bytes
+        assert torch.equal(mp.workspace(panels[0], 2048, G), alone_ws[i]), i
+        np.testing.assert_array_equal(out.cpu().numpy(), alone_out[i])

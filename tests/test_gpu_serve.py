@@ -24,6 +24,8 @@ def test_served_results_equal_alone_and_in_mix(device):
     # staggered arrivals: later jobs arrive while earlier ones are on the GPU
     ids = srv.serve_stream([(0.002 * i, s) for i, s in enumerate(jobs)])
     assert srv.max_concurrent >= 2
+    # the products of several jobs shared launches
+    assert 0 < srv.batch_launches < srv.batched_groups
     for jid, a, s in zip(ids, alone, jobs):
         r = srv.result(jid)
         assert r.error is None
@@ -91,6 +93,19 @@ def test_served_jobs_share_beam_and_named_sky_copies(device):
     np.testing.assert_array_equal(e1.run().cpu().numpy(), plain)
     np.testing.assert_array_equal(e2.run().cpu().numpy(), plain2)
     assert devcache.CACHE.hits >= 2
+
+
+def test_served_results_equal_without_batched_products(device):
+    """The same jobs with each job's products on its own stream (no shared
+    launches) give the same visibilities bit for bit."""
+    jobs = _jobs()[:4]
+    a = VisServer(max_active=4)
+    ia = a.serve_stream([(0.0, s) for s in jobs])
+    b = VisServer(max_active=4, batch_products=False)
+    ib = b.serve_stream([(0.0, s) for s in jobs])
+    assert a.batch_launches > 0 and b.batch_launches == 0
+    for x, y in zip(ia, ib):
+        np.testing.assert_array_equal(a.result(x).vis, b.result(y).vis)
 
 
 def test_served_stream_from_a_generator_without_kept_results(device):
