@@ -41,8 +41,8 @@ __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + 
 __host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 
 int num_sms();
-// Sets a kernel's max dynamic shared memory once per (device, slot < 32);
-// slots 10 and 11 are the beam kernels, 16..30 the Hermitian-product variants.
+// Sets a kernel's max dynamic shared memory once per (device, slot < 64);
+// slots 10 and 11 are the beam kernels, 16..45 the Hermitian-product variants.
 int set_smem_once(const void *fn, int bytes, int slot);
 
 // Columns of a Z panel are zero-filled up to a multiple of this.

@@ -186,7 +186,8 @@ struct HerkTable {
 };
 
 // KD: k-steps accumulated in one TMEM block before it is drained (1, 2 or 4).
-template <int MODE, int KD>
+// TABLE: the units come from the table (a batch) instead of one repeated shape.
+template <int MODE, int KD, bool TABLE>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const uint8_t *__restrict__ zpanels, int64_t zstride, int ngroup, int T, int n_tiles,
                 const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm,
@@ -207,10 +208,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   __shared__ int64_t s_kc[kMaxBatchPanels], s_kvalid[kMaxBatchPanels];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool tabled = table.n > 0;
+  constexpr bool tabled = TABLE;
   int64_t kvalid = 0, kc = 0;
   int per_panel = 0, n_units;
-  if (tabled) {
+  if constexpr (tabled) {
     if (warp == 0) {  // every lane plans (plan_splits is warp-wide); lane 0 records
       int acc = 0;
       for (int q = 0; q < table.n; ++q) {
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   // Where unit u is: its panel and block count, tile, columns and partial tile.
   auto place = [&](int u, const uint8_t *&zpanel, float *&partial, int &Tu, int &I, int &J, int64_t &k0,
                    int64_t &klen) {
-    if (tabled) {
+    if constexpr (tabled) {
       int q = 0;
       while (q + 1 < table.n && s_first[q + 1] <= u) ++q;
       const HerkPanel &e = table.p[q];
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   // a bounded wait ran out: every status word of the launch learns it
   auto flag_timeout = [&]() {
     if (status) atomicOr(status, MVB_DEV_TIMEOUT);
-    if (tabled)
+    if constexpr (tabled)
       for (int q = 0; q < table.n; ++q)
         if (table.p[q].status) atomicOr(table.p[q].status, MVB_DEV_TIMEOUT);
   };
@@ -681,9 +682,9 @@ __global__ void herk_reduce_pairs_kernel(const float *__restrict__ part, int ngr
 // Raises a kernel's dynamic shared-memory limit once per (device, slot); the
 // attribute is not touched again, in particular not during graph capture.
 int set_smem_once(const void *fn, int bytes, int slot) {
-  static bool done[64][32] = {};
+  static bool done[64][64] = {};
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 32)
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || slot < 0 || slot >= 64)
     return fail(MVB_ERR_CUDA, "set_smem_once: bad device");
   if (done[dev][slot]) return MVB_OK;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -715,14 +716,22 @@ static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad,
   }
   const int grid = (int)std::min<int64_t>(max_units, nsm);
   const size_t smem = (size_t)C::STAGES * C::STAGE_BYTES + 1024;
-  // slots 16 + 3 * MODE + {0, 1, 2} for KD = {1, 2, 4}
-  int rc = set_smem_once(reinterpret_cast<const void *>(herk_kernel<MODE, KD>), (int)smem,
-                         16 + 3 * MODE + (KD == 4 ? 2 : KD - 1));
+  // slots 16 + 3 * MODE + {0, 1, 2} for KD = {1, 2, 4}, 15 more for the table forms
+  const int slot = 16 + 3 * MODE + (KD == 4 ? 2 : KD - 1) + (table.n > 0 ? 15 : 0);
+  const void *fn = table.n > 0 ? reinterpret_cast<const void *>(herk_kernel<MODE, KD, true>)
+                               : reinterpret_cast<const void *>(herk_kernel<MODE, KD, false>);
+  int rc = set_smem_once(fn, (int)smem, slot);
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
-  herk_kernel<MODE, KD><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T, n_tiles,
-                                                         n_dev, n_host, kmul, Kcap, k_chunk, nsm, partials, status,
-                                                         g_wait_limit_ns.load(std::memory_order_relaxed), table);
+  const uint64_t wait_ns = g_wait_limit_ns.load(std::memory_order_relaxed);
+  if (table.n > 0)
+    herk_kernel<MODE, KD, true><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T,
+                                                                 n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm,
+                                                                 partials, status, wait_ns, table);
+  else
+    herk_kernel<MODE, KD, false><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T,
+                                                                  n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm,
+                                                                  partials, status, wait_ns, table);
   return check_launch("herk_kernel");
 }
 
