@@ -106,7 +106,7 @@ class VisServer:
         self.steps_per_turn = steps_per_turn
         #: False: results keep the latency and term count only (a long benchmark stream)
         self.keep_results = keep_results
-        #: kernel launches of the admitted jobs (engine.launches_per_run summed)
+        #: kernel launches made for the admitted jobs (shared product launches counted once)
         self.launches = 0
         #: jobs of at most this many (estimated) terms form the priority class
         self.small_job_terms = small_job_terms
@@ -208,7 +208,11 @@ class VisServer:
                     job.engine.allocate()
                     job.engine.upload()
                     job.engine.status.zero_()
-                self.launches += job.engine.launches_per_run()
+                eng = job.engine
+                self.launches += eng.launches_per_run()
+                if self.batch_products and eng.batchable:
+                    # its product launches are shared ones, counted as they are made
+                    self.launches -= len(eng.lsts) * eng.nchunks * -(-len(eng.freqs) // max(eng.fgroup, 1))
                 self._active.append(job)
         self.max_concurrent = max(self.max_concurrent, len(self._active))
 
@@ -277,6 +281,7 @@ class VisServer:
                 done = torch.cuda.Event()
                 done.record(bs)
                 self.batch_launches += 1
+                self.launches += 1
                 self.batched_groups += len(take)
                 for job, g, _ in take:
                     if self._reduce_and_step(job, g, done):
