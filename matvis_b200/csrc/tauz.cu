@@ -56,6 +56,14 @@ __device__ __forceinline__ void store_words(void *p, const uint32_t *w) {
     *reinterpret_cast<uint32_t *>(p) = w[0];
 }
 
+// One 32-byte store of 8 words (p 32-byte aligned): a whole L2 sector in one
+// instruction.
+__device__ __forceinline__ void store_sector(void *p, const uint32_t *w) {
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(w[0]), "r"(w[1]), "r"(w[2]),
+               "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+               : "memory");
+}
+
 // Writes NV consecutive real values of one component (c = 0 real, 1 imaginary)
 // as the P split terms into planes [2p + c] of a panel row, with vector stores:
 // NV = 4 or 8 values: 8- or 16-byte stores of bf16 / fp16 (inside one 16-byte
@@ -97,10 +105,21 @@ __device__ __forceinline__ void put_split(void *z, int64_t plane_stride, int64_t
       wlo[i] = __float_as_uint(lo[i]);
     }
     if constexpr (NV == 8) {
-      store_words<4>(p0, whi);
-      store_words<4>(p1, wlo);
-      store_words<4>(static_cast<float *>(z) + off2 + (int64_t)(0 + comp) * plane_stride, whi + 4);
-      store_words<4>(static_cast<float *>(z) + off2 + (int64_t)(2 + comp) * plane_stride, wlo + 4);
+      // values 0..3 and 4..7 fill the two 16-byte chunks of one 32-byte sector
+      // (the 64-byte swizzle keeps chunk pairs {0, 1} and {2, 3} together, in
+      // either order): one sector store per plane
+      const bool swapped = off2 < off;
+      const int64_t base = swapped ? off2 : off;
+      uint32_t shi[8], slo[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        shi[i] = swapped ? whi[4 + i] : whi[i];
+        shi[4 + i] = swapped ? whi[i] : whi[4 + i];
+        slo[i] = swapped ? wlo[4 + i] : wlo[i];
+        slo[4 + i] = swapped ? wlo[i] : wlo[4 + i];
+      }
+      store_sector(static_cast<float *>(z) + base + (int64_t)(0 + comp) * plane_stride, shi);
+      store_sector(static_cast<float *>(z) + base + (int64_t)(2 + comp) * plane_stride, slo);
     } else {
       store_words<NV>(p0, whi);
       store_words<NV>(p1, wlo);
