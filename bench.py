@@ -431,9 +431,15 @@ def herk_roofline(eng, args, dev) -> dict:
 
 
 def vecdot_roofline(eng, dev) -> dict:
-    """mvb_vecdot (+ its slice reduction) on the engine's last panel.  Algorithmic
-    bytes per launch: the Z rows of the antennas in the pair list read once
-    (F rows x K x 8 B each) plus the FP64 slice partials written and read."""
+    """The pair kernel (+ its slice reduction) on the engine's last panel.
+    Algorithmic bytes per launch: the Z rows of the antennas in the pair list
+    read once (F rows x K x 8 B each) plus the FP64 slice partials written and
+    read.  The staged kernel reads the panel from HBM once and runs from shared
+    memory, so its bound is the shared-memory load rate (F x 8 B per column for
+    a bundle's antenna i and for each of its 3 partners) and the FP32 pipe
+    (8 F^2 flops per pair and column):
+    both are reported against their nominal rates at the 1,965 MHz maximum SM
+    clock (148 SMs x 128 B / clock; 148 x 128 FMA / clock)."""
     import torch
 
     from matvis_b200 import _lib
@@ -457,16 +463,30 @@ def vecdot_roofline(eng, dev) -> dict:
     pairs = np.asarray(mp.antpairs)
     nrows = len(np.unique(pairs)) * eng.nfeed
     nsplit = -(-kvalid // mp.k_chunk)
-    algo_bytes = nrows * kvalid * 8.0 + 2 * nsplit * len(pairs) * eng.nfeed ** 2 * 16.0
+    staged = mp.kernel == "staged"
+    nslots = 3 * mp.nbundles if staged else len(pairs)  # pair steps computed, fillers included
+    algo_bytes = nrows * kvalid * 8.0 + 2 * nsplit * nslots * eng.nfeed ** 2 * 16.0
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved = algo_bytes / (ms / 1000.0) / 1e9
-    return {
+    name = "mvb_vecdot_staged" if staged else "mvb_vecdot"
+    line = {
         "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
         "peak_source": ("measured" if "hbm_gbs" in peaks else "fallback") + " HBM copy (MEASURED_PEAKS.json)",
-        "kernel": f"mvb_vecdot: {len(pairs)} pairs, F={eng.nfeed}, K={kvalid}, k_chunk={mp.k_chunk}",
+        "kernel": f"{name}: {len(pairs)} pairs, F={eng.nfeed}, K={kvalid}, k_chunk={mp.k_chunk}",
         "vecdot_ms": ms, "algorithmic_bytes_per_launch": algo_bytes,
     }
+    fp32_tflops = 8.0 * eng.nfeed ** 2 * len(pairs) * kvalid / (ms / 1000.0) / 1e12
+    nominal_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
+    line["fp32_tflops"] = fp32_tflops
+    line["fp32_frac_of_nominal"] = fp32_tflops / nominal_fp32
+    if staged:
+        smem_tbs = 4.0 * mp.nbundles * kvalid * eng.nfeed * 8 / (ms / 1000.0) / 1e12
+        line["bundles"] = mp.nbundles
+        line["bundle_fill"] = len(pairs) / (3.0 * mp.nbundles)
+        line["smem_load_tbs"] = smem_tbs
+        line["smem_frac_of_nominal"] = smem_tbs / (148 * 128 * 1.965e9 / 1e12)
+    return line
 
 
 # ----------------------------------------------------------------------------- B200 arm
@@ -543,7 +563,11 @@ def run_b200(args, rank, world, local_rank):
     kvalid = int(eng.n_above.item()) * eng.nax
     if eng.method == "VectorDot":
         dtype, kc = "f32", eng.matprod.k_chunk
-        product = ("complex64 Z, FP32 per-pair sums (mvb_vecdot), FP64 warp and slice sums")
+        if eng.matprod.kernel == "staged":
+            product = ("complex64 Z staged in shared memory, FP32 per-pair sums per 16-column stage "
+                       "(mvb_vecdot_staged), FP64 k-slice and slice sums")
+        else:
+            product = "complex64 Z, FP32 per-pair sums (mvb_vecdot), FP64 warp and slice sums"
     else:
         dtype = {"fp16x3": "fp16", "bf16x6": "bf16", "bf16x3": "bf16", "tf32x3": "tf32"}[args.gemm_mode]
         kc = eng.k_chunk
@@ -558,7 +582,7 @@ def run_b200(args, rank, world, local_rank):
         "data": f"synthetic (seeded; {sky}, HERA-350-like array, dipole-like beams)",
         "config": workload_config(args, cfg, desc, terms, counts),
         "implementation": {
-            "pair_kernel": eng.pair_kernel,
+            "pair_kernel": eng.pair_kernel if eng.method != "VectorDot" else f"vecdot ({eng.matprod.kernel})",
             "gemm_mode": None if eng.method == "VectorDot" else args.gemm_mode, "k_chunk": kc,
             "z_panel": "%.2f GB per slice" % (panel.data.numel() * panel.data.element_size() / 1e9 * kvalid /
                                               panel.Kcap),

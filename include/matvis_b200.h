@@ -312,6 +312,29 @@ size_t mvb_vecdot_ws_bytes(int64_t npairs, int nfeed, int64_t Kcap, int k_chunk)
 int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul, int nfeed,
                const int32_t *pairs, int64_t npairs, int k_chunk, void *ws, size_t ws_bytes, void *out, int out_c128,
                int accumulate, void *stream);
+/* Staged form of mvb_vecdot: the same output, with the panel read from HBM
+ * once.  Three steps: (1) mvb_vecdot_plan, host only, orders a HOST pair list
+ * into bundles of 8 int32 {i, j0, j1, j2, pair0, pair1, pair2, flip bits}: up
+ * to three pairs sharing antenna i (pair -1: a filler step; flip bit s: pair s
+ * is (ai, aj) = (j_s, i)).  plan_bytes from mvb_vecdot_plan_bytes; *nbundles
+ * receives the bundle count, a multiple of 32; MVB_ERR_ARG for an antenna
+ * outside [0, nant).  Done once per pair list, at the plugin's setup
+ * (MatProd.setup -> GPUVectorDot.allocate_vis, core/matprod.py:65,
+ * gpu/matprod.py:69-79).  (2) The caller copies the nbundles x 32 plan bytes to
+ * the device (16-byte aligned).  (3) mvb_vecdot_staged runs it: nant antennas
+ * (the panel's first nant * nfeed rows), npairs outputs, workspace of
+ * mvb_vecdot_staged_ws_bytes, k_chunk and Kcap multiples of 16, z 16-byte
+ * aligned.  mvb_vecdot_stage_columns gives the columns of one shared-memory
+ * stage (4, 8 or 16), 0 when nant * nfeed rows do not fit (then
+ * mvb_vecdot_staged returns MVB_ERR_UNSUPPORTED and mvb_vecdot applies). */
+size_t mvb_vecdot_plan_bytes(int64_t npairs, int nfeed);
+int mvb_vecdot_plan(const int32_t *pairs, int64_t npairs, int nant, int nfeed, void *plan, size_t plan_bytes,
+                    int64_t *nbundles);
+int mvb_vecdot_stage_columns(int nant, int nfeed);
+size_t mvb_vecdot_staged_ws_bytes(int64_t nbundles, int nfeed, int64_t Kcap, int k_chunk);
+int mvb_vecdot_staged(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul, int nfeed,
+                      int nant, const void *plan, int64_t nbundles, int64_t npairs, int k_chunk, void *ws,
+                      size_t ws_bytes, void *out, int out_c128, int accumulate, void *stream);
 
 /* ---- Polarised sky ------------------------------------------------------- */
 /* Frame rotation of the source coherency, per above-horizon source slot s < n

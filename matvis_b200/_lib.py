@@ -116,6 +116,15 @@ _SIGNATURES = {
         c_int,
         [_p, c_int64, _p, c_int64, c_int, c_int, _p, c_int64, c_int, _p, c_size_t, _p, c_int, c_int, _p],
     ),
+    "mvb_vecdot_plan_bytes": (c_size_t, [c_int64, c_int]),
+    "mvb_vecdot_plan": (c_int, [_p, c_int64, c_int, c_int, _p, c_size_t, _p]),
+    "mvb_vecdot_stage_columns": (c_int, [c_int, c_int]),
+    "mvb_vecdot_staged_ws_bytes": (c_size_t, [c_int64, c_int, c_int64, c_int]),
+    "mvb_vecdot_staged": (
+        c_int,
+        [_p, c_int64, _p, c_int64, c_int, c_int, c_int, _p, c_int64, c_int64, c_int, _p, c_size_t, _p, c_int, c_int,
+         _p],
+    ),
 }
 
 

@@ -3,8 +3,9 @@
 * :class:`B200MatMul` -- upper-triangle Hermitian product on the tcgen05 tensor
   cores (``mvb_herk`` + ``mvb_herk_reduce``); replaces CPUMatMul / GPUMatMul
   (cpu/matprod.py:8-32, gpu/matprod.py:10-63).
-* :class:`B200VectorDot` -- per-pair warp reduction (``mvb_vecdot``); replaces
-  CPUVectorDot / GPUVectorDot (cpu/matprod.py:35-53, gpu/matprod.py:66-98).
+* :class:`B200VectorDot` -- per-pair sums from shared-memory stages of the panel
+  (``mvb_vecdot_staged``; ``mvb_vecdot`` for arrays too large to stage);
+  replaces CPUVectorDot / GPUVectorDot (cpu/matprod.py:35-53, gpu/matprod.py:66-98).
 
 Output layout (npairs, nfeed, nfeed) with out[i, p, q] pairing feed q of ant1 with
 feed p of ant2, the reference's transposed feed convention (tests/test_matprod.py:57-65).
@@ -12,6 +13,7 @@ feed p of ant2, the reference's transposed feed convention (tests/test_matprod.p
 
 from __future__ import annotations
 
+import ctypes
 from abc import ABC, abstractmethod
 
 import numpy as np
@@ -288,24 +290,77 @@ class B200MatMul(MatProd):
         return out
 
 
-class B200VectorDot(MatProd):
-    """Per-pair source sums (warp reduction) for explicit pair lists."""
+def vecdot_plan(antpairs, nant: int, nfeed: int) -> np.ndarray:
+    """Bundles of the staged pair kernel for a host pair list (``mvb_vecdot_plan``):
+    int32 (nbundles, 8) rows {i, j0, j1, j2, pair0, pair1, pair2, flip bits},
+    nbundles a multiple of 32; pair -1 marks a filler step."""
+    pairs = np.ascontiguousarray(np.asarray(antpairs, dtype=np.int32).reshape(-1, 2))
+    npairs = len(pairs)
+    buf = np.zeros(max(int(_lib.lib.mvb_vecdot_plan_bytes(npairs, nfeed)), 32) // 4, dtype=np.int32)
+    nb = ctypes.c_int64(0)
+    check(_lib.lib.mvb_vecdot_plan(pairs.ctypes.data if npairs else None, npairs, int(nant), int(nfeed),
+                                   buf.ctypes.data, buf.nbytes, ctypes.byref(nb)))
+    return buf[: 8 * nb.value].reshape(-1, 8).copy()
 
-    def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, k_chunk: int = 4096, device=None):
+
+class B200VectorDot(MatProd):
+    """Per-pair source sums for explicit pair lists.
+
+    ``kernel="staged"`` (the default wherever the array's rows fit the
+    shared-memory stages, ``mvb_vecdot_stage_columns``): the panel is read from
+    HBM once and every pair runs from shared memory (``mvb_vecdot_staged``, pair
+    bundles planned once at :meth:`setup`); ``kernel="warp"``: one warp per (k-slice,
+    pair) reading both rows through L2 (``mvb_vecdot``)."""
+
+    def __init__(self, nchunks, nfeed, nant, antpairs, precision=1, k_chunk: int = 4096, device=None,
+                 kernel: str = "auto"):
         super().__init__(nchunks, nfeed, nant, antpairs, precision=precision, device=device)
+        if kernel not in ("auto", "staged", "warp"):
+            raise ValueError(f"kernel must be 'auto', 'staged' or 'warp', not {kernel!r}")
+        staged_ok = _lib.lib.mvb_vecdot_stage_columns(nant, nfeed) > 0
+        if kernel == "staged" and not staged_ok:
+            raise ValueError(f"{nant} x {nfeed} rows do not fit the staged kernel's shared memory")
+        self.kernel = "staged" if kernel in ("auto", "staged") and staged_ok else "warp"
         self.mode = _lib.Z_C64
         self.k_chunk = int(k_chunk)
+        if self.k_chunk % 16:
+            raise ValueError("k_chunk must be a multiple of 16")
         self._ws = None
+        self._plan_dev = None
+        self.nbundles = 0
+
+    def setup(self):
+        super().setup()
+        if self.kernel == "staged":
+            plan = vecdot_plan(self.antpairs, self.nant, self.nfeed)
+            self.nbundles = len(plan)
+            self._plan_dev = torch.as_tensor(plan, device=self.device)
 
     def enqueue(self, panel: ZPanel, out: torch.Tensor, accumulate: bool = False, stream=None):
-        nbytes = _lib.lib.mvb_vecdot_ws_bytes(self.npairs, self.nfeed, panel.Kcap, self.k_chunk)
+        c128 = 1 if out.dtype == torch.complex128 else 0
+        if self.kernel == "staged":
+            if self._plan_dev is None:
+                self.setup()
+            nbytes = _lib.lib.mvb_vecdot_staged_ws_bytes(self.nbundles, self.nfeed, panel.Kcap, self.k_chunk)
+        else:
+            nbytes = _lib.lib.mvb_vecdot_ws_bytes(self.npairs, self.nfeed, panel.Kcap, self.k_chunk)
         if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = None
             self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        if self.kernel == "staged":
+            check(
+                _lib.lib.mvb_vecdot_staged(
+                    ptr(panel.data), panel.Kcap, ptr(panel.n_dev), panel.n_host, panel.nax, self.nfeed, self.nant,
+                    ptr(self._plan_dev), self.nbundles, self.npairs, self.k_chunk, ptr(self._ws), self._ws.numel(),
+                    ptr(out), c128, int(accumulate), stream_handle(stream),
+                )
+            )
+            return
         check(
             _lib.lib.mvb_vecdot(
                 ptr(panel.data), panel.Kcap, ptr(panel.n_dev), panel.n_host, panel.nax, self.nfeed,
                 ptr(self._pairs_dev), self.npairs, self.k_chunk, ptr(self._ws), self._ws.numel(), ptr(out),
-                1 if out.dtype == torch.complex128 else 0, int(accumulate), stream_handle(stream),
+                c128, int(accumulate), stream_handle(stream),
             )
         )
 

@@ -283,6 +283,88 @@ def test_vectordot_random_vs_reference(device):
     np.testing.assert_allclose(out, ref, rtol=0, atol=1e-6 * np.abs(ref).max())
 
 
+def _pair_err(v, ref, z, nant, nfeed, pairs):
+    """max |dV| / sqrt(|V_jj^pp| |V_ii^qq|) for out[i, p, q] of pair (ai, aj) = (i, j)."""
+    zz = z.reshape(nant, nfeed, -1)
+    auto = (np.abs(zz) ** 2).sum(-1)
+    den = np.sqrt(auto[pairs[:, 1]][:, :, None] * auto[pairs[:, 0]][:, None, :])
+    return float(np.max(np.abs(np.asarray(v) - ref) / den)) if len(pairs) else 0.0
+
+
+# nant x nfeed rows staged 16 (700, 37, 14, 3 rows), 8 (1000 rows) and 4 (2000, 1600 rows) columns at a
+# time; odd K ends on a single column
+@pytest.mark.parametrize("nant,nfeed,K,k_chunk,npairs", [(350, 2, 40000, 4096, 5000), (37, 1, 3001, 1024, 63),
+                                                         (7, 2, 555, 64, 40), (3, 1, 100, 16, 5),
+                                                         (1000, 1, 1501, 512, 2500), (1000, 2, 2048, 512, 3000),
+                                                         (1600, 1, 999, 256, 2000)])
+def test_vectordot_staged_vs_oracle(device, nant, nfeed, K, k_chunk, npairs):
+    """Both pair kernels against the FP64 oracle (<= 1e-6 normalised), with
+    autocorrelations (real one-feed autos) and a repeated pair in the list."""
+    rng = np.random.default_rng(nant + K)
+    pairs = rng.integers(0, nant, size=(npairs, 2))
+    pairs[0] = (0, 0)
+    pairs[-1] = pairs[len(pairs) // 2]
+    M = nant * nfeed
+    z = (rng.normal(size=(M, K)) + 1j * rng.normal(size=(M, K))) * rng.lognormal(0, 1, K)[None, :]
+    ref = orc.vectordot_vis(z.astype(np.complex64).astype(np.complex128), nant, nfeed, pairs)
+    outs = {}
+    for kernel in ("staged", "warp"):
+        mp = mv.B200VectorDot(nchunks=1, nfeed=nfeed, nant=nant, antpairs=pairs, precision=2, k_chunk=k_chunk,
+                              kernel=kernel)
+        mp.setup()
+        assert mp.kernel == kernel
+        out = torch.zeros((npairs, nfeed, nfeed), dtype=torch.complex128, device=DEV)
+        mp(z, 0)
+        mp.sum_chunks(out)
+        o = outs[kernel] = out.cpu().numpy()
+        err = _pair_err(o, ref, z, nant, nfeed, pairs)
+        assert err <= 1e-6, f"{kernel}: normalised error {err:.3e}"
+        autos = pairs[:, 0] == pairs[:, 1]
+        for f in range(nfeed):
+            assert (o[autos, f, f].imag == 0).all()
+    # a repeated pair may sit in slots of either orientation: equal to rounding
+    np.testing.assert_allclose(outs["staged"][-1], outs["staged"][len(pairs) // 2], rtol=1e-6)
+
+
+def test_vectordot_staged_accumulate_complex64_and_fallback(device):
+    rng = np.random.default_rng(5)
+    nant, nfeed, K = 50, 2, 5000
+    pairs = rng.integers(0, nant, size=(300, 2))
+    z = rng.normal(size=(nant * nfeed, K)) + 1j * rng.normal(size=(nant * nfeed, K))
+    mp = mv.B200VectorDot(nchunks=1, nfeed=nfeed, nant=nant, antpairs=pairs, precision=1, k_chunk=1024)
+    mp.setup()
+    assert mp.kernel == "staged"
+    panel = mp._as_panel(z, mp.mode)
+    out = torch.zeros((300, nfeed, nfeed), dtype=torch.complex64, device=DEV)
+    mp.enqueue(panel, out)
+    mp.enqueue(panel, out, accumulate=True)
+    torch.cuda.synchronize()
+    ref = orc.vectordot_vis(z.astype(np.complex64).astype(np.complex128), nant, nfeed, pairs)
+    assert _pair_err(out.cpu().numpy().astype(np.complex128) / 2, ref, z, nant, nfeed, pairs) <= 1e-6
+    # rows that do not fit two shared-memory stages: the warp kernel, or an error when asked for staging
+    assert mv.B200VectorDot(1, 2, 4000, np.array([[0, 1]]), kernel="auto").kernel == "warp"
+    with pytest.raises(ValueError, match="shared memory"):
+        mv.B200VectorDot(1, 2, 4000, np.array([[0, 1]]), kernel="staged")
+
+
+def test_vectordot_staged_positive_sums(device):
+    """All-positive terms over a long K (autocorrelation-like): FP32 sums over one
+    16-column stage, FP64 beyond, so the relative error stays near 1e-7."""
+    rng = np.random.default_rng(2)
+    nant, K = 40, 300000
+    z = rng.uniform(0.5, 1.5, size=(nant, K)) * np.exp(1j * 0.01 * rng.normal(size=(nant, K)))
+    pairs = np.column_stack([np.arange(nant), (np.arange(nant) + 1) % nant])
+    pairs = np.concatenate([pairs, np.column_stack([np.arange(nant)] * 2)])
+    mp = mv.B200VectorDot(nchunks=1, nfeed=1, nant=nant, antpairs=pairs, precision=2, k_chunk=16384)
+    mp.setup()
+    out = torch.zeros((len(pairs), 1, 1), dtype=torch.complex128, device=DEV)
+    mp(z, 0)
+    mp.sum_chunks(out)
+    ref = orc.vectordot_vis(z.astype(np.complex64).astype(np.complex128), nant, 1, pairs)
+    rel = np.abs(out.cpu().numpy() - ref) / np.abs(ref)
+    assert rel.max() <= 1e-6, rel.max()
+
+
 @pytest.mark.parametrize("mode", ["bf16x6", "fp16x3"])
 @pytest.mark.parametrize("k_chunk", [512, 2048, 8192])
 def test_herk_accumulation_positive_sums(device, k_chunk, mode):
