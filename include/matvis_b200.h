@@ -323,9 +323,12 @@ int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host
  * gpu/matprod.py:69-79).  (2) The caller copies the nbundles x 32 plan bytes to
  * the device (16-byte aligned).  (3) mvb_vecdot_staged runs it: nant antennas
  * (the panel's first nant * nfeed rows), npairs outputs, workspace of
- * mvb_vecdot_staged_ws_bytes, k_chunk and Kcap multiples of 16, z 16-byte
- * aligned.  mvb_vecdot_stage_columns gives the columns of one shared-memory
- * stage (4, 8 or 16), 0 when nant * nfeed rows do not fit (then
+ * mvb_vecdot_staged_ws_bytes, k_chunk (the longest k-slice; the kernel picks
+ * the slices that fill whole waves of SMs) and Kcap multiples of 16, z 16-byte
+ * aligned.  The panel is staged by bulk-tensor copies; every wait is bounded
+ * (2 s), and one that runs out sets MVB_DEV_TIMEOUT in *status (if not NULL)
+ * and ends the kernel.  mvb_vecdot_stage_columns gives the columns of one
+ * shared-memory stage (4, 8 or 16), 0 when nant * nfeed rows do not fit (then
  * mvb_vecdot_staged returns MVB_ERR_UNSUPPORTED and mvb_vecdot applies). */
 size_t mvb_vecdot_plan_bytes(int64_t npairs, int nfeed);
 int mvb_vecdot_plan(const int32_t *pairs, int64_t npairs, int nant, int nfeed, void *plan, size_t plan_bytes,
@@ -334,7 +337,7 @@ int mvb_vecdot_stage_columns(int nant, int nfeed);
 size_t mvb_vecdot_staged_ws_bytes(int64_t nbundles, int nfeed, int64_t Kcap, int k_chunk);
 int mvb_vecdot_staged(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host, int kmul, int nfeed,
                       int nant, const void *plan, int64_t nbundles, int64_t npairs, int k_chunk, void *ws,
-                      size_t ws_bytes, void *out, int out_c128, int accumulate, void *stream);
+                      size_t ws_bytes, void *out, int out_c128, int accumulate, int32_t *status, void *stream);
 
 /* ---- Polarised sky ------------------------------------------------------- */
 /* Frame rotation of the source coherency, per above-horizon source slot s < n

@@ -123,7 +123,7 @@ _SIGNATURES = {
     "mvb_vecdot_staged": (
         c_int,
         [_p, c_int64, _p, c_int64, c_int, c_int, c_int, _p, c_int64, c_int64, c_int, _p, c_size_t, _p, c_int, c_int,
-         _p],
+         _p, _p],
     ),
 }
 

@@ -378,10 +378,16 @@ __global__ void __launch_bounds__(kTauZThreads)
         if (!write) continue;
         const int64_t m = (int64_t)a * F + f;
         if constexpr (MODE == MVB_Z_C64) {
+          // the row's kTauZSrc * X values start 32-byte aligned (Kcap a multiple
+          // of 64, s0 X of 4): whole 32-byte sectors, four values each
           float2 *zp = static_cast<float2 *>(z) + m * Kcap + s0 * X;
 #pragma unroll
-          for (int i = 0; i < kTauZSrc * X; i += 2)
-            *reinterpret_cast<float4 *>(zp + i) = make_float4(vr[i], vi[i], vr[i + 1], vi[i + 1]);
+          for (int i = 0; i < kTauZSrc * X; i += 4) {
+            const uint32_t w[8] = {__float_as_uint(vr[i]),     __float_as_uint(vi[i]),     __float_as_uint(vr[i + 1]),
+                                   __float_as_uint(vi[i + 1]), __float_as_uint(vr[i + 2]), __float_as_uint(vi[i + 2]),
+                                   __float_as_uint(vr[i + 3]), __float_as_uint(vi[i + 3])};
+            store_sector(zp + i, w);
+          }
         } else {
           // kTauZSrc * X consecutive k from a multiple of kTauZSrc * X: inside one k-block
           constexpr int KB = kKBlockBytes / (MODE == MVB_GEMM_TF32_3 ? 4 : 2);

@@ -38,11 +38,14 @@ def choose_k_chunk(n_tiles: int, kvalid: int, num_sms: int = 148, lo: int = 1024
     return int(min(max(kc, lo), hi))
 
 
-#: Per-column costs measured on one B200 on a config-3 slice (K = 1.0e6 columns):
-#: mvb_vecdot took 11.83 ms for 5,000 pairs at F = 2, i.e. 5.9e-13 s per
-#: (pair x F^2 x column); mvb_herk in fp16x3 took 6.51 ms for 21 tiles of
-#: 128 x 128, i.e. 1.03e-10 s per (tile x split product x column), with TF32
-#: operands at half that rate.  Break-even at F = 2, 21 tiles: ~2,750 pairs.
+#: Per-column costs measured on one B200 on a config-3 slice (K = 1.0e6 columns,
+#: the seeded 5,000 pairs at F = 2): mvb_vecdot_staged took 5.64 ms, i.e.
+#: 2.8e-13 s per (pair x F^2 x column), mvb_vecdot (one warp per pair, for
+#: arrays too large to stage) 11.83 ms, 5.9e-13 s; mvb_herk in fp16x3 took
+#: 6.51 ms for 21 tiles of 128 x 128, i.e. 1.03e-10 s per (tile x split product
+#: x column), with TF32 operands at half that rate.  Break-even at F = 2, 21
+#: tiles: ~5,750 pairs (staged).
+VECDOT_STAGED_S_PER_PAIR_COL = 2.8e-13
 VECDOT_S_PER_PAIR_COL = 5.9e-13
 HERK_S_PER_TILE_PRODUCT_COL = 1.03e-10
 
@@ -52,19 +55,23 @@ def pair_product(nant: int, nfeed: int, npairs: int, gemm_mode="fp16x3") -> str:
 
     Returns ``"herk"`` when the tensor-core Hermitian product over all pairs
     followed by a gather of the listed pairs (mvb_herk + mvb_herk_reduce with a
-    pair list) is predicted faster than per-pair sums (mvb_vecdot), else
-    ``"vecdot"``.  Both give the reference's VectorDot output
+    pair list) is predicted faster than per-pair sums (mvb_vecdot_staged, or
+    mvb_vecdot where the array's rows do not fit its shared-memory stages),
+    else ``"vecdot"``.  Both give the reference's VectorDot output
     out[i, p, q] = sum_k Z[aj F + p, k] conj(Z[ai F + q, k]) (cpu/matprod.py:48-51);
     the per-column cost of each kernel is the measured one above, so the choice
-    does not depend on the source count.  Random lists above a few thousand
-    pairs of a 350-antenna array go to the Hermitian product; short lists
-    (redundant-baseline sets) stay on per-pair sums.
+    does not depend on the source count.  Lists above ~5,750 pairs of a
+    350-antenna two-feed array go to the Hermitian product; shorter ones
+    (redundant-baseline sets of compact arrays, sparse pair selections) stay on
+    per-pair sums.
     """
     T = -(-int(nant) * int(nfeed) // _lib.TILE)
     mode = _lib.GEMM_MODES[gemm_mode] if isinstance(gemm_mode, str) else int(gemm_mode)
     rate = 2.0 if mode == _lib.GEMM_TF32_3 else 1.0
     herk = T * (T + 1) // 2 * _lib.GEMM_PRODUCTS[mode] * rate * HERK_S_PER_TILE_PRODUCT_COL
-    vecdot = int(npairs) * int(nfeed) ** 2 * VECDOT_S_PER_PAIR_COL
+    per = VECDOT_STAGED_S_PER_PAIR_COL if _lib.lib.mvb_vecdot_stage_columns(int(nant), int(nfeed)) > 0 \
+        else VECDOT_S_PER_PAIR_COL
+    vecdot = int(npairs) * int(nfeed) ** 2 * per
     return "herk" if herk < vecdot else "vecdot"
 
 
@@ -352,7 +359,7 @@ class B200VectorDot(MatProd):
                 _lib.lib.mvb_vecdot_staged(
                     ptr(panel.data), panel.Kcap, ptr(panel.n_dev), panel.n_host, panel.nax, self.nfeed, self.nant,
                     ptr(self._plan_dev), self.nbundles, self.npairs, self.k_chunk, ptr(self._ws), self._ws.numel(),
-                    ptr(out), c128, int(accumulate), stream_handle(stream),
+                    ptr(out), c128, int(accumulate), ptr(self.status), stream_handle(stream),
                 )
             )
             return

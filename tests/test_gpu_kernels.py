@@ -291,8 +291,8 @@ def _pair_err(v, ref, z, nant, nfeed, pairs):
     return float(np.max(np.abs(np.asarray(v) - ref) / den)) if len(pairs) else 0.0
 
 
-# nant x nfeed rows staged 16 (700, 37, 14, 3 rows), 8 (1000 rows) and 4 (2000, 1600 rows) columns at a
-# time; odd K ends on a single column
+# nant x nfeed rows staged 16 (700, 37, 14, 3 rows), 8 (1000, 1600 rows) and 4 (2000 rows) columns at
+# a time; odd K ends on a single column
 @pytest.mark.parametrize("nant,nfeed,K,k_chunk,npairs", [(350, 2, 40000, 4096, 5000), (37, 1, 3001, 1024, 63),
                                                          (7, 2, 555, 64, 40), (3, 1, 100, 16, 5),
                                                          (1000, 1, 1501, 512, 2500), (1000, 2, 2048, 512, 3000),

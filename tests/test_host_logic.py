@@ -65,16 +65,21 @@ def test_matprod_names():
 
 
 def test_pair_product_cost_model():
-    """Measured break-even of the per-pair kernel against the Hermitian product
-    with a pair gather: ~2,750 pairs for 350 two-feed antennas (21 tiles)."""
-    assert pair_product(350, 2, 5000) == "herk"
-    assert pair_product(350, 2, 2000) == "vecdot"
+    """Measured break-even of the staged per-pair kernel against the Hermitian
+    product with a pair gather: ~5,750 pairs for 350 two-feed antennas (21
+    tiles); ~2,750 for arrays too large to stage (the warp kernel)."""
+    assert pair_product(350, 2, 5000) == "vecdot"
+    assert pair_product(350, 2, 7000) == "herk"
+    assert pair_product(350, 2, 10649) == "herk"  # the redundant-baseline list of the 350-antenna array
     assert pair_product(350, 2, 350 * 351 // 2) == "herk"
     assert pair_product(37, 1, 63) == "vecdot"  # redundant-baseline representatives of a 37-element hexagon
     # TF32 operands and six split products double the product's cost
-    assert pair_product(350, 2, 5000, "tf32x3") == "vecdot"
-    assert pair_product(350, 2, 5000, "bf16x6") == "vecdot"
+    assert pair_product(350, 2, 10000, "tf32x3") == "vecdot"
+    assert pair_product(350, 2, 10000, "bf16x6") == "vecdot"
     assert pair_product(350, 2, 12000, "bf16x6") == "herk"
+    # 4,000 two-feed antennas do not fit the stages: 2,016 tiles against the warp kernel (~264,000 pairs)
+    assert pair_product(4000, 2, 200000) == "vecdot"
+    assert pair_product(4000, 2, 300000) == "herk"
 
 
 def test_resolve_product():
@@ -85,9 +90,9 @@ def test_resolve_product():
 
     pairs = np.stack(np.triu_indices(350, 1), axis=1)
     assert _resolve_product(spec()) == ("MatMul", None)
-    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:5000])) == ("MatMul", "herk")
+    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:8000])) == ("MatMul", "herk")
     assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:500])) == ("VectorDot", "vecdot")
-    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:5000], pair_product="vecdot")) == \
+    assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:8000], pair_product="vecdot")) == \
         ("VectorDot", "vecdot")
     assert _resolve_product(spec(matprod="VectorDot", antpairs=pairs[:50], pair_product="herk")) == \
         ("MatMul", "herk")

@@ -115,12 +115,15 @@ def test_plan_empty_and_errors():
 
 
 def test_stage_columns_and_workspace():
+    # the widest stage of which two fit in shared memory; none past ~2,400 rows
     assert _lib.lib.mvb_vecdot_stage_columns(350, 2) == 16
-    assert _lib.lib.mvb_vecdot_stage_columns(1000, 2) == 4
-    assert _lib.lib.mvb_vecdot_stage_columns(1600, 1) == 4
+    assert _lib.lib.mvb_vecdot_stage_columns(37, 1) == 16
     assert _lib.lib.mvb_vecdot_stage_columns(1000, 1) == 8
+    assert _lib.lib.mvb_vecdot_stage_columns(1600, 1) == 8
+    assert _lib.lib.mvb_vecdot_stage_columns(1000, 2) == 4
     assert _lib.lib.mvb_vecdot_stage_columns(4000, 2) == 0
     assert _lib.lib.mvb_vecdot_stage_columns(0, 2) == 0
-    assert _lib.lib.mvb_vecdot_staged_ws_bytes(64, 2, 4096, 1024) == 4 * 64 * 3 * 8 * 8
-    rc = _lib.lib.mvb_vecdot_staged(None, 0, None, 0, 1, 2, 10, None, 0, 0, 16, None, 0, None, 0, 0, None)
+    # up to 31 k-slices beyond ceil(Kcap / min(k_chunk, 1024))
+    assert _lib.lib.mvb_vecdot_staged_ws_bytes(64, 2, 4096, 4096) == (4 + 31) * 64 * 3 * 8 * 8
+    rc = _lib.lib.mvb_vecdot_staged(None, 0, None, 0, 1, 2, 10, None, 0, 0, 16, None, 0, None, 0, 0, None, None)
     assert rc == _lib.MVB_ERR_ARG
