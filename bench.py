@@ -94,6 +94,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-nsrc-max", type=int, default=500_000)
     ap.add_argument("--serve-max-active", type=int, default=32)
+    ap.add_argument("--serve-turns-ahead", type=int, default=2,
+                    help="served form: turns enqueued ahead of the GPU (0: no bound)")
     ap.add_argument("--serve-small-terms", type=float, default=2e11,
                     help="jobs of at most this many terms are the server's priority class (0: none)")
     return ap.parse_args()
@@ -727,10 +729,13 @@ def run_serve(args, local_rank):
     _, first = next(wl.config5_stream(njobs=1, rate_hz=args.serve_rate, nsrc_max=args.serve_nsrc_max))
     first.gemm_mode = args.gemm_mode
     small = args.serve_small_terms or None
-    warm = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False, small_job_terms=small)
+    ahead = args.serve_turns_ahead or None
+    warm = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False, small_job_terms=small,
+                     turns_ahead=ahead)
     warm.serve_stream([(0.0, first)])  # kernel warm-up, not timed
     warm.close()
-    srv = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False, small_job_terms=small)
+    srv = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False, small_job_terms=small,
+                    turns_ahead=ahead)
     hits0, miss0 = devcache.CACHE.hits, devcache.CACHE.misses
     t0 = time.perf_counter()
     srv.serve_stream(stream())
@@ -747,7 +752,7 @@ def run_serve(args, local_rank):
         "config": {"workload": f"config5 stream: {args.serve_jobs} jobs, Poisson {args.serve_rate}/s, Nant log-U[16,512], "
                                f"Nsrc log-U[1e3,{args.serve_nsrc_max}], Nf U{{1..32}}, Nt U{{1..16}}, Gaussian or "
                                f"polarised grid beam", "gemm_mode": args.gemm_mode,
-                   "max_active": args.serve_max_active, "small_job_terms": small,
+                   "max_active": args.serve_max_active, "small_job_terms": small, "turns_ahead": ahead,
                    "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS")},
     }
     print(json.dumps(line), flush=True)

@@ -8,7 +8,9 @@ Jobs (``JobSpec``) arrive at any time.  The server
 * keeps every admitted job's sky, beams, Z panel and partial visibilities
   resident on the device, and gives it its own CUDA stream;
 * advances the active jobs round robin, so their kernels overlap on the
-  device: each turn, every job's next group of frequencies gets its tau/Z on
+  device, with at most ``turns_ahead`` turns enqueued ahead of the GPU (so a
+  job admitted now starts behind a bounded backlog): each turn, every job's
+  next group of frequencies gets its tau/Z on
   the job's stream, and the Hermitian products of all those groups run in one
   launch (``mvb_herk_batch``, up to 32 panels) on a shared stream, ordered
   against the jobs' streams by events; each job then reduces its own group
@@ -91,7 +93,7 @@ class VisServer:
 
     def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 32, steps_per_turn: int = 1,
                  reserve_fraction: float = 0.5, keep_results: bool = True, small_job_terms: float | None = 2e11,
-                 batch_products: bool = True):
+                 batch_products: bool = True, turns_ahead: int | None = 2):
         self.device = _lib.require_cuda(device)
         free = torch.cuda.mem_get_info(self.device)[0]
         self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
@@ -104,6 +106,12 @@ class VisServer:
             del reserve
         self.max_active = max_active
         self.steps_per_turn = steps_per_turn
+        #: turns enqueued on the device and not yet complete before the server
+        #: waits to enqueue another (None: no bound).  Without a bound the host
+        #: runs ahead of the GPU and a newly admitted job's first kernels queue
+        #: behind every turn already enqueued for the others.
+        self.turns_ahead = turns_ahead
+        self._turns: deque[list] = deque()
         #: False: results keep the latency and term count only (a long benchmark stream)
         self.keep_results = keep_results
         #: kernel launches made for the admitted jobs (shared product launches counted once)
@@ -216,7 +224,18 @@ class VisServer:
                 self._active.append(job)
         self.max_concurrent = max(self.max_concurrent, len(self._active))
 
+    def _throttled(self) -> bool:
+        """True while turns_ahead turns are enqueued and not yet complete."""
+        if self.turns_ahead is None:
+            return False
+        while self._turns and all(e.query() for e in self._turns[0]):
+            self._turns.popleft()
+        return len(self._turns) >= self.turns_ahead
+
     def _advance(self):
+        if self._throttled():
+            return
+        self._turn: list = []  # events that complete this turn's work
         still = []
         batch = []
         for job in self._active:
@@ -242,11 +261,16 @@ class VisServer:
                         break
                     eng.enqueue_time(job.next_t, stream=job.stream)
                     job.next_t += 1
+                step_done = torch.cuda.Event()
+                step_done.record(job.stream)
+                self._turn.append(step_done)
                 if job.next_t >= nt:
                     self._finish(job)
                     continue
             still.append(job)
         self._active = still + (self._launch_batches(batch) if batch else [])
+        if self._turn:
+            self._turns.append(self._turn)
 
     def _finish(self, job: _Job):
         """The job's last kernel is enqueued: hand it to the copier."""
@@ -280,6 +304,7 @@ class VisServer:
                                                    _lib.stream_handle(bs)))
                 done = torch.cuda.Event()
                 done.record(bs)
+                self._turn.append(done)
                 self.batch_launches += 1
                 self.launches += 1
                 self.batched_groups += len(take)
@@ -356,7 +381,7 @@ class VisServer:
         t0 = time.perf_counter()
         while not self.idle():
             self.poll()
-            if not self._active and self._finishing:
+            if (not self._active and self._finishing) or self._throttled():
                 time.sleep(0.0005)
             if time.perf_counter() - t0 > timeout_s:
                 raise TimeoutError("server did not drain in time")
@@ -381,8 +406,8 @@ class VisServer:
                 time.sleep(min(0.001, max(0.0, nxt[0] - now)))
                 continue
             self.poll()
-            if not self._active and self._finishing and not self._pending:
-                time.sleep(0.0002)  # only copies in flight: leave the interpreter to the copier
+            if (not self._active and self._finishing and not self._pending) or self._throttled():
+                time.sleep(0.0002)  # copies or enqueued turns in flight: leave the interpreter to the copier
             if time.perf_counter() - t0 > timeout_s:
                 raise TimeoutError("serve_stream did not finish in time")
         return ids
