@@ -749,6 +749,9 @@ def run_serve(args, local_rank):
         "arrival_span_s": arrivals[0], "max_concurrent": srv.max_concurrent, "peak_hbm_gb": srv.peak_in_use / 1e9,
         "launches_per_job": srv.launches / max(summ["jobs"] + summ.get("errors", 0), 1),
         "device_cache": {"hits": devcache.CACHE.hits - hits0, "misses": devcache.CACHE.misses - miss0},
+        "allocator": {k: torch.cuda.memory_stats(dev).get(k) for k in ("num_alloc_retries", "num_device_alloc",
+                                                                      "num_device_free")},
+        "alloc_conf": os.environ.get("PYTORCH_CUDA_ALLOC_CONF"),
         "config": {"workload": f"config5 stream: {args.serve_jobs} jobs, Poisson {args.serve_rate}/s, Nant log-U[16,512], "
                                f"Nsrc log-U[1e3,{args.serve_nsrc_max}], Nf U{{1..32}}, Nt U{{1..16}}, Gaussian or "
                                f"polarised grid beam", "gemm_mode": args.gemm_mode,

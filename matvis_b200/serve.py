@@ -121,6 +121,13 @@ class VisServer:
         self._small: deque[_Job] = deque()
         #: run the products of the active jobs' current frequency groups in shared launches
         self.batch_products = batch_products
+        # every admitted job's buffers are allocated on this one stream, so the
+        # caching allocator hands a finished job's blocks to the next job (blocks
+        # are cached per allocating stream; a fresh stream per job would strand
+        # them, until an out-of-memory retry frees the whole cache with a device
+        # synchronisation).  A job's buffers are freed only after its last
+        # kernel has completed, so any stream may reuse them.
+        self._alloc_stream = torch.cuda.Stream(device=self.device)
         self._batch_streams = {False: torch.cuda.Stream(device=self.device),
                                True: torch.cuda.Stream(device=self.device, priority=-1)}
         #: product launches (mvb_herk_batch) and the panel groups they carried
@@ -211,9 +218,11 @@ class VisServer:
                 self.peak_in_use = max(self.peak_in_use, self.in_use)
                 job.t_admit = time.perf_counter()
                 job.stream = torch.cuda.Stream(device=self.device, priority=-1 if job.small else 0)
-                with torch.cuda.stream(job.stream):
+                with torch.cuda.stream(self._alloc_stream):
                     job.engine = VisEngine(job.spec, device=self.device)
                     job.engine.allocate()
+                job.stream.wait_stream(self._alloc_stream)  # the buffers' zero fills
+                with torch.cuda.stream(job.stream):
                     job.engine.upload()
                     job.engine.status.zero_()
                 eng = job.engine
