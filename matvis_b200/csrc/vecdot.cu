@@ -478,8 +478,11 @@ extern "C" int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int
 
 extern "C" size_t mvb_vecdot_plan_bytes(int64_t npairs, int nfeed) {
   if (npairs < 0 || (nfeed != 1 && nfeed != 2)) return 0;
-  // every phase of 8 bundles places at least one pair; fillers complete warps
-  return (size_t)(kVdClasses * npairs + 32) * kVdBundleInts * sizeof(int32_t);
+  // each step of a phase places at least one pair (the lane holding the antenna
+  // with the most pairs left always has a partner class), so a phase of 8
+  // bundles places 3 while 3 are left: at most npairs / 3 + 1 phases, plus
+  // fillers to whole warps
+  return (size_t)(kVdClasses * (npairs / kVdSteps + 2) + 32) * kVdBundleInts * sizeof(int32_t);
 }
 
 namespace {

@@ -98,6 +98,12 @@ def test_plan_duplicates_autos_and_one_class():
     pairs = np.array([[0, 8], [8, 16], [16, 0], [0, 0], [8, 8], [0, 8], [0, 8]])
     plan = vecdot_plan(pairs, 24, 2)
     _check_structure(plan, pairs, 24)
+    # the worst case for the plan's size: one antenna pair repeated (one lane per step)
+    for n in (1, 2, 3, 4, 299, 300, 301):
+        pairs = np.tile([[0, 8]], (n, 1))
+        plan = vecdot_plan(pairs, 16, 2)
+        _check_structure(plan, pairs, 16)
+        assert len(plan) <= 8 * (n // 3 + 2) + 24
 
 
 def test_plan_empty_and_errors():
