@@ -171,9 +171,10 @@ __device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *m
 // nbox bulk-tensor loads of box_rows rows x kb columns (8 kb bytes, swizzled in
 // 16-byte units by the 8 kb-byte swizzle mode) complete on the stage's full
 // barrier; each compute warp releases a stage on its empty barrier.  In the
-// swizzled layout the 16-byte unit u of row r sits in bank group
-// (r + (u ^ swz(r))) mod 8 when rows are 128 bytes (and likewise for 64 and 32),
-// so 8 rows of distinct residues mod 8 never share a bank group.  A thread
+// swizzled layout the 16-byte unit u of a 128-byte row r sits in bank group
+// u ^ (r mod 8) (64- and 32-byte rows share a 128-byte line two or four to a
+// line, with the XOR taken from the line index), so 8 rows of distinct residues
+// mod 8 never share a bank group.  A thread
 // loads 16 bytes = two columns of one row.  For F = 2 the rows of antenna a are
 // 2a and 2a + 1; the thread reads row 2a + ba first (ba = bit 2 of a), then
 // row 2a + 1 - ba: 8 antennas of distinct residues mod 8 give rows of distinct
