@@ -288,11 +288,11 @@ int mvb_herk_reduce_grouped(const void *ws, size_t ws_bytes, int ngroup, int64_t
                             const int32_t *pairs, int64_t npairs, void *out, size_t out_stride, int out_c128,
                             double vscale, int accumulate, void *stream);
 /* Wall-time limit, in nanoseconds, of each pipeline wait inside mvb_herk
- * (process-wide; 0 restores the default of 4 s).  Returns the previous limit.
- * A wait that runs out sets MVB_DEV_TIMEOUT in the status word; the kernel then
- * stops issuing work, waits (at most 0.2 s) for the copies and tensor-core
- * operations it issued, releases its tensor memory and returns, so the context
- * stays usable.  For failure-detection tests and diagnostics: a limit shorter
+ * (and its grouped and batched forms) and mvb_vecdot_staged (process-wide; 0
+ * restores the default of 4 s).  Returns the previous limit.  A wait that runs
+ * out sets MVB_DEV_TIMEOUT in the status word; the kernel then stops issuing
+ * work, waits (at most 0.2 s) for the copies and tensor-core operations it
+ * issued, releases its tensor memory and returns, so the context stays usable.  For failure-detection tests and diagnostics: a limit shorter
  * than a normal wait makes products fail.  No counterpart in the reference,
  * whose device waits are unbounded (gpu/gpu.py:249). */
 uint64_t mvb_set_wait_limit_ns(uint64_t limit_ns);
@@ -326,8 +326,8 @@ int mvb_vecdot(const void *z, int64_t Kcap, const int32_t *n_dev, int64_t n_host
  * mvb_vecdot_staged_ws_bytes, k_chunk (the longest k-slice; the kernel picks
  * the slices that fill whole waves of SMs) and Kcap multiples of 16, z 16-byte
  * aligned.  The panel is staged by bulk-tensor copies; every wait is bounded
- * (2 s), and one that runs out sets MVB_DEV_TIMEOUT in *status (if not NULL)
- * and ends the kernel.  mvb_vecdot_stage_columns gives the columns of one
+ * (mvb_set_wait_limit_ns), and one that runs out sets MVB_DEV_TIMEOUT in
+ * *status (if not NULL) and ends the kernel.  mvb_vecdot_stage_columns gives the columns of one
  * shared-memory stage (4, 8 or 16), 0 when nant * nfeed rows do not fit (then
  * mvb_vecdot_staged returns MVB_ERR_UNSUPPORTED and mvb_vecdot applies). */
 size_t mvb_vecdot_plan_bytes(int64_t npairs, int nfeed);

@@ -45,6 +45,9 @@ int num_sms();
 // slots 10 and 11 are the beam kernels, 16..45 the Hermitian-product variants,
 // 48 and 49 the staged pair kernels.
 int set_smem_once(const void *fn, int bytes, int slot);
+// Wall-time limit of a pipeline wait in the product and the staged pair kernel
+// (process-wide, set by mvb_set_wait_limit_ns; 4 s by default).
+uint64_t wait_limit_ns();
 
 // Columns of a Z panel are zero-filled up to a multiple of this.
 constexpr int kKAlign = 64;

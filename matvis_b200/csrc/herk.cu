@@ -696,6 +696,7 @@ int set_smem_once(const void *fn, int bytes, int slot) {
 // Wall-time limit of the product's pipeline waits, process-wide (see
 // mvb_set_wait_limit_ns); read at each launch.
 static std::atomic<uint64_t> g_wait_limit_ns{kWaitLimitNs};
+uint64_t wait_limit_ns() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
 
 // table.n > 0: the units come from the table (z, ngroup, shape and status arguments unused).
 template <int MODE, int KD>
@@ -723,7 +724,7 @@ static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad,
   int rc = set_smem_once(fn, (int)smem, slot);
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
-  const uint64_t wait_ns = g_wait_limit_ns.load(std::memory_order_relaxed);
+  const uint64_t wait_ns = wait_limit_ns();
   if (table.n > 0)
     herk_kernel<MODE, KD, true><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T,
                                                                  n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm,

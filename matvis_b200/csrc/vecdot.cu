@@ -121,7 +121,6 @@ constexpr int kVdClasses = 8;             // lanes served by one 128-byte shared
 constexpr int kVdBundleInts = 8;          // {i, j[3], pair[3], flip bits}
 constexpr int kVdSplitExtra = 31;         // extra k-slices the planner may add to fill the SMs
 constexpr int kVdSliceMax = 1024;         // longest k-slice: FP32 sums over at most 1,024 columns
-constexpr uint64_t kVdWaitNs = 2000000000ull;  // 2 s: limit of a stage wait
 constexpr uint64_t kVdDrainNs = 200000000ull;  // 0.2 s: limit of the in-flight wait on abort
 
 // Splits K_valid into nsplit k-slices of kc columns (a multiple of 16, at most
@@ -719,13 +718,13 @@ extern "C" int mvb_vecdot_staged(const void *z, int64_t Kcap, const int32_t *n_d
     if (rc) return rc;
     vecdot_staged_kernel<2><<<nsm, kVdCtaThreads, smem, s>>>(tmap, Kcap, n_dev, n_host, kmul, nant, bd,
                                                             (int)nbundles, group_size, ngroups, sg.kb, sg.nstage,
-                                                            sg.box_rows, sg.nbox, kmax, part, status, kVdWaitNs);
+                                                            sg.box_rows, sg.nbox, kmax, part, status, wait_limit_ns());
   } else {
     rc = set_smem_once(reinterpret_cast<const void *>(vecdot_staged_kernel<1>), kVdSmemBytes, 49);
     if (rc) return rc;
     vecdot_staged_kernel<1><<<nsm, kVdCtaThreads, smem, s>>>(tmap, Kcap, n_dev, n_host, kmul, nant, bd,
                                                             (int)nbundles, group_size, ngroups, sg.kb, sg.nstage,
-                                                            sg.box_rows, sg.nbox, kmax, part, status, kVdWaitNs);
+                                                            sg.box_rows, sg.nbox, kmax, part, status, wait_limit_ns());
   }
   rc = check_launch("vecdot_staged_kernel");
   if (rc) return rc;
