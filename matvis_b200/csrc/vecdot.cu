@@ -624,9 +624,8 @@ extern "C" int mvb_vecdot_plan(const int32_t *pairs, int64_t npairs, int nant, i
 // Shared-memory stages of the staged kernel for P rows: kb columns of 8 kb
 // bytes per row, the widest of which two fit (up to four stages; measured on
 // 700 rows: 16 columns in two stages 5.6 ms, 8 columns in four 10.0 ms), as
-// nbox boxes of
-// box_rows rows, each box a whole number of 1024-byte blocks so that every box
-// starts on a swizzle-pattern boundary.
+// nbox boxes of box_rows rows, each box a whole number of 1024-byte blocks so
+// that every box starts on a swizzle-pattern boundary.
 struct VdStages {
   int kb = 0, nstage = 0, box_rows = 0, nbox = 0, stage_bytes = 0;
 };
