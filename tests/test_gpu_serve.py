@@ -137,3 +137,25 @@ def test_small_jobs_form_a_priority_class(device):
     assert srv.result(js).queue_s <= srv.result(jb).queue_s
     np.testing.assert_array_equal(srv.result(js).vis, (lambda a: a if small.polarized else a[..., 0, 0])(
         VisEngine(small).run().cpu().numpy()))
+
+
+def test_turn_backlog_is_bounded(device):
+    """With turns_ahead=1 the server never holds more than one enqueued,
+    incomplete turn when it enqueues the next, and the results equal the
+    unbounded server's bit for bit."""
+    jobs = _jobs()[:4]
+    srv = VisServer(max_active=4, turns_ahead=1)
+    seen = []
+    advance = srv._advance
+
+    def watched():
+        seen.append(len(srv._turns))
+        advance()
+
+    srv._advance = watched
+    ia = srv.serve_stream([(0.0, s) for s in jobs])
+    free = VisServer(max_active=4, turns_ahead=None)
+    ib = free.serve_stream([(0.0, s) for s in jobs])
+    assert seen and max(seen) <= 1
+    for x, y in zip(ia, ib):
+        np.testing.assert_array_equal(srv.result(x).vis, free.result(y).vis)
