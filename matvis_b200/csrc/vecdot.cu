@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kVdCtaThreads, 1)
                       &full_bar[b]);
       }
     }
-      if (abort_flag) {
+    if (abort_flag) {
       // copies in flight land in this CTA's shared memory: wait (bounded) for the
       // last stage issued into each buffer
       for (int64_t x = g - nstage; x < g; ++x)
