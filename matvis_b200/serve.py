@@ -112,6 +112,7 @@ class VisServer:
         #: behind every turn already enqueued for the others.
         self.turns_ahead = turns_ahead
         self._turns: deque[list] = deque()
+        self._turn: list = []  # events that complete the turn being enqueued
         #: False: results keep the latency and term count only (a long benchmark stream)
         self.keep_results = keep_results
         #: kernel launches made for the admitted jobs (shared product launches counted once)
@@ -244,7 +245,7 @@ class VisServer:
     def _advance(self):
         if self._throttled():
             return
-        self._turn: list = []  # events that complete this turn's work
+        self._turn = []
         still = []
         batch = []
         for job in self._active:
