@@ -128,7 +128,13 @@ int mvb_horizon_compact_static(const double *topo, int64_t ld, int64_t c0, int64
  * GPUBeamInterpolator._interp (core/beams.py:184-208, gpu/beams.py:103-200). */
 int mvb_beam_interp(const void *grids, int grid_kind, int nbeam, int nax, int nfeed, int nza, int naz,
                     const double *params, const double *crd, int64_t ld, const int32_t *n_dev, int64_t nsrc,
-                    void *out, int out_c128, int64_t nout, int32_t *status, void *stream);
+                    void *out, int out_c128, int64_t nout, int32_t *status, void *ws, size_t ws_bytes,
+                    void *stream);
+/* Workspace of mvb_beam_interp (2 nbeam nout doubles).  With it (ws != NULL)
+ * each source's az/za and grid coordinates are computed once for all planes
+ * (a first kernel), with the same FP64 expressions; with ws = NULL every
+ * plane's threads recompute them. */
+size_t mvb_beam_interp_ws_bytes(int nbeam, int64_t nout);
 /* Same interpolation at given (azimuth, zenith angle) rows azza (SoA, leading
  * dim ld): the reference's gpu_beam_interpolation(beam, daz, dza, azmin, az, za)
  * (gpu/beams.py:127-200).  Output (nbeam, nfeed, nax, nsrc). */

@@ -64,8 +64,10 @@ _SIGNATURES = {
     ),
     "mvb_beam_interp": (
         c_int,
-        [_p, c_int, c_int, c_int, c_int, c_int, c_int, _p, _p, c_int64, _p, c_int64, _p, c_int, c_int64, _p, _p],
+        [_p, c_int, c_int, c_int, c_int, c_int, c_int, _p, _p, c_int64, _p, c_int64, _p, c_int, c_int64, _p, _p,
+         c_size_t, _p],
     ),
+    "mvb_beam_interp_ws_bytes": (c_size_t, [c_int, c_int64]),
     "mvb_beam_interp_azza": (
         c_int, [_p, c_int, c_int, c_int, c_int, c_int, c_int, _p, _p, c_int64, c_int64, _p, c_int, _p]
     ),

@@ -185,6 +185,7 @@ class B200BeamInterpolator(BeamInterpolator):
             (self.nbeam, self.nfeed, self.nax, self.nsrc), dtype=self.complex_dtype, device=dev
         )
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._coord_ws = None  # made at the first launch, or handed over by the engine
 
     def launch(self, crd: torch.Tensor, ld: int, n_dev, nsrc: int, out: torch.Tensor, stream=None, status=None):
         """Enqueue the interpolation at crd (SoA float64, leading dimension ld)."""
@@ -192,10 +193,15 @@ class B200BeamInterpolator(BeamInterpolator):
         nout = out.shape[-1]
         sh = stream_handle(stream)
         if self.use_interp:
+            # per-source grid coordinates, computed once for all the planes
+            if self._coord_ws is None or self._coord_ws.numel() < 2 * self.nbeam * nout:
+                self._coord_ws = torch.empty(2 * self.nbeam * nout, dtype=torch.float64, device=self.device)
+            ws = self._coord_ws
             check(
                 _lib.lib.mvb_beam_interp(
                     ptr(self.grids), self.grid_kind, self.nbeam, self.nax, self.nfeed, self.nza, self.naz,
-                    ptr(self.params), ptr(crd), ld, ptr(n_dev), nsrc, ptr(out), out_c128, nout, ptr(status), sh,
+                    ptr(self.params), ptr(crd), ld, ptr(n_dev), nsrc, ptr(out), out_c128, nout, ptr(status),
+                    ptr(ws), 0 if ws is None else ws.numel() * 8, sh,
                 )
             )
         else:

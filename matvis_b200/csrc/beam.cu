@@ -13,9 +13,10 @@
 // Layout: grids (nbeam, nax, nfeed, nza, naz), complex64 or float32 power;
 // output (nbeam, nfeed, nax, nout) complex.  One CTA stages ONE real plane
 // (a component of one (beam, ax, feed) grid, <= 200 KB) in shared memory and
-// interpolates it for a slice of the sources; the source's (az, za) is
-// recomputed in FP64 by each CTA that needs it.  Planes larger than the shared
-// memory budget are read through L2 instead.
+// interpolates it for a slice of the sources.  With a workspace, a first kernel
+// computes each source's FP64 (az, za) and its grid coordinates for every beam
+// once; without one, every plane's CTA recomputes them.  Planes larger than the
+// shared memory budget are read through L2 instead.
 #include <math_constants.h>
 
 #include "common.cuh"
@@ -58,10 +59,31 @@ __device__ __forceinline__ double bilinear(Load p, int nza, int naz, double row,
   return (1.0 - fr) * ((1.0 - fc) * v00 + fc * v01) + fr * ((1.0 - fc) * v10 + fc * v11);
 }
 
+// Grid coordinates of every source for every beam, once per call:
+// rc[(2 b) nout + i] = za / dza_b, rc[(2 b + 1) nout + i] = (az - azmin_b) / daz_b
+// (the plane kernel's own FP64 expressions), and row -1 (outside every grid:
+// a zero) for the slots i >= n.  One thread per source.
+__global__ void beam_rowcol_kernel(const BeamParams *__restrict__ params, int nbeam, const double *__restrict__ crd,
+                                   int64_t ld, const int32_t *__restrict__ n_dev, int64_t nsrc, int64_t nout,
+                                   double *__restrict__ rc) {
+  const int64_t n = n_dev ? min((int64_t)*n_dev, nsrc) : nsrc;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nout; i += (int64_t)gridDim.x * blockDim.x) {
+    double az = 0.0, za = 0.0;
+    if (i < n) az_za_uvbeam(crd[i], crd[ld + i], az, za);
+    for (int b = 0; b < nbeam; ++b) {
+      const BeamParams bp = params[b];
+      rc[(2 * b) * nout + i] = i < n ? za / bp.dza : -1.0;
+      rc[(2 * b + 1) * nout + i] = i < n ? (az - bp.azmin) / bp.daz : -1.0;
+    }
+  }
+}
+
 // grid_kind 0: complex64 (ncomp = 2), 1: float32 power (ncomp = 1).
 // plane q = ((b * nax + ax) * nfeed + fd) * ncomp + comp.
-// kAzZa: crd holds (az, za) rows instead of ENU (e, n) rows.
-template <bool kStaged, bool kAzZa = false>
+// kCoord 0: crd holds ENU (e, n) rows, az/za computed here per plane;
+// 1: crd holds (az, za) rows; 2: crd holds beam_rowcol_kernel's grid
+// coordinates (leading dimension nout), so no per-plane trigonometry.
+template <bool kStaged, int kCoord = 0>
 __global__ void __launch_bounds__(kBeamThreads)
     beam_plane_kernel(const float *__restrict__ grids, int grid_kind, int nbeam, int nax, int nfeed, int nza, int naz,
                       const BeamParams *__restrict__ params, const double *__restrict__ crd, int64_t ld,
@@ -89,14 +111,21 @@ __global__ void __launch_bounds__(kBeamThreads)
   for (int64_t i = blockIdx.y * (int64_t)kBeamThreads + threadIdx.x; i < nout; i += (int64_t)gridDim.y * kBeamThreads) {
     double v = 0.0;
     if (i < n) {
-      double az, za;
-      if (kAzZa) {
-        az = crd[i];
-        za = crd[ld + i];
+      double row, col;
+      if constexpr (kCoord == 2) {
+        row = crd[(2 * b) * nout + i];
+        col = crd[(2 * b + 1) * nout + i];
       } else {
-        az_za_uvbeam(crd[i], crd[ld + i], az, za);
+        double az, za;
+        if constexpr (kCoord == 1) {
+          az = crd[i];
+          za = crd[ld + i];
+        } else {
+          az_za_uvbeam(crd[i], crd[ld + i], az, za);
+        }
+        row = za / bp.dza;
+        col = (az - bp.azmin) / bp.daz;
       }
-      const double row = za / bp.dza, col = (az - bp.azmin) / bp.daz;
       if (kStaged)
         v = bilinear([&](int r, int c) { return (double)plane_smem[(int64_t)r * naz + c]; }, nza, naz, row, col);
       else
@@ -150,10 +179,14 @@ using namespace mvb;
 
 static int beam_interp_impl(bool azza, const void *grids, int grid_kind, int nbeam, int nax, int nfeed, int nza,
                             int naz, const double *params, const double *crd, int64_t ld, const int32_t *n_dev,
-                            int64_t nsrc, void *out, int out_c128, int64_t nout, int32_t *status, void *stream) {
+                            int64_t nsrc, void *out, int out_c128, int64_t nout, int32_t *status, void *ws,
+                            size_t ws_bytes, void *stream) {
+  const char *who = azza ? "mvb_beam_interp_azza" : "mvb_beam_interp";
   if (!grids || !params || !out || (nsrc > 0 && !crd) || nbeam <= 0 || nax <= 0 || nfeed <= 0 || nza < 1 || naz < 1 ||
       (grid_kind != 0 && grid_kind != 1) || nout < nsrc || nsrc < 0)
-    return fail(MVB_ERR_ARG, azza ? "mvb_beam_interp_azza: bad arguments" : "mvb_beam_interp: bad arguments");
+    return fail(MVB_ERR_ARG, "%s: bad arguments", who);
+  if (ws && (ws_bytes < (size_t)2 * nbeam * nout * sizeof(double) || reinterpret_cast<uintptr_t>(ws) % 8))
+    return fail(MVB_ERR_ARG, "%s: workspace too small", who);
   if (nout == 0) return MVB_OK;
   const int ncomp = grid_kind == 0 ? 2 : 1;
   const int nplanes = nbeam * nax * nfeed * ncomp;
@@ -165,39 +198,64 @@ static int beam_interp_impl(bool azza, const void *grids, int grid_kind, int nbe
   cudaStream_t s = as_stream(stream);
   const BeamParams *bp = reinterpret_cast<const BeamParams *>(params);
   const float *g = static_cast<const float *>(grids);
-#define MVB_BEAM(ST, AZ, SM)                                                                                          \
-  beam_plane_kernel<ST, AZ><<<grid, kBeamThreads, SM, s>>>(g, grid_kind, nbeam, nax, nfeed, nza, naz, bp, crd, ld, n_dev, \
-                                                           nsrc, out, out_c128, nout, status)
-  if (plane_bytes <= kBeamSmemMax) {
-    int rc = azza ? set_smem_once(reinterpret_cast<const void *>(beam_plane_kernel<true, true>), (int)kBeamSmemMax, 10)
-                  : set_smem_once(reinterpret_cast<const void *>(beam_plane_kernel<true, false>), (int)kBeamSmemMax, 11);
+  // with a workspace, the grid coordinates of each source are computed once for
+  // all planes (the ENU form only)
+  const bool pre = ws && !azza;
+  const double *coords = crd;
+  if (pre) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(nout, kBeamThreads), (int64_t)nsm * 8);
+    beam_rowcol_kernel<<<(unsigned)blocks, kBeamThreads, 0, s>>>(bp, nbeam, crd, ld, n_dev, nsrc, nout,
+                                                                 static_cast<double *>(ws));
+    int rc = check_launch("beam_rowcol_kernel");
     if (rc) return rc;
-    if (azza)
-      MVB_BEAM(true, true, plane_bytes);
+    coords = static_cast<const double *>(ws);
+  }
+#define MVB_BEAM(ST, CO, SM)                                                                                        \
+  beam_plane_kernel<ST, CO><<<grid, kBeamThreads, SM, s>>>(g, grid_kind, nbeam, nax, nfeed, nza, naz, bp, coords, ld, \
+                                                           n_dev, nsrc, out, out_c128, nout, status)
+  const int co = pre ? 2 : (azza ? 1 : 0);
+  if (plane_bytes <= kBeamSmemMax) {
+    const void *fn = co == 2 ? reinterpret_cast<const void *>(beam_plane_kernel<true, 2>)
+                             : (co == 1 ? reinterpret_cast<const void *>(beam_plane_kernel<true, 1>)
+                                        : reinterpret_cast<const void *>(beam_plane_kernel<true, 0>));
+    int rc = set_smem_once(fn, (int)kBeamSmemMax, 10 + co);
+    if (rc) return rc;
+    if (co == 2)
+      MVB_BEAM(true, 2, plane_bytes);
+    else if (co == 1)
+      MVB_BEAM(true, 1, plane_bytes);
     else
-      MVB_BEAM(true, false, plane_bytes);
+      MVB_BEAM(true, 0, plane_bytes);
   } else {
-    if (azza)
-      MVB_BEAM(false, true, 0);
+    if (co == 2)
+      MVB_BEAM(false, 2, 0);
+    else if (co == 1)
+      MVB_BEAM(false, 1, 0);
     else
-      MVB_BEAM(false, false, 0);
+      MVB_BEAM(false, 0, 0);
   }
 #undef MVB_BEAM
   return check_launch("beam_plane_kernel");
 }
 
+extern "C" size_t mvb_beam_interp_ws_bytes(int nbeam, int64_t nout) {
+  if (nbeam <= 0 || nout <= 0) return 8;
+  return (size_t)2 * nbeam * nout * sizeof(double);
+}
+
 extern "C" int mvb_beam_interp(const void *grids, int grid_kind, int nbeam, int nax, int nfeed, int nza, int naz,
                                const double *params, const double *crd, int64_t ld, const int32_t *n_dev, int64_t nsrc,
-                               void *out, int out_c128, int64_t nout, int32_t *status, void *stream) {
+                               void *out, int out_c128, int64_t nout, int32_t *status, void *ws, size_t ws_bytes,
+                               void *stream) {
   return beam_interp_impl(false, grids, grid_kind, nbeam, nax, nfeed, nza, naz, params, crd, ld, n_dev, nsrc, out,
-                          out_c128, nout, status, stream);
+                          out_c128, nout, status, ws, ws_bytes, stream);
 }
 
 extern "C" int mvb_beam_interp_azza(const void *grids, int grid_kind, int nbeam, int nax, int nfeed, int nza, int naz,
                                     const double *params, const double *azza, int64_t ld, int64_t nsrc, void *out,
                                     int out_c128, void *stream) {
   return beam_interp_impl(true, grids, grid_kind, nbeam, nax, nfeed, nza, naz, params, azza, ld, nullptr, nsrc, out,
-                          out_c128, nsrc, nullptr, stream);
+                          out_c128, nsrc, nullptr, nullptr, 0, stream);
 }
 
 extern "C" int mvb_beam_gaussian(const double *sigmas, int nbeam, const double *crd, int64_t ld, const int32_t *n_dev,

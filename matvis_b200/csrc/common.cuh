@@ -42,7 +42,7 @@ __host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return ceil_
 
 int num_sms();
 // Sets a kernel's max dynamic shared memory once per (device, slot < 64);
-// slots 10 and 11 are the beam kernels, 16..45 the Hermitian-product variants,
+// slots 10..12 are the beam kernels, 16..45 the Hermitian-product variants,
 // 48 and 49 the staged pair kernels.
 int set_smem_once(const void *fn, int bytes, int slot);
 // Wall-time limit of a pipeline wait in the product and the staged pair kernel

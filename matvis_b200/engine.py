@@ -282,8 +282,14 @@ class VisEngine:
                                       precision=1, device=dev)
             bf.setup()
             if self.bmfuncs:
+                # the per-frequency interpolators run in turn on one stream: one
+                # output and one coordinate workspace serve them all
                 bf.interpolated_beam = self.bmfuncs[0].interpolated_beam
             self.bmfuncs.append(bf)
+        if self.bmfuncs[0].use_interp:
+            ws = torch.empty(2 * self.bmfuncs[0].nbeam * max(self.cap, 1), dtype=torch.float64, device=dev)
+            for bf in self.bmfuncs:
+                bf._coord_ws = ws
         self.bmfunc = self.bmfuncs[0]
         if self.method == "MatMul":
             self.matprod = B200MatMul(1, self.nfeed, A, s.antpairs, precision=s.precision, gemm_mode=s.gemm_mode,
@@ -661,12 +667,17 @@ def estimate_device_bytes(spec: JobSpec) -> int:
         T = mpad // _lib.TILE
         kc = spec.k_chunk or choose_k_chunk(T * (T + 1) // 2, kcap)
         ws = G * _lib.lib.mvb_herk_ws_bytes(mpad, kcap, kc)
+    elif _lib.lib.mvb_vecdot_stage_columns(A, F) > 0:
+        # the staged pair kernel: bundles of up to 3 pairs, ~0.85 filled, in warps of 32
+        nb = -(-(int(npairs / 3 / 0.85) + 8) // 32) * 32
+        ws = _lib.lib.mvb_vecdot_staged_ws_bytes(nb, F, kcap, spec.k_chunk or 4096) + 32 * nb
     else:
         ws = _lib.lib.mvb_vecdot_ws_bytes(npairs, F, kcap, spec.k_chunk or 4096)
     nbeam = len(spec.beams)
     pol_sky = np.ndim(spec.fluxes) == 4
     extra = (16 * Nf * N + 16 * N + 16 * cap) if pol_sky else 0  # coherency, ra/dec, frame rotations
-    return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + 8 * nbeam * F * X * cap + panel + ws
+    beam = 8 * nbeam * F * X * cap + 16 * nbeam * cap  # interpolated beams, per-source grid coordinates
+    return int(24 * N + 8 * 3 * A + 4 * Nf * N + 24 * N + 28 * cap + beam + panel + ws
                + Nf * Nt * npairs * F * F * csize + extra)
 
 

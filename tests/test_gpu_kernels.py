@@ -117,6 +117,37 @@ def test_beam_interpolator_enu_matches_oracle(device):
     np.testing.assert_allclose(out, ref, rtol=0, atol=1e-6)
 
 
+def test_beam_coordinate_workspace_matches_per_plane_path(device):
+    """With a workspace the per-source grid coordinates are computed once for all
+    planes; the result equals the per-plane recomputation (same FP64
+    expressions) to the last bits of FP64, with the device's above-horizon count
+    bounding the sources and the slots past it zero."""
+    rng = np.random.default_rng(9)
+    beams = workloads.dipole_beams(rng, 3, dgrid_deg=1.0)
+    nout, n = 7000, 6123
+    e = rng.uniform(-0.7, 0.7, nout)
+    nn = rng.uniform(-0.7, 0.7, nout)
+    bi = mv.B200BeamInterpolator(beam_list=beams, beam_idx=np.array([0, 1, 2]), polarized=True, nant=3, freq=1e8,
+                                 nsrc=nout, precision=2)
+    bi.setup()
+    crd = torch.as_tensor(np.stack([e, nn]), device=DEV).contiguous()
+    n_dev = torch.tensor([n], dtype=torch.int32, device=DEV)
+    outs = []
+    for ws in (None, torch.empty(2 * 3 * nout, dtype=torch.float64, device=DEV)):
+        out = torch.full((3, 2, 2, nout), 7.0 + 7.0j, dtype=torch.complex128, device=DEV)
+        _lib.check(_lib.lib.mvb_beam_interp(
+            _lib.ptr(bi.grids), bi.grid_kind, 3, 2, 2, bi.nza, bi.naz, _lib.ptr(bi.params), _lib.ptr(crd), nout,
+            _lib.ptr(n_dev), nout, _lib.ptr(out), 1, nout, None, _lib.ptr(ws), 0 if ws is None else ws.numel() * 8,
+            _lib.stream_handle()))
+        outs.append(out.cpu().numpy())
+    np.testing.assert_allclose(outs[1], outs[0], rtol=1e-14, atol=1e-15)
+    assert (outs[1][..., n:] == 0).all() and np.abs(outs[1][..., :n]).max() > 0.1
+    with pytest.raises(ValueError, match="workspace"):
+        _lib.check(_lib.lib.mvb_beam_interp(
+            _lib.ptr(bi.grids), bi.grid_kind, 3, 2, 2, bi.nza, bi.naz, _lib.ptr(bi.params), _lib.ptr(crd), nout,
+            None, nout, _lib.ptr(out), 1, nout, None, _lib.ptr(ws), 8, _lib.stream_handle()))
+
+
 def test_hera_beamfits_beam_on_device_matches_oracle(device):
     """The reference's own HERA dipole file (tests/conftest.py:9-24), interpolated
     to 100.4 MHz and re-gridded on the host, then interpolated at 20,000 directions
