@@ -376,7 +376,13 @@ def run_reference(args, rank, world):
 
 
 def herk_roofline(eng, args, dev) -> dict:
-    """mvb_herk on the engine's last panel: algorithmic flops 4 M (M+1) K per launch."""
+    """mvb_herk on the engine's last panel.  ``achieved`` counts the split's
+    products on the upper triangle, P x 4 M (M+1) K flops per launch (P = 3 for
+    fp16x3 / tf32x3 / bf16x3, 6 for bf16x6), against the tensor peak of the
+    operands' precision (the measured bf16 burst; half of it for TF32, which has
+    no measured peak).  Also reported: the useful flops alone (one product,
+    ``useful_*``) and the flops the padded 128 x 128 tiles execute
+    (``executed_tensor_*``)."""
     import torch
 
     from matvis_b200 import _lib
@@ -409,7 +415,8 @@ def herk_roofline(eng, args, dev) -> dict:
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     bf16_peak = peaks.get("bf16_tflops", 1590.0)
     peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
-    achieved = algo_flops / (herk_ms / 1000.0) / 1e12
+    useful = algo_flops / (herk_ms / 1000.0) / 1e12
+    achieved = nprod * useful
     tensor_peak = bf16_peak / 2 if args.gemm_mode.startswith("tf32") else bf16_peak
     # DRAM bytes per launch from an ncu capture (dram__bytes_read/write.sum) of the
     # nside-64 slice of this workload (K = 49,152, k_chunk 4096: 305.8 MB read, 24.4 MB
@@ -419,10 +426,13 @@ def herk_roofline(eng, args, dev) -> dict:
     plane_bytes = 2 * (3 if args.gemm_mode == "bf16x6" else 2) * (4 if args.gemm_mode.startswith("tf32") else 2)
     traffic = 305.779968e6 / 49152 * kvalid * plane_bytes / 8 + 24.417536e6 / 252 * n_units
     roofline = {
-        "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
+        "bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s", "frac": achieved / tensor_peak,
+        "flops_counted": f"{nprod} split products x 4 M (M+1) K (upper triangle incl. diagonal)",
+        "useful_tflops": useful, "useful_frac_of_bf16": useful / bf16_peak,
         "traffic": traffic,
         "traffic_source": "ncu dram bytes of the nside-64 fp16x3 slice, scaled by columns, units and plane bytes",
-        "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)",
+        "peak_source": f"{peak_src} bf16 burst (MEASURED_PEAKS.json)"
+                       + ("; TF32 counted at half of it" if args.gemm_mode.startswith("tf32") else ""),
         "kernel": f"mvb_herk {args.gemm_mode}: M={M}, K={kvalid}, k_chunk={kc}",
         "herk_ms": herk_ms,
         "algorithmic_flops_per_launch": algo_flops,
