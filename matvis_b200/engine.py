@@ -508,8 +508,10 @@ class VisEngine:
         # and its reduction (mvb_herk[_grouped] + reduce, or vecdot_kernel + its slice reduction)
         per_f = 3
         nlaunch = len(self.freqs) if self.fgroup <= 1 else -(-len(self.freqs) // self.fgroup)
+        # a gridded beam is two launches (grid coordinates, then the planes), an analytic one one
+        bl = 1 if all(hasattr(b, "sigma") for b in self.spec.beams) else 2
         # count + scatter + beam (+ frame), per frequency (+ its beam for a beamfits beam)
-        per_chunk = 2 + int(not self.chromatic) + (per_f + int(self.chromatic)) * nlaunch + int(self.pol_sky)
+        per_chunk = 2 + bl * int(not self.chromatic) + (per_f + bl * int(self.chromatic)) * nlaunch + int(self.pol_sky)
         n = len(self.lsts) * (1 + self.nchunks * per_chunk)
         return n + (sum(self.bcrs_plan) if self.bcrs_plan is not None else 0)
 

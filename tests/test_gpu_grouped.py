@@ -96,7 +96,8 @@ def test_job_with_frequency_groups_vs_oracle(device, group):
     eng = VisEngine(_spec(cfg, freq_group=group, precision=2))
     vis = eng.run().cpu().numpy()
     assert eng.fgroup == min(group, 7)
-    assert eng.launches_per_run() == 2 * (1 + 3 + 3 * -(-7 // eng.fgroup))
+    # per time step: rotate, count, scatter, beam coordinates, beam planes, then tau/Z, product, reduce per group
+    assert eng.launches_per_run() == 2 * (1 + 4 + 3 * -(-7 // eng.fgroup))
     beams = [orc.GridBeam(data=b.data.astype(np.complex128), az=b.az, za=b.za) for b in cfg["beams"]]
     ref = orc.simulate_vis(ants={i: tuple(p) for i, p in enumerate(cfg["antpos"])}, fluxes=cfg["fluxes"],
                            ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"], lsts=cfg["lsts"],
