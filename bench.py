@@ -96,6 +96,10 @@ def parse():
     ap.add_argument("--serve-max-active", type=int, default=32)
     ap.add_argument("--serve-turns-ahead", type=int, default=2,
                     help="served form: turns enqueued ahead of the GPU (0: no bound)")
+    ap.add_argument("--serve-hbm-frac", type=float, default=0.75,
+                    help="served form: admission budget as a fraction of the free device memory")
+    ap.add_argument("--serve-turn-terms", type=float, default=2e11,
+                    help="served form: terms per turn, least work left first (0: every job every turn)")
     ap.add_argument("--serve-small-terms", type=float, default=2e11,
                     help="jobs of at most this many terms are the server's priority class (0: none)")
     return ap.parse_args()
@@ -740,12 +744,14 @@ def run_serve(args, local_rank):
     first.gemm_mode = args.gemm_mode
     small = args.serve_small_terms or None
     ahead = args.serve_turns_ahead or None
+    tt = args.serve_turn_terms or None
     warm = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False, small_job_terms=small,
-                     turns_ahead=ahead)
+                     turns_ahead=ahead, turn_terms=tt)
     warm.serve_stream([(0.0, first)])  # kernel warm-up, not timed
     warm.close()
-    srv = VisServer(device=dev, max_active=args.serve_max_active, keep_results=False, small_job_terms=small,
-                    turns_ahead=ahead)
+    budget = int(args.serve_hbm_frac * torch.cuda.mem_get_info(dev)[0])
+    srv = VisServer(device=dev, hbm_budget=budget, max_active=args.serve_max_active, keep_results=False,
+                    small_job_terms=small, turns_ahead=ahead, turn_terms=tt)
     hits0, miss0 = devcache.CACHE.hits, devcache.CACHE.misses
     t0 = time.perf_counter()
     srv.serve_stream(stream())
@@ -762,10 +768,12 @@ def run_serve(args, local_rank):
         "allocator": {k: torch.cuda.memory_stats(dev).get(k) for k in ("num_alloc_retries", "num_device_alloc",
                                                                       "num_device_free")},
         "alloc_conf": os.environ.get("PYTORCH_CUDA_ALLOC_CONF"),
+        "admission_oom_retries": srv.oom_retries,
         "config": {"workload": f"config5 stream: {args.serve_jobs} jobs, Poisson {args.serve_rate}/s, Nant log-U[16,512], "
                                f"Nsrc log-U[1e3,{args.serve_nsrc_max}], Nf U{{1..32}}, Nt U{{1..16}}, Gaussian or "
                                f"polarised grid beam", "gemm_mode": args.gemm_mode,
                    "max_active": args.serve_max_active, "small_job_terms": small, "turns_ahead": ahead,
+                   "turn_terms": tt, "hbm_budget_gb": budget / 1e9,
                    "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS")},
     }
     print(json.dumps(line), flush=True)

@@ -7,10 +7,13 @@ Jobs (``JobSpec``) arrive at any time.  The server
   others are on the GPU are admitted as soon as slots and memory free up;
 * keeps every admitted job's sky, beams, Z panel and partial visibilities
   resident on the device, and gives it its own CUDA stream;
-* advances the active jobs round robin, so their kernels overlap on the
-  device, with at most ``turns_ahead`` turns enqueued ahead of the GPU (so a
-  job admitted now starts behind a bounded backlog): each turn, every job's
-  next group of frequencies gets its tau/Z on
+* advances the active jobs in turns, so their kernels overlap on the device,
+  with at most ``turns_ahead`` turns enqueued ahead of the GPU (so a job
+  admitted now starts behind a bounded backlog).  A turn takes the jobs with
+  the least estimated work left first, until their next groups add up to
+  ``turn_terms`` terms (a job passed over ``max_skipped`` turns in a row is
+  taken regardless; ``turn_terms=None`` is plain round robin): each chosen
+  job's next group of frequencies gets its tau/Z on
   the job's stream, and the Hermitian products of all those groups run in one
   launch (``mvb_herk_batch``, up to 32 panels) on a shared stream, ordered
   against the jobs' streams by events; each job then reduces its own group
@@ -21,6 +24,8 @@ Jobs (``JobSpec``) arrive at any time.  The server
   high-priority streams, whose thread blocks the GPU dispatches first as SMs
   free up, so a short job does not wait behind a long one; larger jobs keep
   their arrival order;
+* defers a job whose buffers the allocator cannot place (fragmentation) until
+  another job retires, and fails it alone only if nothing else holds memory;
 * hands each finished job to a copier thread, which waits for the job's last
   kernel on its own stream, copies the visibilities and the status word to the
   host (touching the result's pages first), and counts the job's terms, so the
@@ -76,6 +81,9 @@ class _Job:
     t_done: float = 0.0
     terms: float = 0.0
     error: str | None = None
+    #: estimated terms of one frequency group, and turns passed over in a row
+    group_terms: float = 0.0
+    skipped: int = 0
 
 
 @dataclass
@@ -92,18 +100,30 @@ class VisServer:
     """Continuous-batching visibility server on one device."""
 
     def __init__(self, device=None, hbm_budget: int | None = None, max_active: int = 32, steps_per_turn: int = 1,
-                 reserve_fraction: float = 0.5, keep_results: bool = True, small_job_terms: float | None = 2e11,
-                 batch_products: bool = True, turns_ahead: int | None = 2):
+                 reserve_fraction: float = 0.0, keep_results: bool = True, small_job_terms: float | None = 2e11,
+                 batch_products: bool = True, turns_ahead: int | None = 2, turn_terms: float | None = 2e11,
+                 max_skipped: int = 8):
         self.device = _lib.require_cuda(device)
         free = torch.cuda.mem_get_info(self.device)[0]
-        self.budget = int(hbm_budget if hbm_budget is not None else 0.85 * free)
-        # Device allocations for a newly admitted job would otherwise reach
-        # cudaMalloc, which waits for the kernels of the jobs already running;
-        # a block of the budget taken once and handed back to torch's caching
-        # allocator lets admission carve the job's buffers from the cache.
+        # 0.75 of the free memory: at 0.85 the caching allocator's fragmentation
+        # made admissions run out of memory several times more often
+        self.budget = int(hbm_budget if hbm_budget is not None else 0.75 * free)
+        # every admitted job's buffers are allocated on this one stream, so the
+        # caching allocator hands a finished job's blocks to the next job (blocks
+        # are cached per allocating stream; a fresh stream per job would strand
+        # them, until an out-of-memory retry frees the whole cache with a device
+        # synchronisation).  A job's buffers are freed only after its last
+        # kernel has completed, so any stream may reuse them.
+        self._alloc_stream = torch.cuda.Stream(device=self.device)
+        # optionally, a block of the budget taken once and handed back to the
+        # cache of that stream, for jobs to be carved from (fewer cudaMalloc
+        # calls, at the risk of fragmenting one segment that can then never be
+        # released: off by default)
         if reserve_fraction > 0:
-            reserve = torch.empty(int(self.budget * min(reserve_fraction, 1.0)), dtype=torch.uint8, device=self.device)
-            del reserve
+            with torch.cuda.stream(self._alloc_stream):
+                reserve = torch.empty(int(self.budget * min(reserve_fraction, 1.0)), dtype=torch.uint8,
+                                      device=self.device)
+                del reserve
         self.max_active = max_active
         self.steps_per_turn = steps_per_turn
         #: turns enqueued on the device and not yet complete before the server
@@ -112,6 +132,16 @@ class VisServer:
         #: behind every turn already enqueued for the others.
         self.turns_ahead = turns_ahead
         self._turns: deque[list] = deque()
+        #: None: every active job advances each turn (round robin).  Otherwise a
+        #: turn takes the batched jobs with the least estimated work left first,
+        #: until their groups add up to this many terms; a job passed over
+        #: max_skipped turns in a row is taken regardless.
+        self.turn_terms = turn_terms
+        self.max_skipped = max_skipped
+        #: admissions that ran out of device memory (retried later), and the
+        #: memory in use when the last one did
+        self.oom_retries = 0
+        self._oom_wait: int | None = None
         self._turn: list = []  # events that complete the turn being enqueued
         #: False: results keep the latency and term count only (a long benchmark stream)
         self.keep_results = keep_results
@@ -122,13 +152,6 @@ class VisServer:
         self._small: deque[_Job] = deque()
         #: run the products of the active jobs' current frequency groups in shared launches
         self.batch_products = batch_products
-        # every admitted job's buffers are allocated on this one stream, so the
-        # caching allocator hands a finished job's blocks to the next job (blocks
-        # are cached per allocating stream; a fresh stream per job would strand
-        # them, until an out-of-memory retry frees the whole cache with a device
-        # synchronisation).  A job's buffers are freed only after its last
-        # kernel has completed, so any stream may reuse them.
-        self._alloc_stream = torch.cuda.Stream(device=self.device)
         self._batch_streams = {False: torch.cuda.Stream(device=self.device),
                                True: torch.cuda.Stream(device=self.device, priority=-1)}
         #: product launches (mvb_herk_batch) and the panel groups they carried
@@ -214,25 +237,55 @@ class VisServer:
                 job = q[0]
                 if self.in_use + job.footprint > self.budget:
                     break
+                if self._oom_wait is not None and self.in_use >= self._oom_wait:
+                    break  # the last admission ran out of device memory: wait for jobs to retire
+                self._oom_wait = None
+                if not self._allocate(job):
+                    if self._active or self._finishing:
+                        # the budget has room but the allocator could not place the
+                        # job's buffers: keep it at the head of its queue until a job
+                        # retires
+                        self._oom_wait = self.in_use
+                        break
+                    # nothing else holds device memory: the job cannot run here
+                    q.popleft()
+                    now = time.perf_counter()
+                    self._results[job.jid] = JobResult(jid=job.jid, vis=None, latency_s=now - job.t_submit,
+                                                       queue_s=now - job.t_submit, terms=0.0,
+                                                       error="out of device memory at admission")
+                    continue
                 q.popleft()
                 self.in_use += job.footprint
                 self.peak_in_use = max(self.peak_in_use, self.in_use)
                 job.t_admit = time.perf_counter()
                 job.stream = torch.cuda.Stream(device=self.device, priority=-1 if job.small else 0)
-                with torch.cuda.stream(self._alloc_stream):
-                    job.engine = VisEngine(job.spec, device=self.device)
-                    job.engine.allocate()
                 job.stream.wait_stream(self._alloc_stream)  # the buffers' zero fills
                 with torch.cuda.stream(job.stream):
                     job.engine.upload()
                     job.engine.status.zero_()
                 eng = job.engine
+                ngroups = len(eng.lsts) * eng.nchunks * -(-len(eng.freqs) // max(eng.fgroup, 1))
+                job.group_terms = estimate_terms(job.spec) / max(ngroups, 1)
                 self.launches += eng.launches_per_run()
                 if self.batch_products and eng.batchable:
                     # its product launches are shared ones, counted as they are made
                     self.launches -= len(eng.lsts) * eng.nchunks * -(-len(eng.freqs) // max(eng.fgroup, 1))
                 self._active.append(job)
         self.max_concurrent = max(self.max_concurrent, len(self._active))
+
+    def _allocate(self, job: _Job) -> bool:
+        """The job's engine and device buffers, on the allocation stream; False
+        (nothing kept) when the device cannot hold them (torch's allocator has
+        already released its unused cached blocks and retried before it raises)."""
+        try:
+            with torch.cuda.stream(self._alloc_stream):
+                job.engine = VisEngine(job.spec, device=self.device)
+                job.engine.allocate()
+            return True
+        except torch.OutOfMemoryError:
+            job.engine = None
+            self.oom_retries += 1
+            return False
 
     def _throttled(self) -> bool:
         """True while turns_ahead turns are enqueued and not yet complete."""
@@ -248,9 +301,15 @@ class VisServer:
         self._turn = []
         still = []
         batch = []
+        chosen = self._choose_batched()
         for job in self._active:
             eng = job.engine
             if self.batch_products and eng.batchable:
+                if chosen is not None and job.jid not in chosen:
+                    job.skipped += 1
+                    still.append(job)
+                    continue
+                job.skipped = 0
                 # this turn: the job's next frequency group up to its product
                 t, c, f0 = job.cursor
                 if t >= len(eng.lsts):  # no time steps at all
@@ -281,6 +340,28 @@ class VisServer:
         self._active = still + (self._launch_batches(batch) if batch else [])
         if self._turn:
             self._turns.append(self._turn)
+
+    def _remaining_terms(self, job: _Job) -> float:
+        eng = job.engine
+        t, c, f0 = job.cursor
+        per_t = eng.nchunks * -(-len(eng.freqs) // max(eng.fgroup, 1))
+        done = t * per_t + c * -(-len(eng.freqs) // max(eng.fgroup, 1)) + f0 // max(eng.fgroup, 1)
+        return (len(eng.lsts) * per_t - done) * job.group_terms
+
+    def _choose_batched(self) -> set | None:
+        """The batched jobs that advance this turn (None: all of them)."""
+        if self.turn_terms is None or not self.batch_products:
+            return None
+        jobs = [j for j in self._active if j.engine.batchable]
+        if not jobs:
+            return None
+        chosen, total = set(), 0.0
+        for j in sorted(jobs, key=lambda j: (j.skipped < self.max_skipped, self._remaining_terms(j))):
+            if chosen and total + j.group_terms > self.turn_terms and j.skipped < self.max_skipped:
+                continue
+            chosen.add(j.jid)
+            total += j.group_terms
+        return chosen
 
     def _finish(self, job: _Job):
         """The job's last kernel is enqueued: hand it to the copier."""

@@ -159,3 +159,32 @@ def test_turn_backlog_is_bounded(device):
     assert seen and max(seen) <= 1
     for x, y in zip(ia, ib):
         np.testing.assert_array_equal(srv.result(x).vis, free.result(y).vis)
+
+
+def test_admission_survives_out_of_memory(device, monkeypatch):
+    """An allocation that runs out of device memory at admission keeps the job
+    queued while others run (it is admitted once one retires), and fails only
+    that job when nothing else holds memory; the server keeps serving."""
+    import matvis_b200.serve as serve_mod
+
+    jobs = _jobs()[:3]
+    real = serve_mod.VisEngine.allocate
+    fails = {"n": 1}  # the second job's first admission runs out
+
+    def flaky(self):
+        if getattr(self.spec, "_flaky", False) and fails["n"] > 0:
+            fails["n"] -= 1
+            raise torch.OutOfMemoryError("simulated")
+        return real(self)
+
+    monkeypatch.setattr(serve_mod.VisEngine, "allocate", flaky)
+    jobs[1]._flaky = True
+    srv = VisServer(max_active=4)
+    ids = srv.serve_stream([(0.0, s) for s in jobs])
+    assert srv.oom_retries == 1
+    assert all(srv.result(i).error is None for i in ids)
+    # alone on the device, a job that cannot be placed fails by itself
+    fails["n"] = 1
+    lone = VisServer(max_active=4)
+    (jid,) = lone.serve_stream([(0.0, jobs[1])])
+    assert lone.result(jid).error == "out of device memory at admission"
