@@ -201,7 +201,7 @@ class B200BeamInterpolator(BeamInterpolator):
                 _lib.lib.mvb_beam_interp(
                     ptr(self.grids), self.grid_kind, self.nbeam, self.nax, self.nfeed, self.nza, self.naz,
                     ptr(self.params), ptr(crd), ld, ptr(n_dev), nsrc, ptr(out), out_c128, nout, ptr(status),
-                    ptr(ws), 0 if ws is None else ws.numel() * 8, sh,
+                    ptr(ws), ws.numel() * 8, sh,
                 )
             )
         else:
