@@ -19,7 +19,9 @@ on the job's own Z panel; frequencies per grouped launch sized to memory.
 ``tune_product`` times every candidate pair (a few launches each, CUDA events
 on a side stream) -- the product together with its reduction when the caller
 passes ``run`` -- and caches the winner per (mode, Mpad, K bucket, device) for
-the life of the process.  ``last_choice`` reports the latest decision.
+the life of the process; ``cached_choice`` hands it to later jobs of the same
+shape that are not captured (``simulate_vis``).  ``last_choice`` reports the
+latest decision.
 """
 
 from __future__ import annotations
@@ -108,6 +110,16 @@ def tune_product(panel, mode: int, status: torch.Tensor, run=None, reps: int = 3
     last_choice = {"k_chunk": best[0], "drain_ksteps": best[1], "ms": round(best_ms, 4), "timed_ms": timed,
                    "shape": {"Mpad": panel.Mpad, "K": kvalid, "mode": mode}}
     return best
+
+
+def cached_choice(mode: int, Mpad: int, kvalid: int, device: int) -> tuple[int, int] | None:
+    """A (k_chunk, drain_ksteps) already tuned in this process for this shape
+    (mode, Mpad, K bucket, device), or None."""
+    b = _bucket(max(int(kvalid), 1))
+    for key, choice in _cache.items():
+        if key[:4] == (mode, Mpad, b, device):
+            return choice
+    return None
 
 
 def tune_k_chunk(panel, mode: int, status: torch.Tensor, reps: int = 3, candidates=KC_CANDIDATES, run=None) -> int:

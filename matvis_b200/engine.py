@@ -317,6 +317,14 @@ class VisEngine:
         if self.method == "MatMul":
             panel = self.zcalc.z
             self.k_chunk = int(s.k_chunk) if s.k_chunk else DEFAULT_K_CHUNK
+            if not s.k_chunk and not self.matprod.drain_ksteps:
+                # a choice the autotuner made earlier in this process for this shape
+                # (about half the sky above the horizon)
+                hit = autotune.cached_choice(self.matprod.mode, panel.Mpad, self.nsrc // 2 * self.nax,
+                                             torch.device(dev).index or 0)
+                if hit is not None:
+                    self.k_chunk, self.matprod.drain_ksteps = hit
+                    self.tuned = {"k_chunk": hit[0], "drain_ksteps": hit[1], "cached": True}
             self.matprod.workspace(panel, self.k_chunk, self.fgroup)
         self._allocated = True
 

@@ -126,6 +126,13 @@ def test_autotuner_reports_its_choice(device):
                            ra=cfg["ra"], dec=cfg["dec"], freqs=cfg["freqs"], lsts=cfg["lsts"],
                            latitude=cfg["latitude"], beams=beams, polarized=True, beam_idx=cfg["beam_idx"])
     assert orc.cosine_error_metric(vis, ref, 2) <= 1e-6
+    # a later, uncaptured job of the same shape (simulate_vis's path) takes the tuned choice
+    again = VisEngine(_spec(cfg, precision=2))
+    again.allocate()
+    assert (again.k_chunk, again.matprod.drain_ksteps) == (t["k_chunk"], t["drain_ksteps"])
+    assert again.tuned["cached"]
+    out = again.run_to_host()
+    assert orc.cosine_error_metric(out, ref, 2) <= 1e-6
 
 
 def test_batched_products_of_different_shapes_equal_their_own_launches(device):
