@@ -415,7 +415,9 @@ def herk_roofline(eng, args, dev) -> dict:
     algo_flops = 4.0 * M * (M + 1) * kvalid
     T = panel.Mpad // 128
     nprod = _lib.GEMM_PRODUCTS[_lib.GEMM_MODES[args.gemm_mode]]
-    exec_flops = 8.0 * (T * (T + 1) // 2) * 128 * 128 * kvalid * nprod
+    # 128 x 128 complex tiles: four real products per split product off the diagonal,
+    # three on the T diagonal tiles (their imaginary half is W - W^T of one product)
+    exec_flops = 2.0 * 128 * 128 * kvalid * nprod * (4 * (T * (T - 1) // 2) + 3 * T)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     bf16_peak = peaks.get("bf16_tflops", 1590.0)
     peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
