@@ -213,8 +213,10 @@ int mvb_absmax(const void *z, int z_c128, int64_t n, float *out, void *stream);
  *   K_valid = min(n * kmul, Kcap),  n = *n_dev if n_dev != NULL else n_host,
  * i.e. a source count times the columns per source (nax); the device count
  * comes straight from mvb_horizon_compact, with no host round trip. */
-/* Workspace bytes: one FP32 partial tile (256 x 128 floats) per (k-slice, tile);
- * the workspace must be 16-byte aligned. */
+/* Workspace bytes: one FP32 partial tile (256 x 128 floats) per (k-slice, tile)
+ * and 256 bytes for the launch's work-unit counter (its last 16 bytes; the
+ * product zeroes it on its stream before each launch, so two products must not
+ * run at once on one workspace); the workspace must be 16-byte aligned. */
 size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
 /* Upper-triangle 128 x 128 complex tiles of V = conj(Z) Z^T over K_valid
  * columns, on the tcgen05 tensor cores with TMEM accumulators, fed by one bulk
@@ -223,7 +225,10 @@ size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk);
  * K_valid is cut into equal k-slices of at most k_chunk columns (a multiple of
  * 64).  Their count, between ceil(K_valid / k_chunk) and 31 more, is chosen on
  * the device from K_valid so that tiles x slices fills whole waves of SMs; one
- * partial tile is written per (k-slice, tile).
+ * partial tile is written per (k-slice, tile).  The persistent CTAs take these
+ * work units in order from the counter in the workspace; a diagonal tile's
+ * imaginary half holds W, with Im V = W - W^T formed by the reductions, so the
+ * partial tiles are meant for mvb_herk_reduce* only.
  * drain_ksteps (1, 2 or 4; 0 = default 2) is the number of 32-byte k-steps
  * summed in one TMEM block before the block is added to FP32 registers: the
  * tensor core rounds its accumulator toward zero at every instruction, so short

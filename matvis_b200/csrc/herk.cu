@@ -42,8 +42,15 @@
 // that run together read the same Z columns (L2 reuse).  A launch covers ngroup
 // panels of one shape (the frequencies of a time step, zstride bytes apart)
 // that share the column count; with ngroup = 1 it is one product.  Persistent CTAs (one per SM,
-// 192 KB of shared memory) loop over units.  Warp roles (576 threads):
-//   warp 0 lane 0 : producer, one 1-D bulk copy per operand per stage: the
+// 192 KB of shared memory) take units in index order from a counter in the
+// workspace (zeroed on the stream before each launch), so a CTA that drew
+// cheaper diagonal tiles takes more units: with static round-robin the CTAs'
+// loads differed by up to a tile's work (one panel of 700 rows: 0.92-0.96 of
+// the mean).  Each unit's sums do not depend on which CTA computes it.
+// Warp roles (576 threads):
+//   warp 0 lane 0 : producer; fetches the CTA's next unit index and hands it
+//                   to the other roles through a 4-entry shared-memory ring
+//                   (full / empty mbarriers); one 1-D bulk copy per operand per stage: the
 //                   panel stores each (k-block, row block) as the stage's
 //                   shared-memory image (all 2P split/component planes of 128
 //                   rows x 64 bytes, 64-byte swizzled; two k-steps), so an
@@ -78,6 +85,8 @@ constexpr uint64_t kWaitLimitNs = 4000000000ull;   // 4 s: the default limit of 
 constexpr uint64_t kDrainLimitNs = 200000000ull;   // 0.2 s
 constexpr int kPlaneBytes = 128 * 64;              // one 128-row x 64-byte plane tile (two k-steps)
 constexpr int kSmemBudget = 192 * 1024;
+constexpr int kUnitRing = 4;       // unit indices the producer may fetch ahead of the MMA and epilogue
+constexpr size_t kCounterBytes = 256;  // the launch's unit counter, in the last 16 bytes of the workspace
 
 template <int MODE>
 struct HerkCfg {
@@ -197,8 +206,8 @@ template <int MODE, int KD, bool TABLE>
 __global__ void __launch_bounds__(kHerkThreads, 1)
     herk_kernel(const uint8_t *__restrict__ zpanels, int64_t zstride, int ngroup, int T, int n_tiles,
                 const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap, int k_chunk, int nsm,
-                float *__restrict__ partials, int32_t *__restrict__ status, uint64_t wait_ns,
-                const __grid_constant__ HerkTable table) {
+                float *__restrict__ partials, int32_t *__restrict__ status, int *__restrict__ unit_next,
+                uint64_t wait_ns, const __grid_constant__ HerkTable table) {
   using C = HerkCfg<MODE>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[C::STAGES];
@@ -206,6 +215,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   __shared__ __align__(8) uint64_t dfull_bar[2];
   __shared__ __align__(8) uint64_t dempty_bar[2];
   __shared__ __align__(8) uint64_t drain_bar;
+  __shared__ __align__(8) uint64_t ufull_bar[kUnitRing];   // a unit index is in unit_q
+  __shared__ __align__(8) uint64_t uempty_bar[kUnitRing];  // every role has read it
+  __shared__ int unit_q[kUnitRing];
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
 
@@ -292,6 +304,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       mbar_init(&dempty_bar[b], kEpiWarps);
     }
     mbar_init(&drain_bar, 1);
+    for (int i = 0; i < kUnitRing; ++i) {
+      mbar_init(&ufull_bar[i], 1);
+      mbar_init(&uempty_bar[i], 1 + kEpiWarps);
+    }
     abort_flag = 0;
     fence_mbar_init();
   }
@@ -308,7 +324,18 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   if (warp == 0 && lane == 0) {
     // ---------------- bulk-copy producer ----------------
     uint32_t st = 0, ph = 0;
-    for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
+    for (uint32_t uk = 0; !abort_flag; ++uk) {
+      // the CTA's next unit from the launch's counter, handed to the other roles
+      const int us = uk % kUnitRing;
+      if (!mbar_wait(&uempty_bar[us], ((uk / kUnitRing) & 1u) ^ 1u, wait_ns)) {
+        flag_timeout();
+        abort_flag = 1;
+        break;
+      }
+      const int u = min(atomicAdd(unit_next, 1), n_units);
+      unit_q[us] = u;
+      mbar_arrive(&ufull_bar[us]);
+      if (u >= n_units) break;
       const uint8_t *zpanel;
       float *partial;
       int Tu, I, J;
@@ -341,7 +368,16 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   } else if (warp == 1 && lane == 0) {
     // ---------------- UMMA issuer: one fresh TMEM block per KD k-steps ----------------
     uint32_t st = 0, ph = 0, buf = 0, dph = 0;
-    for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
+    for (uint32_t uk = 0; !abort_flag; ++uk) {
+      const int us = uk % kUnitRing;
+      if (!mbar_wait(&ufull_bar[us], (uk / kUnitRing) & 1u, wait_ns)) {
+        flag_timeout();
+        abort_flag = 1;
+        break;
+      }
+      const int u = unit_q[us];
+      mbar_arrive(&uempty_bar[us]);
+      if (u >= n_units) break;
       const uint8_t *zpanel;
       float *partial;
       int Tu, I, J;
@@ -471,7 +507,18 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     float acc[64];
 #pragma unroll
     for (int j = 0; j < 64; ++j) acc[j] = 0.f;
-    for (int u = blockIdx.x; u < n_units && !abort_flag; u += gridDim.x) {
+    for (uint32_t uk = 0; !abort_flag; ++uk) {
+      const int us = uk % kUnitRing;
+      // every lane waits; the vote keeps the warp converged
+      if (!__all_sync(0xffffffffu, mbar_wait(&ufull_bar[us], (uk / kUnitRing) & 1u, wait_ns))) {
+        if (lane == 0) flag_timeout();
+        abort_flag = 1;
+        break;
+      }
+      const int u = unit_q[us];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&uempty_bar[us]);
+      if (u >= n_units) break;
       const uint8_t *zpanel;
       float *partial;
       int Tu, I, J;
@@ -739,8 +786,8 @@ uint64_t wait_limit_ns() { return g_wait_limit_ns.load(std::memory_order_relaxed
 // table.n > 0: the units come from the table (z, ngroup, shape and status arguments unused).
 template <int MODE, int KD>
 static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad, int64_t Kcap, const int32_t *n_dev,
-                       int64_t n_host, int kmul, int k_chunk, float *partials, int32_t *status, cudaStream_t s,
-                       const HerkTable &table) {
+                       int64_t n_host, int kmul, int k_chunk, float *partials, int32_t *status, int *unit_next,
+                       cudaStream_t s, const HerkTable &table) {
   using C = HerkCfg<MODE>;
   const int T = (int)(Mpad / 128);
   const int n_tiles = T * (T + 1) / 2;
@@ -763,14 +810,17 @@ static int launch_herk(const void *z, int64_t zstride, int ngroup, int64_t Mpad,
   if (rc) return rc;
   if (grid <= 0) return MVB_OK;
   const uint64_t wait_ns = wait_limit_ns();
+  // the CTAs take units from this counter, zeroed on the launch's stream
+  cudaError_t e = cudaMemsetAsync(unit_next, 0, sizeof(int), s);
+  if (e != cudaSuccess) return fail(MVB_ERR_CUDA, "herk unit counter: %s", cudaGetErrorString(e));
   if (table.n > 0)
     herk_kernel<MODE, KD, true><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T,
                                                                  n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm,
-                                                                 partials, status, wait_ns, table);
+                                                                 partials, status, unit_next, wait_ns, table);
   else
     herk_kernel<MODE, KD, false><<<grid, kHerkThreads, smem, s>>>(static_cast<const uint8_t *>(z), zstride, ngroup, T,
                                                                   n_tiles, n_dev, n_host, kmul, Kcap, k_chunk, nsm,
-                                                                  partials, status, wait_ns, table);
+                                                                  partials, status, unit_next, wait_ns, table);
   return check_launch("herk_kernel");
 }
 
@@ -819,13 +869,15 @@ static int herk_impl(const char *who, const void *z, int64_t zstride, int ngroup
   const int kd = drain_ksteps ? drain_ksteps : 2;
   cudaStream_t s = as_stream(stream);
   float *part = static_cast<float *>(ws);
-#define MVB_HERK(M)                                                                                                 \
-  return kd == 1   ? launch_herk<M, 1>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s, \
-                                       table)                                                                       \
-         : kd == 2 ? launch_herk<M, 2>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s, \
-                                       table)                                                                       \
-                   : launch_herk<M, 4>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, s, \
-                                       table)
+  // past every partial tile: each group's share of ws_bytes holds kCounterBytes spare
+  int *next = reinterpret_cast<int *>(static_cast<uint8_t *>(ws) + ((ws_bytes - 16) & ~size_t(15)));
+#define MVB_HERK(M)                                                                                          \
+  return kd == 1   ? launch_herk<M, 1>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, \
+                                       next, s, table)                                                       \
+         : kd == 2 ? launch_herk<M, 2>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, \
+                                       next, s, table)                                                       \
+                   : launch_herk<M, 4>(z, zstride, ngroup, Mpad, Kcap, n_dev, n_host, kmul, k_chunk, part, status, \
+                                       next, s, table)
   switch (mode) {
     case MVB_GEMM_BF16_3: MVB_HERK(MVB_GEMM_BF16_3);
     case MVB_GEMM_BF16_6: MVB_HERK(MVB_GEMM_BF16_6);
@@ -894,7 +946,8 @@ extern "C" uint64_t mvb_set_wait_limit_ns(uint64_t limit_ns) {
 extern "C" size_t mvb_herk_ws_bytes(int64_t Mpad, int64_t Kcap, int k_chunk) {
   if (Mpad <= 0 || Kcap <= 0 || k_chunk <= 0) return 0;
   const int64_t T = Mpad / 128;
-  return (size_t)(T * (T + 1) / 2) * (size_t)(ceil_div(Kcap, k_chunk) + kPlanExtra) * 256 * 128 * sizeof(float);
+  return (size_t)(T * (T + 1) / 2) * (size_t)(ceil_div(Kcap, k_chunk) + kPlanExtra) * 256 * 128 * sizeof(float) +
+         kCounterBytes;
 }
 
 extern "C" int mvb_herk(const void *z, int mode, int64_t Mpad, int64_t Kcap, const int32_t *n_dev, int64_t n_host,

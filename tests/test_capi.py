@@ -44,7 +44,7 @@ def test_workspace_queries_without_gpu():
     from matvis_b200 import _lib
 
     assert _lib.lib.mvb_version() == 1
-    assert _lib.lib.mvb_herk_ws_bytes(768, 393216, 2048) == 21 * (192 + 31) * 256 * 128 * 4  # up to 31 slices beyond ceil(K / k_chunk)
+    assert _lib.lib.mvb_herk_ws_bytes(768, 393216, 2048) == 21 * (192 + 31) * 256 * 128 * 4 + 256  # up to 31 slices beyond ceil(K / k_chunk), and the unit counter
     assert _lib.lib.mvb_zpanel_bytes(_lib.GEMM_BF16_6, 768, 393216) == 6 * 768 * 393216 * 2
     assert _lib.lib.mvb_horizon_ws_bytes(196608) == 192 * 4
     assert _lib.lib.mvb_vecdot_ws_bytes(10, 2, 4096, 1024) == 4 * 10 * 4 * 2 * 8

@@ -174,6 +174,8 @@ def test_batched_products_of_different_shapes_equal_their_own_launches(device):
         mp.reduce_grouped(panels, out, k_chunk=2048)
         torch.cuda.synchronize()
         _lib.check_status_word(mp.status, f"batched group {i}")
-        # the whole workspace (zeroed before either run) holds the same bytes
-        assert torch.equal(mp.workspace(panels[0], 2048, G), alone_ws[i]), i
+        # the workspace (zeroed before either run) holds the same bytes, all but
+        # its last 256: the launch's work-unit counter, which ends at a count that
+        # depends on the launch (units plus CTAs)
+        assert torch.equal(mp.workspace(panels[0], 2048, G)[:-256], alone_ws[i][:-256]), i
         np.testing.assert_array_equal(out.cpu().numpy(), alone_out[i])
