@@ -618,45 +618,83 @@ struct FF {
 };
 
 // Sums of the k-slices' partial values of this thread's four rows r0 .. r0 + 3
-// of column c: real and imaginary halves, and for a diagonal tile (DIAG) also
-// the imaginary half's transposed elements (row c, columns r0 .. r0 + 3; the
-// CTA's 8 column warps read one 32-byte sector of each such column, through L1).
-template <bool DIAG>
+// of column c, real and imaginary halves.
 __device__ __forceinline__ void sum_slices(const float *__restrict__ tile, int nsplit, size_t tstride, int c, int r0,
-                                           FF (&are)[4], FF (&aim)[4], FF (&aimt)[4]) {
+                                           FF (&are)[4], FF (&aim)[4]) {
   const size_t sstride = tstride / 4;  // in float4
   const float4 *pre = reinterpret_cast<const float4 *>(tile + c * 128 + r0);
   const float4 *pim = reinterpret_cast<const float4 *>(tile + (128 + c) * 128 + r0);
-  const float *pimt = tile + (128 + r0) * 128 + c;
   int s = 0;
   // eight slices per step: 16 independent 16-byte loads in flight, sums in slice order
   for (; s + 8 <= nsplit; s += 8) {
     float4 vr[8], vi[8];
-    float vt[DIAG ? 8 : 1][4];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       vr[u] = __ldg(pre + (s + u) * sstride);
       vi[u] = __ldg(pim + (s + u) * sstride);
-      if constexpr (DIAG)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) vt[u][k] = __ldg(pimt + (s + u) * tstride + k * 128);
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       are[0].add(vr[u].x), are[1].add(vr[u].y), are[2].add(vr[u].z), are[3].add(vr[u].w);
       aim[0].add(vi[u].x), aim[1].add(vi[u].y), aim[2].add(vi[u].z), aim[3].add(vi[u].w);
-      if constexpr (DIAG)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) aimt[k].add(vt[u][k]);
     }
   }
   for (; s < nsplit; ++s) {
     const float4 vr = __ldg(pre + s * sstride), vi = __ldg(pim + s * sstride);
     are[0].add(vr.x), are[1].add(vr.y), are[2].add(vr.z), are[3].add(vr.w);
     aim[0].add(vi.x), aim[1].add(vi.y), aim[2].add(vi.z), aim[3].add(vi.w);
-    if constexpr (DIAG)
+  }
+}
+
+// sum_slices for a diagonal tile, plus the imaginary half's transposed elements
+// (row c, columns r0 .. r0 + 3) for Im V = W - W^T.  The CTA (columns c0 ..
+// c0 + 7, warp w = c - c0) stages them through shared memory two slices at a
+// time (eight held 176 registers a thread and four spilled at the 80 registers
+// that keep three CTAs of the kernel on an SM): thread i loads 16 bytes of column i / 2 (rows c0 + 4 (i % 2) .. + 3, two
+// threads per 32-byte sector) and scatters them so that every thread then
+// reads its four values as one 16-byte word.  Every thread of the CTA must
+// call it: it holds __syncthreads, and nsplit is uniform over the CTA.
+__device__ __forceinline__ void sum_slices_diag(const float *__restrict__ tile, int nsplit, size_t tstride, int c0,
+                                                int w, int lane, FF (&are)[4], FF (&aim)[4], FF (&aimt)[4]) {
+  constexpr int kS = 2;              // slices per step
+  __shared__ float4 tsm[kS][8][32];  // [slice of the step][column warp][lane]: rows 4 lane .. 4 lane + 3
+  const int c = c0 + w, r0 = 4 * lane;
+  const size_t sstride = tstride / 4;  // in float4
+  const float4 *pre = reinterpret_cast<const float4 *>(tile + c * 128 + r0);
+  const float4 *pim = reinterpret_cast<const float4 *>(tile + (128 + c) * 128 + r0);
+  const int rr = threadIdx.x >> 1, hh = threadIdx.x & 1;  // this thread's load: column rr, rows c0 + 4 hh ..
+  const float4 *pt = reinterpret_cast<const float4 *>(tile + (128 + rr) * 128 + c0 + 4 * hh);
+  // element (row c0 + 4 hh + j, column rr) belongs to warp 4 hh + j, lane rr / 4, component rr % 4
+  float *tdst = reinterpret_cast<float *>(&tsm[0][4 * hh][rr >> 2]) + (rr & 3);
+  for (int s = 0; s < nsplit; s += kS) {
+    const int nu = min(kS, nsplit - s);
+    float4 vr[kS], vi[kS], vt[kS];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) aimt[k].add(__ldg(pimt + s * tstride + k * 128));
+    for (int u = 0; u < kS; ++u)
+      if (u < nu) {
+        vr[u] = __ldg(pre + (s + u) * sstride);
+        vi[u] = __ldg(pim + (s + u) * sstride);
+        vt[u] = __ldg(pt + (s + u) * sstride);
+      }
+    __syncthreads();  // the previous step's reads of tsm are done
+#pragma unroll
+    for (int u = 0; u < kS; ++u)
+      if (u < nu) {
+        float *d = tdst + u * (8 * 32 * 4);
+        d[0 * 32 * 4] = vt[u].x;
+        d[1 * 32 * 4] = vt[u].y;
+        d[2 * 32 * 4] = vt[u].z;
+        d[3 * 32 * 4] = vt[u].w;
+      }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kS; ++u)
+      if (u < nu) {
+        const float4 t4 = tsm[u][w][lane];
+        are[0].add(vr[u].x), are[1].add(vr[u].y), are[2].add(vr[u].z), are[3].add(vr[u].w);
+        aim[0].add(vi[u].x), aim[1].add(vi[u].y), aim[2].add(vi[u].z), aim[3].add(vi[u].w);
+        aimt[0].add(t4.x), aimt[1].add(t4.y), aimt[2].add(t4.z), aimt[3].add(t4.w);
+      }
   }
 }
 
@@ -668,7 +706,7 @@ __device__ __forceinline__ void sum_slices(const float *__restrict__ tile, int n
 // arithmetic).  blockIdx.y is the panel of a grouped product; its output is
 // out_stride bytes further.
 template <typename OT, int F>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     herk_reduce_all_kernel(const float *__restrict__ part, int ngroup, int T, int n_tiles,
                            const int32_t *__restrict__ n_dev, int64_t n_host, int kmul, int64_t Kcap, int k_chunk,
                            int nsm, int A, void *__restrict__ out_base, int64_t out_stride, double vscale,
@@ -687,14 +725,18 @@ __global__ void __launch_bounds__(256)
   const int c = g * 8 + w;
   const int n = J * 128 + c;
   const int r0 = 4 * lane;
-  if (n >= M || I * 128 + r0 >= M) return;  // nothing of this thread's to write
+  const bool live = n < M && I * 128 + r0 < M;  // this thread has outputs to write
   FF are[4], aim[4], aimt[4];
   const float *tile = part + (size_t)t * (256 * 128);
   const size_t tstride = (size_t)n_tiles * (256 * 128);
-  if (I == J)
-    sum_slices<true>(tile, nsplit, tstride, c, r0, are, aim, aimt);
-  else
-    sum_slices<false>(tile, nsplit, tstride, c, r0, are, aim, aimt);
+  if (I == J) {
+    // every thread takes part (the staging synchronises the CTA); its reads stay inside the tile
+    sum_slices_diag(tile, nsplit, tstride, g * 8, w, lane, are, aim, aimt);
+    if (!live) return;
+  } else {
+    if (!live) return;
+    sum_slices(tile, nsplit, tstride, c, r0, are, aim);
+  }
   const int64_t AF2 = (int64_t)A * F * F;
   const int jj = n / F, pp = n % F;  // F is 1 or 2: shifts and masks
 #pragma unroll
