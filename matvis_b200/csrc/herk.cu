@@ -41,20 +41,20 @@
 // Schedule.  Work unit u = (panel g, k-slice s, tile t), t fastest so the CTAs
 // that run together read the same Z columns (L2 reuse).  A launch covers ngroup
 // panels of one shape (the frequencies of a time step, zstride bytes apart)
-// that share the column count; with ngroup = 1 it is one product.  Persistent CTAs (one per SM,
-// 192 KB of shared memory) take units in index order from a counter in the
-// workspace (zeroed on the stream before each launch), so a CTA that drew
-// cheaper diagonal tiles takes more units: with static round-robin the CTAs'
-// loads differed by up to a tile's work (one panel of 700 rows: 0.92-0.96 of
-// the mean).  Each unit's sums do not depend on which CTA computes it.
-// Warp roles (576 threads):
+// that share the column count; with ngroup = 1 it is one product.
+// Persistent CTAs (one per SM, 192 KB of shared memory) take units in index
+// order from a counter in the workspace (zeroed on the stream before each
+// launch), so a CTA that drew cheaper diagonal tiles takes more units: with
+// static round-robin the CTAs' loads differed by up to a tile's work (one
+// panel of 700 rows: 0.92-0.96 of the mean).  Each unit's sums do not depend
+// on which CTA computes it.  Warp roles (576 threads):
 //   warp 0 lane 0 : producer; fetches the CTA's next unit index and hands it
 //                   to the other roles through a 4-entry shared-memory ring
-//                   (full / empty mbarriers); one 1-D bulk copy per operand per stage: the
-//                   panel stores each (k-block, row block) as the stage's
-//                   shared-memory image (all 2P split/component planes of 128
-//                   rows x 64 bytes, 64-byte swizzled; two k-steps), so an
-//                   operand is one contiguous 2P x 8 KB run.  A bulk copy of it
+//                   (full / empty mbarriers); one 1-D bulk copy per operand
+//                   per stage: the panel stores each (k-block, row block) as
+//                   the stage's shared-memory image (all 2P split/component
+//                   planes of 128 rows x 64 bytes, 64-byte swizzled; two
+//                   k-steps), so an operand is one contiguous 2P x 8 KB run.  A bulk copy of it
 //                   completes in about half the time of the same bytes as tiled
 //                   TMA boxes of 64-byte rows, and the three stages in flight no
 //                   longer leave the MMA waiting;
